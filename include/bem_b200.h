@@ -1,0 +1,192 @@
+/*
+ * bem_b200.h -- C ABI of the B200 boundary-element library (libbemb200.so).
+ *
+ * Dense complex Helmholtz Galerkin BEM on triangle meshes in the P1 vertex
+ * basis: single-/double-layer (and adjoint-double, hypersingular,
+ * Burton-Miller) matrix assembly, the exterior-Neumann solve and
+ * boundary-to-listener evaluation.  It replaces the pybind module that the
+ * NeuralAT reference JIT-builds from src/bem/cuda/bind.cu (bindings at
+ * bind.cu:178-223, loader src/bem/solver.py:9-31).
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers on the current CUDA device,
+ *    unless a comment says "host".
+ *  - vertices: float32 (nv, 3) row-major; triangles: int32 (nt, 3) row-major.
+ *  - Complex arrays are interleaved complex64 (re, im) unless marked complex128.
+ *  - Matrices are row-major: entry (a, b) at a * nv + b, rows = test-triangle
+ *    vertices, columns = trial-triangle vertices (bind.cu:144-151).
+ *  - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ *    stream).  Functions return a bem_status; 0 = success.  Functions that
+ *    must inspect data on the host (geometry set-up, solver convergence)
+ *    synchronise `stream`; all others are asynchronous.
+ *  - The library never allocates device memory for outputs: the caller
+ *    passes every output and workspace buffer.  Workspace sizes are queried
+ *    with the *_bytes functions.
+ *  - The library has no CPU fallback: without a usable CUDA device every
+ *    entry point returns BEM_ERR_CUDA.
+ */
+#ifndef BEM_B200_H
+#define BEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* bem_stream_t; /* cudaStream_t */
+
+typedef enum bem_status {
+  BEM_OK = 0,
+  BEM_ERR_INVALID_ARGUMENT = 1, /* null pointer, negative size, unknown enum */
+  BEM_ERR_INDEX = 2,            /* triangle vertex index outside [0, nv) */
+  BEM_ERR_DEGENERATE = 3,       /* zero-area triangle or repeated vertex */
+  BEM_ERR_WORKSPACE = 4,        /* workspace missing, too small or not built */
+  BEM_ERR_NONFINITE = 5,        /* NaN / Inf in an input */
+  BEM_ERR_NOT_CONVERGED = 6,    /* iteration limit reached before tolerance */
+  BEM_ERR_BREAKDOWN = 7,        /* Krylov breakdown / singular system */
+  BEM_ERR_CUDA = 8,             /* CUDA runtime error (incl. no device) */
+  BEM_ERR_UNSUPPORTED = 9       /* valid request this build does not support */
+} bem_status;
+
+/* Operator types, same order as the reference's PotentialType
+ * (src/bem/cuda/include/potential.h:7-15). */
+enum {
+  BEM_SINGLE_LAYER = 0,
+  BEM_DOUBLE_LAYER = 1,
+  BEM_ADJOINT_DOUBLE_LAYER = 2,
+  BEM_HYPERSINGULAR = 3,
+  BEM_BM_LHS = 4,
+  BEM_BM_RHS = 5
+};
+
+/* Quadrature orders: (singular Gauss-Legendre points per dimension,
+ * regular triangle-rule points), bind.cu:180-215. */
+enum {
+  BEM_ORDER_EXACT = 0,    /* <4,6>  "*_boundary_matrix"          */
+  BEM_ORDER_APPROX = 1,   /* <2,3>  "*_boundary_matrix_approx"   */
+  BEM_ORDER_APPROX_1 = 2  /* <2,1>  "*_boundary_matrix_approx_1" */
+};
+
+/* Human-readable name of a status code (static string). */
+const char* bem_status_string(int status);
+/* Library version string (static). */
+const char* bem_version(void);
+
+/* ------------------------------------------------------------------------
+ * Geometry.  Replaces the per-call mesh handling of bind.cu:49-66 and the
+ * Python preprocess (src/bem/solver.py:40-58): validates the mesh, computes
+ * unit normals, surface curls, quadrature points, a locality-sorted triangle
+ * order with 16-triangle tiles, and the touching-pair lists (the reference
+ * rediscovers these by an O(T^2) scan in every call, bind.cu:81-97).
+ * Both calls copy the mesh to the host and synchronise `stream`.
+ * ---------------------------------------------------------------------- */
+int bem_geometry_bytes(const float* vertices, int nv, const int* triangles, int nt, size_t* bytes,
+                       bem_stream_t stream);
+int bem_geometry_build(const float* vertices, int nv, const int* triangles, int nt, void* geom,
+                       size_t geom_bytes, bem_stream_t stream);
+/* Copies the per-triangle unit normals (nt,3) and surface curls (nt,3,3)
+ * (rows b: n x grad phi_b), solver.py:40-58.  Either output may be NULL. */
+int bem_geometry_normals(const void* geom, float* normals, float* curls, bem_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Assembly on a built geometry.
+ * ---------------------------------------------------------------------- */
+
+/* Dense nv x nv Galerkin matrix of `layer` at quadrature `order`,
+ * overwriting `out` (complex64).  Replaces the 18 assemble_matrix
+ * bindings, bind.cu:49-154,180-215.  `normals`/`curls` (may be NULL: the
+ * geometry's own) are the per-triangle arrays the reference passes in for
+ * the hypersingular and Burton-Miller operators (bind.cu:100-104). */
+int bem_boundary_matrix(const void* geom, int layer, int order, float k, const float* normals,
+                        const float* curls, void* out, bem_stream_t stream);
+
+/* Fused single-layer + double-layer assembly (exact order): one pass over
+ * all triangle pairs evaluates each distance and phase once for both.
+ *   v_out (may be NULL)  <- V
+ *   k_out (may be NULL)  <- mass_coeff * M + k_coeff * K
+ * With mass_coeff = 0.5, k_coeff = -1 this is the CBIE left-hand side
+ * 0.5 I - K of src/bem/solver.py:97-104. */
+int bem_boundary_matrices_vk(const void* geom, float k, void* v_out, void* k_out, float mass_coeff,
+                             float k_coeff, bem_stream_t stream);
+
+/* Dense P1 mass matrix (bind.cu:10-21), overwriting out. */
+int bem_identity_matrix(const void* geom, void* out, bem_stream_t stream);
+
+/* Per-triangle complex values averaged onto vertices, bind.cu:23-48.
+ * tri_values (nt) complex64 -> out (nv) complex64.  `counts` is an int32
+ * scratch array of nv entries. */
+int bem_triangle2vertex(const void* geom, const void* tri_values, void* out, int* counts,
+                        bem_stream_t stream);
+
+/* Listener potential matrix (np x nv complex64, overwritten) of the single
+ * (layer 0) or double (layer 1) layer, bind.cu:156-176. */
+int bem_potential_matrix(const void* geom, int layer, const float* points, int np, float k, void* out,
+                         bem_stream_t stream);
+
+/* Fused listener evaluation without a potential matrix:
+ *   out(:, s) = -S neumann(:, s) + D dirichlet(:, s),   s = 0..nrhs-1
+ * (src/bem/solver.py:140-147).  neumann/dirichlet are (nv, nrhs) complex64
+ * row-major (either may be NULL = zero); out is (np, nrhs) complex64,
+ * overwritten.  scratch: bem_boundary2potential_scratch_bytes() bytes. */
+size_t bem_boundary2potential_scratch_bytes(int nt, int nrhs);
+int bem_boundary2potential(const void* geom, const float* points, int np, float k, const void* neumann,
+                           const void* dirichlet, int nrhs, void* out, void* scratch,
+                           size_t scratch_bytes, bem_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Dense complex linear algebra.
+ * ---------------------------------------------------------------------- */
+
+/* Y = A X for an n x n complex64 row-major A and m right-hand sides
+ * X (n, m) row-major complex64 -> Y (n, m) complex64 (overwritten).
+ * Replaces the cuBLAS gemv the reference calls through torch `@`
+ * (src/bem/solver.py:103,147; BiCGSTAB.py:52,68,73). */
+int bem_cmatmul(const void* A, int n, const void* X, int m, void* Y, bem_stream_t stream);
+
+/* Solver precision of the dense operator. */
+enum {
+  BEM_PREC_FP32 = 0,   /* complex64 CUDA-core matvec */
+  BEM_PREC_BF16X3 = 1, /* tensor-core bf16 hi/lo split (3 products), FP32 accumulate */
+  BEM_PREC_BF16 = 2    /* tensor-core bf16 (1 product), FP32 accumulate */
+};
+
+typedef struct bem_solver_params {
+  int precision;     /* BEM_PREC_* of the inner Krylov matvec */
+  int restart;       /* GMRES restart length (Krylov dimension), >= 1 */
+  int max_iters;     /* total inner iterations per solve */
+  int max_refine;    /* outer FP64 refinement steps (>= 1) */
+  double rtol;       /* stop when ||b - A x|| <= rtol ||b|| (per column) */
+  double atol;       /* or when ||b - A x|| <= atol */
+  double inner_rtol; /* inner GMRES tolerance relative to its own RHS */
+} bem_solver_params;
+
+typedef struct bem_solver_info {
+  int status;         /* bem_status of the whole solve */
+  int iterations;     /* inner iterations (max over columns) */
+  int refinements;    /* outer refinement steps taken */
+  int matvecs;        /* operator applications */
+  double rel_residual; /* max over columns of ||b - A x|| / ||b|| (FP64, FP32 A) */
+} bem_solver_info;
+
+/* Workspace bytes for bem_gmres_solve (n unknowns, m right-hand sides). */
+size_t bem_gmres_workspace_bytes(int n, int m, const bem_solver_params* params);
+
+/* Solve A X = B for m right-hand sides with restarted GMRES (device-resident
+ * Arnoldi, FP64 classical Gram-Schmidt with re-orthogonalisation and Givens
+ * rotations) wrapped in FP64 iterative refinement against the FP32 matrix.
+ * A: n x n complex64 row-major.  B: (n, m) complex64.  X: (n, m) complex64,
+ * used as the initial guess when `use_x0` != 0 and overwritten with the
+ * solution.  `info` is a HOST pointer.  Synchronises `stream` once per
+ * restart cycle.  Replaces solve_linear_equation / BiCGSTAB
+ * (src/bem/solver.py:61-66, src/bem/BiCGSTAB.py:5-107). */
+int bem_gmres_solve(const void* A, int n, const void* B, int m, void* X, int use_x0,
+                    const bem_solver_params* params, void* workspace, size_t workspace_bytes,
+                    bem_solver_info* info, bem_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEM_B200_H */

@@ -1,0 +1,577 @@
+// Dense Galerkin assembly of the Helmholtz single-layer (V) and double-layer
+// (K) matrices in the P1 vertex basis, plus the P1 mass matrix.
+//
+// Reference behaviour (file:line inside the NeuralAT project):
+//   regular pairs     src/bem/cuda/bind.cu:67-79, integrand.h:187-235,280-329
+//   singular pairs    src/bem/cuda/bind.cu:81-152, integrand.h:63-185,331-394
+//   kernels           src/bem/cuda/include/potential.h:18-32 (r >= 1e-3 clamp)
+//   mass matrix       src/bem/cuda/bind.cu:10-21, integrand.h:257-278
+//
+// Design (B200): the reference launches one block per test triangle, sweeps
+// every trial triangle with one thread each, recomputes r and exp(ikr)
+// separately for V and for K, and scatters 18 float atomics per pair into the
+// N x N matrix.  Here:
+//   * one pass evaluates each quadrature-point pair once for BOTH operators
+//     (shared r, rsqrt and sincos), with the 6-point rule's constant weights
+//     folded into immediate FMA operands;
+//   * a CTA owns 32 test triangles (one per lane) x one 16-triangle trial
+//     tile; all 8 warps share the test triangles and broadcast their trial
+//     triangles from shared memory;
+//   * pair blocks go to a shared-memory "corner" slab (test corner x trial
+//     corner) and are reduced on chip onto the tile's distinct vertices, so
+//     each matrix entry receives ~0.8 vector atomics per triangle pair instead
+//     of the reference's 18 scalar atomics;
+//   * touching pairs are masked out of the regular pass and integrated by
+//     separate Sauter-Schwab kernels (coincident pairs in FP64), one warp per
+//     pair over a precomputed pair list (no O(T^2) adjacency scan).
+
+#include <cmath>
+
+#include "bem_common.cuh"
+
+namespace bemb {
+
+int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Regular triangle pairs.
+// ---------------------------------------------------------------------------
+constexpr int kRegThreads = 256;
+constexpr int kRegWarps = kRegThreads / 32;
+constexpr int kTestTris = 32;                  // one test triangle per lane
+constexpr int kTestCorners = 3 * kTestTris;     // 96
+constexpr int kSlotStride = kTileCorners + 1;   // 49 float2: conflict-free column writes
+
+template <bool DO_V, bool DO_K>
+struct RegSmem {
+  float2 slotV[DO_V ? kTestCorners : 1][kSlotStride];
+  float2 slotK[DO_K ? kTestCorners : 1][kSlotStride];
+  TriRec trial[kTile];
+  TileRec tileJ;
+  TileRec tileI[2];
+};
+
+// 3x3 P1 blocks of one (test, trial) pair under the 6x6 point rule:
+//   aV[3a+b] = sum_pq C_ap C_bq e^{ikr}/r,
+//   aK[3a+b] = sum_pq C_ap C_bq dn_p (c + kr s + i(s - kr c)) / r^3,
+// with C_aq = w_q phi_a(q), dn_p = n_j . (y - x_p) (constant over the trial
+// plane), r clamped to >= 1e-3 (potential.h:21-23).  The 1/(4 pi), the
+// areas and the double layer's minus sign are applied by the caller.
+template <bool DO_V, bool DO_K>
+__device__ __forceinline__ void pair_block(const float (&xq)[18], const float (&yq)[18], float njx, float njy,
+                                           float njz, float cjx, float cjy, float cjz, float k, float2 (&aV)[9],
+                                           float2 (&aK)[9]) {
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    aV[e] = make_float2(0.f, 0.f);
+    aK[e] = make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int p = 0; p < 6; p++) {
+    const float px = xq[3 * p], py = xq[3 * p + 1], pz = xq[3 * p + 2];
+    const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);
+    float2 tV[3], tK[3];
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      tV[b] = make_float2(0.f, 0.f);
+      tK[b] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const float dx = yq[3 * q] - px, dy = yq[3 * q + 1] - py, dz = yq[3 * q + 2] - pz;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float rinv = fminf(rsqrtf(r2), 1.0f / kEps);
+      const float r = fmaxf(r2 * rinv, kEps);
+      float s, c;
+      __sincosf(k * r, &s, &c);
+      const float gvr = c * rinv, gvi = s * rinv;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        const float w = (float)(tri6_w(q) * tri6_phi(q, b));
+        if (DO_V) {
+          tV[b].x = fmaf(w, gvr, tV[b].x);
+          tV[b].y = fmaf(w, gvi, tV[b].y);
+        }
+      }
+      if (DO_K) {
+        const float rinv2 = rinv * rinv;
+        const float gkr = fmaf(k, s, gvr) * rinv2;   // (c + kr s) / r^3
+        const float gki = fmaf(-k, c, gvi) * rinv2;  // (s - kr c) / r^3
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          const float w = (float)(tri6_w(q) * tri6_phi(q, b));
+          tK[b].x = fmaf(w, gkr, tK[b].x);
+          tK[b].y = fmaf(w, gki, tK[b].y);
+        }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float wa = (float)(tri6_w(p) * tri6_phi(p, a));
+      const float wk = wa * dn;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        if (DO_V) {
+          aV[3 * a + b].x = fmaf(wa, tV[b].x, aV[3 * a + b].x);
+          aV[3 * a + b].y = fmaf(wa, tV[b].y, aV[3 * a + b].y);
+        }
+        if (DO_K) {
+          aK[3 * a + b].x = fmaf(wk, tK[b].x, aK[3 * a + b].x);
+          aK[3 * a + b].y = fmaf(wk, tK[b].y, aK[3 * a + b].y);
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes, int tid, int nthreads) {
+  const int4* s = (const int4*)src;
+  int4* d = (int4*)dst;
+  for (int i = tid; i < bytes / 16; i += nthreads) d[i] = s[i];
+}
+
+// Work item = (group of 32 test triangles = 2 tiles) x (chunk of `chunk`
+// trial tiles).  Items are dealt round-robin to a persistent grid.
+template <bool DO_V, bool DO_K>
+__global__ void __launch_bounds__(kRegThreads, 2)
+    regular_vk_kernel(GeomView g, float k, float2* __restrict__ V, float2* __restrict__ K, float v_scale,
+                      float k_scale, int chunk, int n_chunks, int n_items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RegSmem<DO_V, DO_K>& sm = *reinterpret_cast<RegSmem<DO_V, DO_K>*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nt = g.nt, nv = g.nv;
+
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int grp = item / n_chunks;
+    const int ch = item - grp * n_chunks;
+    const int tile0 = 2 * grp;
+    const bool has_t1 = tile0 + 1 < g.ntiles;
+
+    // test triangle of this lane (all warps hold the same 32)
+    const int ti = grp * kTestTris + lane;
+    const bool valid_i = ti < nt;
+    const TriRec& ri = g.rec[valid_i ? ti : nt - 1];
+    float xq[18];
+#pragma unroll
+    for (int e = 0; e < 18; e++) xq[e] = ri.qp[e];
+    const float area_i = ri.area;
+    const int iv0 = ri.v[0], iv1 = ri.v[1], iv2 = ri.v[2];
+
+    __syncthreads();  // previous item's gather has finished with tileI
+    copy_words(&sm.tileI[0], &g.tiles[tile0], sizeof(TileRec), tid, kRegThreads);
+    if (has_t1) copy_words(&sm.tileI[1], &g.tiles[tile0 + 1], sizeof(TileRec), tid, kRegThreads);
+
+    const int jt_begin = ch * chunk;
+    const int jt_end = min(jt_begin + chunk, g.ntiles);
+    for (int jt = jt_begin; jt < jt_end; jt++) {
+      __syncthreads();  // gather of the previous trial tile is done with the slots
+      copy_words(&sm.tileJ, &g.tiles[jt], sizeof(TileRec), tid, kRegThreads);
+      const int ntriJ = min(kTile, nt - jt * kTile);
+      copy_words(sm.trial, &g.rec[jt * kTile], ntriJ * (int)sizeof(TriRec), tid, kRegThreads);
+      __syncthreads();
+
+      // ---- compute: each warp takes trial triangles warp and warp + 8 ----
+#pragma unroll 1
+      for (int tt = warp; tt < ntriJ; tt += kRegWarps) {
+        const TriRec& rj = sm.trial[tt];
+        float yq[18];
+#pragma unroll
+        for (int e = 0; e < 18; e++) yq[e] = rj.qp[e];
+        float2 aV[9], aK[9];
+        pair_block<DO_V, DO_K>(xq, yq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aV, aK);
+        const int j0 = rj.v[0], j1 = rj.v[1], j2 = rj.v[2];
+        const bool touching = (iv0 == j0) | (iv0 == j1) | (iv0 == j2) | (iv1 == j0) | (iv1 == j1) | (iv1 == j2) |
+                              (iv2 == j0) | (iv2 == j1) | (iv2 == j2);
+        const float aa = (valid_i && !touching) ? area_i * rj.area : 0.f;
+        const float sv = aa * v_scale, sk = aa * k_scale;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int b = 0; b < 3; b++) {
+            if (DO_V) sm.slotV[3 * lane + a][3 * tt + b] = make_float2(aV[3 * a + b].x * sv, aV[3 * a + b].y * sv);
+            if (DO_K) sm.slotK[3 * lane + a][3 * tt + b] = make_float2(aK[3 * a + b].x * sk, aK[3 * a + b].y * sk);
+          }
+      }
+      __syncthreads();
+
+      // ---- reduce corner slots onto distinct vertices, one atomic per entry ----
+      const int nI0 = sm.tileI[0].nlv;
+      const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
+      const int nJ = sm.tileJ.nlv;
+      const int total = (nI0 + nI1) * nJ;
+      for (int e = tid; e < total; e += kRegThreads) {
+        const int ai = e / nJ;
+        const int b = e - ai * nJ;
+        const int s = ai >= nI0;
+        const int a = ai - s * nI0;
+        const TileRec& TI = sm.tileI[s];
+        float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f);
+        const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+        const int cb0 = sm.tileJ.lv_ptr[b], cb1 = sm.tileJ.lv_ptr[b + 1];
+        for (int ca = ca0; ca < ca1; ca++) {
+          const int row = s * kTileCorners + TI.lv_corner[ca];
+          for (int cb = cb0; cb < cb1; cb++) {
+            const int col = sm.tileJ.lv_corner[cb];
+            if (DO_V) {
+              acc_v.x += sm.slotV[row][col].x;
+              acc_v.y += sm.slotV[row][col].y;
+            }
+            if (DO_K) {
+              acc_k.x += sm.slotK[row][col].x;
+              acc_k.y += sm.slotK[row][col].y;
+            }
+          }
+        }
+        const size_t idx = (size_t)TI.vid[a] * nv + sm.tileJ.vid[b];
+        if (DO_V) atomicAdd(&V[idx], acc_v);
+        if (DO_K) atomicAdd(&K[idx], acc_k);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Singular (touching) pairs: Sauter-Schwab quadrature on the reference
+// triangle (0,0),(1,0),(1,1) (integrand.h:54-185), after re-ordering so the
+// shared vertices come first (integrand.h:351-387).  One warp per pair; the
+// lanes split the 4^4 Gauss-Legendre points; blocks are reduced with
+// shuffles and added with one atomic per entry.
+// ---------------------------------------------------------------------------
+
+template <typename R>
+struct R3 {
+  R x, y, z;
+};
+
+template <typename R>
+__device__ __forceinline__ void sincos_t(R x, R* s, R* c);
+template <>
+__device__ __forceinline__ void sincos_t<double>(double x, double* s, double* c) {
+  sincos(x, s, c);
+}
+template <>
+__device__ __forceinline__ void sincos_t<float>(float x, float* s, float* c) {
+  sincosf(x, s, c);
+}
+
+// Re-ordering of the reference (integrand.h:351-387): for a common edge the
+// shared vertices take local slots 0,1 in trial order; for a common vertex it
+// is swapped into slot 0 on both triangles.
+__device__ __forceinline__ void reorder_pair(const int si[3], const int sj[3], int ncommon, int pi[3], int pj[3]) {
+  pi[0] = 0; pi[1] = 1; pi[2] = 2;
+  pj[0] = 0; pj[1] = 1; pj[2] = 2;
+  if (ncommon == 2) {
+    int idx = 0;
+#pragma unroll
+    for (int jj = 0; jj < 3; jj++)
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++)
+        if (si[ii] == sj[jj] && idx < 2) {
+          pi[idx] = ii;
+          pj[idx] = jj;
+          idx++;
+        }
+    pi[2] = 3 - pi[0] - pi[1];
+    pj[2] = 3 - pj[0] - pj[1];
+  } else if (ncommon == 1) {
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+      for (int jj = 0; jj < 3; jj++)
+        if (si[ii] == sj[jj]) {
+          if (ii != 0) { pi[0] = ii; pi[ii] = 0; }
+          if (jj != 0) { pj[0] = jj; pj[jj] = 0; }
+        }
+  }
+}
+
+template <typename R, int NCOMMON, bool DO_V, bool DO_K>
+struct SingularAcc {
+  R v[18];  // 9 complex, (re, im) pairs, index 3 * test + trial (re-ordered)
+  R kk[18];
+  R3<R> a[3];  // re-ordered test vertices
+  R3<R> b[3];  // re-ordered trial vertices
+  R3<R> nj;    // unit normal of the trial triangle
+  R k;
+
+  // One Sauter-Schwab region: point (x1, x2) on the test triangle and (y1, y2)
+  // on the trial triangle, shape functions (1 - s, s - t, t), weight ww.
+  __device__ __forceinline__ void region(R x1, R x2, R y1, R y2, R ww) {
+    const R lx0 = R(1) - x1, lx1 = x1 - x2, lx2 = x2;
+    const R ly0 = R(1) - y1, ly1 = y1 - y2, ly2 = y2;
+    const R xx = lx0 * a[0].x + lx1 * a[1].x + lx2 * a[2].x;
+    const R xy = lx0 * a[0].y + lx1 * a[1].y + lx2 * a[2].y;
+    const R xz = lx0 * a[0].z + lx1 * a[1].z + lx2 * a[2].z;
+    const R yx = ly0 * b[0].x + ly1 * b[1].x + ly2 * b[2].x;
+    const R yy = ly0 * b[0].y + ly1 * b[1].y + ly2 * b[2].y;
+    const R yz = ly0 * b[0].z + ly1 * b[1].z + ly2 * b[2].z;
+    const R dx = yx - xx, dy = yy - xy, dz = yz - xz;
+    R r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (r < R(kEps)) r = R(kEps);
+    R s, c;
+    const R kr = k * r;
+    sincos_t<R>(kr, &s, &c);
+    const R inv_r = R(1) / r;
+    const R gvr = c * inv_r * ww, gvi = s * inv_r * ww;
+    R gkr = 0, gki = 0;
+    if (DO_K) {
+      const R dn = dx * nj.x + dy * nj.y + dz * nj.z;  // (y - x) . n_trial
+      const R f = dn * inv_r * inv_r * inv_r * ww;
+      gkr = (c + kr * s) * f;
+      gki = (s - kr * c) * f;
+    }
+    const R lx[3] = {lx0, lx1, lx2}, ly[3] = {ly0, ly1, ly2};
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+      for (int jj = 0; jj < 3; jj++) {
+        const R f = lx[ii] * ly[jj];
+        if (DO_V) {
+          v[2 * (3 * ii + jj)] += gvr * f;
+          v[2 * (3 * ii + jj) + 1] += gvi * f;
+        }
+        if (DO_K) {
+          kk[2 * (3 * ii + jj)] += gkr * f;
+          kk[2 * (3 * ii + jj) + 1] += gki * f;
+        }
+      }
+  }
+
+  // One 4D Gauss point (xi, e1, e2, e3 on [0,1]) of weight w0; the region
+  // Jacobian w (integrand.h:121,134,146) is applied to every region.
+  __device__ __forceinline__ void point(R xi, R e1, R e2, R e3, R w0) {
+    const R e12 = e1 * e2, e123 = e1 * e2 * e3;
+    if (NCOMMON == 3) {
+      const R sc = xi * xi * xi * e1 * e1 * e2 * w0;
+      region(xi, xi * (R(1) - e1 + e12), xi * (R(1) - e123), xi * (R(1) - e1), sc);
+      region(xi * (R(1) - e123), xi * (R(1) - e1), xi, xi * (R(1) - e1 + e12), sc);
+      region(xi, xi * (e1 - e12 + e123), xi * (R(1) - e12), xi * (e1 - e12), sc);
+      region(xi * (R(1) - e12), xi * (e1 - e12), xi, xi * (e1 - e12 + e123), sc);
+      region(xi * (R(1) - e123), xi * (e1 - e123), xi, xi * (e1 - e12), sc);
+      region(xi, xi * (e1 - e12), xi * (R(1) - e123), xi * (e1 - e123), sc);
+    } else if (NCOMMON == 2) {
+      const R sc = xi * xi * xi * e1 * e1 * w0;
+      region(xi, xi * e1 * e3, xi * (R(1) - e12), xi * e1 * (R(1) - e2), sc);
+      region(xi, xi * e1, xi * (R(1) - e123), xi * e1 * e2 * (R(1) - e3), e2 * sc);
+      region(xi * (R(1) - e12), xi * e1 * (R(1) - e2), xi, xi * e123, e2 * sc);
+      region(xi * (R(1) - e123), xi * e12 * (R(1) - e3), xi, xi * e1, e2 * sc);
+      region(xi * (R(1) - e123), xi * e1 * (R(1) - e2 * e3), xi, xi * e12, e2 * sc);
+    } else {
+      const R sc = xi * xi * xi * e2 * w0;
+      region(xi, xi * e1, xi * e2, xi * e2 * e3, sc);
+      region(xi * e2, xi * e2 * e3, xi, xi * e1, sc);
+    }
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ R warp_sum(R x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// NCOMMON = 3: pairs (i, i), i = pair index; otherwise pairs from the list.
+template <typename R, int NCOMMON, bool DO_V, bool DO_K>
+__global__ void __launch_bounds__(128)
+    singular_vk_kernel(GeomView g, const int2* __restrict__ pairs, int npairs, float k, float2* __restrict__ V,
+                       float2* __restrict__ K, float v_scale, float k_scale, float mass_coeff) {
+  const int lane = threadIdx.x & 31;
+  const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pair >= npairs) return;
+  const int ti = NCOMMON == 3 ? pair : pairs[pair].x;
+  const int tj = NCOMMON == 3 ? pair : pairs[pair].y;
+  int si[3], sj[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    si[c] = g.triangles[3 * ti + c];
+    sj[c] = g.triangles[3 * tj + c];
+  }
+  int pi[3], pj[3];
+  reorder_pair(si, sj, NCOMMON, pi, pj);
+  R3<R> pa[3], pb[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int va = si[pi[c]], vb = sj[pj[c]];
+    pa[c] = {(R)g.vertices[3 * va], (R)g.vertices[3 * va + 1], (R)g.vertices[3 * va + 2]};
+    pb[c] = {(R)g.vertices[3 * vb], (R)g.vertices[3 * vb + 1], (R)g.vertices[3 * vb + 2]};
+  }
+  // Jacobians and the trial normal of the un-permuted triangles
+  auto jac_normal = [](const R3<R>* p, R3<R>* n) {
+    const R e1x = p[1].x - p[0].x, e1y = p[1].y - p[0].y, e1z = p[1].z - p[0].z;
+    const R e2x = p[2].x - p[0].x, e2y = p[2].y - p[0].y, e2z = p[2].z - p[0].z;
+    const R cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+    const R J = sqrt(cx * cx + cy * cy + cz * cz);
+    if (n) *n = {cx / J, cy / J, cz / J};
+    return J;
+  };
+  R3<R> oa[3], ob[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    oa[c] = {(R)g.vertices[3 * si[c]], (R)g.vertices[3 * si[c] + 1], (R)g.vertices[3 * si[c] + 2]};
+    ob[c] = {(R)g.vertices[3 * sj[c]], (R)g.vertices[3 * sj[c] + 1], (R)g.vertices[3 * sj[c] + 2]};
+  }
+  R3<R> nj;
+  const R Ji = jac_normal(oa, nullptr);
+  const R Jj = jac_normal(ob, &nj);
+
+  SingularAcc<R, NCOMMON, DO_V, DO_K> acc;
+#pragma unroll
+  for (int e = 0; e < 18; e++) {
+    acc.v[e] = 0;
+    acc.kk[e] = 0;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc.a[c] = pa[c];
+    acc.b[c] = pb[c];
+  }
+  acc.nj = nj;
+  acc.k = (R)k;
+  const R jw = Ji * Jj / R(16);
+#pragma unroll 1
+  for (int pt = lane; pt < 256; pt += 32) {
+    const int i0 = pt >> 6, i1 = (pt >> 4) & 3, i2 = (pt >> 2) & 3, i3 = pt & 3;
+    const R xi = R(0.5) * (R(gl4_x(i0)) + R(1));
+    const R e1 = R(0.5) * (R(gl4_x(i1)) + R(1));
+    const R e2 = R(0.5) * (R(gl4_x(i2)) + R(1));
+    const R e3 = R(0.5) * (R(gl4_x(i3)) + R(1));
+    const R w0 = R(gl4_w(i0)) * R(gl4_w(i1)) * R(gl4_w(i2)) * R(gl4_w(i3)) * jw;
+    acc.point(xi, e1, e2, e3, w0);
+  }
+  // reduce; lane e (< 9) owns V entry e, lane 9 + e owns K entry e
+  float out_re = 0.f, out_im = 0.f;
+  int out_row = -1, out_col = -1;
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    R vr = DO_V ? warp_sum(acc.v[2 * e]) : R(0), vi = DO_V ? warp_sum(acc.v[2 * e + 1]) : R(0);
+    R kr = DO_K ? warp_sum(acc.kk[2 * e]) : R(0), ki = DO_K ? warp_sum(acc.kk[2 * e + 1]) : R(0);
+    const int ii = e / 3, jj = e % 3;
+    if (lane == e) {
+      out_re = (float)(vr * R(v_scale));
+      out_im = (float)(vi * R(v_scale));
+      out_row = si[pi[ii]];
+      out_col = sj[pj[jj]];
+    }
+    if (lane == 9 + e) {
+      out_re = (float)(kr * R(k_scale));
+      out_im = (float)(ki * R(k_scale));
+      out_row = si[pi[ii]];
+      out_col = sj[pj[jj]];
+    }
+  }
+  const size_t nv = (size_t)g.nv;
+  if (lane < 9 && DO_V) atomicAdd(&V[out_row * nv + out_col], make_float2(out_re, out_im));
+  if (lane >= 9 && lane < 18 && DO_K) {
+    float add_re = out_re;
+    if (NCOMMON == 3 && mass_coeff != 0.f) {
+      // P1 mass block of a coincident pair (integrand.h:257-278): area * sum_q w_q phi_a phi_b
+      const int e = lane - 9, a = pi[e / 3], b = pj[e % 3];
+      double m = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; q++) m += tri6_w(q) * tri6_phi(q, a) * tri6_phi(q, b);
+      add_re += (float)(mass_coeff * 0.5 * (double)Ji * m);
+    }
+    atomicAdd(&K[out_row * nv + out_col], make_float2(add_re, out_im));
+  }
+}
+
+// Dense P1 mass matrix, one thread per triangle (bind.cu:10-21).
+__global__ void mass_kernel(GeomView g, float2* __restrict__ M, float coeff) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nt) return;
+  const TriRec& r = g.rec_orig[i];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      double m = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; q++) m += tri6_w(q) * tri6_phi(q, a) * tri6_phi(q, b);
+      atomicAdd(&M[(size_t)r.v[a] * g.nv + r.v[b]], make_float2((float)(coeff * r.area * m), 0.f));
+    }
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+template <bool DO_V, bool DO_K>
+int launch_regular(const GeomView& g, float k, float2* V, float2* K, float v_scale, float k_scale, cudaStream_t s) {
+  const int smem = (int)sizeof(RegSmem<DO_V, DO_K>);
+  static bool attr_set = false;
+  if (!attr_set) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(regular_vk_kernel<DO_V, DO_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_set = true;
+  }
+  const int n_groups = (g.nt + kTestTris - 1) / kTestTris;
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_vk_kernel<DO_V, DO_K>, kRegThreads, smem));
+  const int grid = sm_count() * (occ > 0 ? occ : 1);
+  // chunk of trial tiles per work item: enough items to balance the grid
+  int chunk = (int)((long long)n_groups * g.ntiles / (8LL * grid));
+  chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
+  const int n_chunks = (g.ntiles + chunk - 1) / chunk;
+  const int n_items = n_groups * n_chunks;
+  regular_vk_kernel<DO_V, DO_K><<<grid < n_items ? grid : n_items, kRegThreads, smem, s>>>(
+      g, k, V, K, v_scale, k_scale, chunk, n_chunks, n_items);
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+template <bool DO_V, bool DO_K>
+int launch_singular(const GeomView& g, float k, float2* V, float2* K, float v_scale, float k_scale, float mass_coeff,
+                    cudaStream_t s) {
+  const int wpb = 4;  // warps per block
+  singular_vk_kernel<double, 3, DO_V, DO_K><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+      g, nullptr, g.nt, k, V, K, v_scale, k_scale, mass_coeff);
+  if (g.n_edge)
+    singular_vk_kernel<float, 2, DO_V, DO_K><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+        g, g.edge_pairs, g.n_edge, k, V, K, v_scale, k_scale, 0.f);
+  if (g.n_vert)
+    singular_vk_kernel<float, 1, DO_V, DO_K><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+        g, g.vert_pairs, g.n_vert, k, V, K, v_scale, k_scale, 0.f);
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+}  // namespace
+
+// V and/or (mass_coeff M + k_coeff K), both overwritten.
+int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_coeff, float k_coeff, cudaStream_t s) {
+  const size_t bytes = sizeof(float2) * (size_t)g.nv * g.nv;
+  if (V) BEM_CUDA_TRY(cudaMemsetAsync(V, 0, bytes, s));
+  if (Kout) BEM_CUDA_TRY(cudaMemsetAsync(Kout, 0, bytes, s));
+  const float v_scale = kInv4Pi;
+  const float k_scale = -kInv4Pi * k_coeff;  // K = -(...)/(4 pi)
+  int rc;
+  if (V && Kout) {
+    if ((rc = launch_regular<true, true>(g, k, V, Kout, v_scale, k_scale, s))) return rc;
+    return launch_singular<true, true>(g, k, V, Kout, v_scale, k_scale, mass_coeff, s);
+  } else if (V) {
+    if ((rc = launch_regular<true, false>(g, k, V, nullptr, v_scale, 0.f, s))) return rc;
+    return launch_singular<true, false>(g, k, V, nullptr, v_scale, 0.f, 0.f, s);
+  } else if (Kout) {
+    if ((rc = launch_regular<false, true>(g, k, nullptr, Kout, 0.f, k_scale, s))) return rc;
+    return launch_singular<false, true>(g, k, nullptr, Kout, 0.f, k_scale, mass_coeff, s);
+  }
+  return BEM_OK;
+}
+
+int assemble_mass(const GeomView& g, float2* M, float coeff, bool zero, cudaStream_t s) {
+  if (zero) BEM_CUDA_TRY(cudaMemsetAsync(M, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
+  mass_kernel<<<(g.nt + 127) / 128, 128, 0, s>>>(g, M, coeff);
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+}  // namespace bemb

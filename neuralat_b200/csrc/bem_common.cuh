@@ -1,0 +1,135 @@
+// Shared definitions for the B200 boundary-element kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/bem_b200.h"
+
+namespace bemb {
+
+// ---- quadrature ---------------------------------------------------------
+// Six-point degree-4 triangle rule (Dunavant), the rule the reference uses for
+// regular pairs, the mass matrix and listener potentials
+// (src/bem/cuda/include/gauss.h:106-126).  Points are given by barycentric
+// orbits (a, a, 1-2a); weights sum to one.  Point q has its dominant
+// barycentric weight at local vertex q % 3, which the kernels exploit.
+constexpr double kTriA1 = 0.44594849091596489;   // orbit 1: (1-2a1) on the dominant vertex
+constexpr double kTriA2 = 0.091576213509770743;  // orbit 2
+constexpr double kTriW1 = 0.22338158967801147;
+constexpr double kTriW2 = 0.10995174365532187;
+
+// barycentric coordinate of quadrature point q (0..5) at local vertex b (0..2)
+__host__ __device__ constexpr double tri6_phi(int q, int b) {
+  return (q < 3) ? ((q == b) ? 1.0 - 2.0 * kTriA1 : kTriA1) : ((q - 3 == b) ? 1.0 - 2.0 * kTriA2 : kTriA2);
+}
+__host__ __device__ constexpr double tri6_w(int q) { return q < 3 ? kTriW1 : kTriW2; }
+
+// Gauss-Legendre 4-point rule on [-1, 1] (gauss.h:44-54).
+constexpr double kGL4x0 = 0.86113631159405258, kGL4x1 = 0.33998104358485626;
+constexpr double kGL4w0 = 0.34785484513745385, kGL4w1 = 0.65214515486254614;
+__host__ __device__ constexpr double gl4_x(int i) {
+  return i == 0 ? kGL4x0 : i == 1 ? kGL4x1 : i == 2 ? -kGL4x1 : -kGL4x0;
+}
+__host__ __device__ constexpr double gl4_w(int i) { return (i == 0 || i == 3) ? kGL4w0 : kGL4w1; }
+
+constexpr float kEps = 1e-3f;  // r clamp of the reference kernels (potential.h:16-23)
+constexpr double kPi = 3.14159265358979323846;
+constexpr float kInv4Pi = (float)(1.0 / (4.0 * kPi));
+
+// ---- geometry -------------------------------------------------------------
+// One record per triangle, 32 words.  Quadrature points in rule order
+// (q = 0..5), unit normal, centroid, area = J/2, and the three vertex ids.
+struct __align__(16) TriRec {
+  float qp[18];
+  float n[3];
+  float c[3];
+  float area;
+  int v[3];
+  float h;  // n . v0 (plane offset)
+  float pad;
+};
+static_assert(sizeof(TriRec) == 128, "TriRec must be 128 bytes");
+
+constexpr int kTile = 16;               // triangles per geometry tile
+constexpr int kTileCorners = 3 * kTile;  // 48
+
+// Per-tile local-vertex tables, one per 16-triangle tile of the sorted order.
+struct __align__(16) TileRec {
+  int nlv;                       // number of distinct vertices in the tile
+  int ntri;                      // triangles in the tile (last tile may be short)
+  int pad0, pad1;
+  int vid[kTileCorners];         // global vertex id of each local vertex (ascending)
+  uint8_t corner_lv[kTileCorners];     // local vertex of corner (3*t + a)
+  uint8_t lv_ptr[kTileCorners + 4];    // CSR: corners of local vertex l are lv_corner[lv_ptr[l]..lv_ptr[l+1])
+  uint8_t lv_corner[kTileCorners];
+  uint8_t pad2[12];
+};
+static_assert(sizeof(TileRec) % 16 == 0, "TileRec alignment");
+
+// Header at the start of the geometry workspace.  All offsets in bytes from
+// the start of the workspace.
+struct GeomHeader {
+  uint32_t magic;
+  int nv, nt, ntiles;
+  int n_edge, n_vert;  // ordered singular pairs sharing 2 / 1 vertices
+  int max_valence;
+  int pad;
+  uint64_t off_vertices;   // float[nv*3] (copy of the input)
+  uint64_t off_triangles;  // int[nt*3] (copy of the input)
+  uint64_t off_perm;       // int[nt]  sorted position -> triangle id
+  uint64_t off_trirec;     // TriRec[nt] in sorted order
+  uint64_t off_trirec_orig;  // TriRec[nt] in input order
+  uint64_t off_tiles;      // TileRec[ntiles]
+  uint64_t off_edge_pairs;  // int2[n_edge]  (test tri, trial tri), input ids
+  uint64_t off_vert_pairs;  // int2[n_vert]
+  uint64_t off_normals;    // float[nt*3]
+  uint64_t off_curls;      // float[nt*9]   rows: n x grad(phi_b)
+  uint64_t bytes;
+};
+constexpr uint32_t kGeomMagic = 0x42454D32u;  // "BEM2"
+
+// Device-side view of a built geometry.
+struct GeomView {
+  int nv, nt, ntiles, n_edge, n_vert;
+  const float* vertices;
+  const int* triangles;
+  const int* perm;
+  const TriRec* rec;       // sorted order
+  const TriRec* rec_orig;  // input order
+  const TileRec* tiles;
+  const int2* edge_pairs;
+  const int2* vert_pairs;
+  const float* normals;
+  const float* curls;
+};
+
+// ---- small math -------------------------------------------------------------
+struct f3 {
+  float x, y, z;
+};
+__device__ __forceinline__ f3 make3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 sub(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct d3 {
+  double x, y, z;
+};
+__device__ __forceinline__ d3 sub(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ double dot3(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross3(d3 a, d3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+__device__ __forceinline__ void atomic_add_c64(float2* p, float re, float im) {
+  atomicAdd(p, make_float2(re, im));  // vector red.global.add.v2.f32 (sm_90+)
+}
+
+}  // namespace bemb
+
+// error-checking helper for host code inside the library
+#define BEM_CUDA_TRY(expr)                          \
+  do {                                              \
+    cudaError_t _e = (expr);                        \
+    if (_e != cudaSuccess) return BEM_ERR_CUDA;     \
+  } while (0)

@@ -1,0 +1,67 @@
+// extern "C" entry points for assembly, plus status strings.
+
+#include <cmath>
+
+#include "bem_common.cuh"
+
+namespace bemb {
+int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
+int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_coeff, float k_coeff, cudaStream_t s);
+int assemble_mass(const GeomView& g, float2* M, float coeff, bool zero, cudaStream_t s);
+int assemble_generic(const GeomView& g, int layer, int order, float k, const float* normals, const float* curls,
+                     float2* out, cudaStream_t s);
+}  // namespace bemb
+
+using namespace bemb;
+
+extern "C" const char* bem_status_string(int status) {
+  switch (status) {
+    case BEM_OK: return "ok";
+    case BEM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case BEM_ERR_INDEX: return "triangle vertex index out of range";
+    case BEM_ERR_DEGENERATE: return "degenerate mesh (zero-area, repeated-vertex or duplicated triangle)";
+    case BEM_ERR_WORKSPACE: return "workspace missing, too small or not a built geometry";
+    case BEM_ERR_NONFINITE: return "non-finite value";
+    case BEM_ERR_NOT_CONVERGED: return "iterative solver did not converge";
+    case BEM_ERR_BREAKDOWN: return "iterative solver breakdown";
+    case BEM_ERR_CUDA: return "CUDA error";
+    case BEM_ERR_UNSUPPORTED: return "unsupported request";
+  }
+  return "unknown status";
+}
+
+extern "C" const char* bem_version(void) { return "bemb200 0.1 sm_100a"; }
+
+extern "C" int bem_boundary_matrices_vk(const void* geom, float k, void* v_out, void* k_out, float mass_coeff,
+                                        float k_coeff, bem_stream_t stream) {
+  GeomView g;
+  int rc = geom_view(geom, &g, nullptr);
+  if (rc) return rc;
+  if (!std::isfinite(k)) return BEM_ERR_NONFINITE;
+  return assemble_vk(g, k, (float2*)v_out, (float2*)k_out, mass_coeff, k_coeff, (cudaStream_t)stream);
+}
+
+extern "C" int bem_boundary_matrix(const void* geom, int layer, int order, float k, const float* normals,
+                                   const float* curls, void* out, bem_stream_t stream) {
+  GeomView g;
+  int rc = geom_view(geom, &g, nullptr);
+  if (rc) return rc;
+  if (!out) return BEM_ERR_INVALID_ARGUMENT;
+  if (layer < BEM_SINGLE_LAYER || layer > BEM_BM_RHS || order < BEM_ORDER_EXACT || order > BEM_ORDER_APPROX_1)
+    return BEM_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(k)) return BEM_ERR_NONFINITE;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (order == BEM_ORDER_EXACT && layer == BEM_SINGLE_LAYER)
+    return assemble_vk(g, k, (float2*)out, nullptr, 0.f, 0.f, s);
+  if (order == BEM_ORDER_EXACT && layer == BEM_DOUBLE_LAYER)
+    return assemble_vk(g, k, nullptr, (float2*)out, 0.f, 1.f, s);
+  return assemble_generic(g, layer, order, k, normals, curls, (float2*)out, s);
+}
+
+extern "C" int bem_identity_matrix(const void* geom, void* out, bem_stream_t stream) {
+  GeomView g;
+  int rc = geom_view(geom, &g, nullptr);
+  if (rc) return rc;
+  if (!out) return BEM_ERR_INVALID_ARGUMENT;
+  return assemble_mass(g, (float2*)out, 1.f, true, (cudaStream_t)stream);
+}
