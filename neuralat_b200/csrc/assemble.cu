@@ -258,33 +258,41 @@ __device__ __forceinline__ void sincos_t<float>(float x, float* s, float* c) {
 
 // Re-ordering of the reference (integrand.h:351-387): for a common edge the
 // shared vertices take local slots 0,1 in trial order; for a common vertex it
-// is swapped into slot 0 on both triangles.
-__device__ __forceinline__ void reorder_pair(const int si[3], const int sj[3], int ncommon, int pi[3], int pj[3]) {
-  pi[0] = 0; pi[1] = 1; pi[2] = 2;
-  pj[0] = 0; pj[1] = 1; pj[2] = 2;
-  if (ncommon == 2) {
-    int idx = 0;
+// is swapped into slot 0 on both triangles.  Kept in scalar registers (no
+// runtime-indexed local arrays): p.i[c] / p.j[c] is the original local index
+// of re-ordered slot c.
+struct Perm {
+  int i0, i1, i2, j0, j1, j2;
+};
+
+__device__ __forceinline__ int pick3(int a0, int a1, int a2, int idx) { return idx == 0 ? a0 : (idx == 1 ? a1 : a2); }
+
+template <int NCOMMON>
+__device__ __forceinline__ Perm reorder_pair(int s0, int s1, int s2, int t0, int t1, int t2) {
+  Perm p{0, 1, 2, 0, 1, 2};
+  const int si[3] = {s0, s1, s2}, sj[3] = {t0, t1, t2};
+  if (NCOMMON == 2) {
+    int mi0 = 0, mj0 = 0, mi1 = 1, mj1 = 1, cnt = 0;
 #pragma unroll
     for (int jj = 0; jj < 3; jj++)
 #pragma unroll
-      for (int ii = 0; ii < 3; ii++)
-        if (si[ii] == sj[jj] && idx < 2) {
-          pi[idx] = ii;
-          pj[idx] = jj;
-          idx++;
-        }
-    pi[2] = 3 - pi[0] - pi[1];
-    pj[2] = 3 - pj[0] - pj[1];
-  } else if (ncommon == 1) {
+      for (int ii = 0; ii < 3; ii++) {
+        const bool eq = si[ii] == sj[jj];
+        if (eq && cnt == 0) { mi0 = ii; mj0 = jj; }
+        if (eq && cnt == 1) { mi1 = ii; mj1 = jj; }
+        cnt += eq ? 1 : 0;
+      }
+    p = Perm{mi0, mi1, 3 - mi0 - mi1, mj0, mj1, 3 - mj0 - mj1};
+  } else if (NCOMMON == 1) {
+    int ci = 0, cj = 0;
 #pragma unroll
     for (int ii = 0; ii < 3; ii++)
 #pragma unroll
       for (int jj = 0; jj < 3; jj++)
-        if (si[ii] == sj[jj]) {
-          if (ii != 0) { pi[0] = ii; pi[ii] = 0; }
-          if (jj != 0) { pj[0] = jj; pj[jj] = 0; }
-        }
+        if (si[ii] == sj[jj]) { ci = ii; cj = jj; }
+    p = Perm{ci, ci == 1 ? 0 : 1, ci == 2 ? 0 : 2, cj, cj == 1 ? 0 : 1, cj == 2 ? 0 : 2};
   }
+  return p;
 }
 
 template <typename R, int NCOMMON, bool DO_V, bool DO_K>
@@ -383,21 +391,18 @@ __global__ void __launch_bounds__(128)
   if (pair >= npairs) return;
   const int ti = NCOMMON == 3 ? pair : pairs[pair].x;
   const int tj = NCOMMON == 3 ? pair : pairs[pair].y;
-  int si[3], sj[3];
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    si[c] = g.triangles[3 * ti + c];
-    sj[c] = g.triangles[3 * tj + c];
-  }
-  int pi[3], pj[3];
-  reorder_pair(si, sj, NCOMMON, pi, pj);
+  const int s0 = g.triangles[3 * ti], s1 = g.triangles[3 * ti + 1], s2 = g.triangles[3 * ti + 2];
+  const int t0 = g.triangles[3 * tj], t1 = g.triangles[3 * tj + 1], t2 = g.triangles[3 * tj + 2];
+  const Perm pm = reorder_pair<NCOMMON>(s0, s1, s2, t0, t1, t2);
+  const int pi_[3] = {pm.i0, pm.i1, pm.i2}, pj_[3] = {pm.j0, pm.j1, pm.j2};
   R3<R> pa[3], pb[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const int va = si[pi[c]], vb = sj[pj[c]];
+    const int va = pick3(s0, s1, s2, pi_[c]), vb = pick3(t0, t1, t2, pj_[c]);
     pa[c] = {(R)g.vertices[3 * va], (R)g.vertices[3 * va + 1], (R)g.vertices[3 * va + 2]};
     pb[c] = {(R)g.vertices[3 * vb], (R)g.vertices[3 * vb + 1], (R)g.vertices[3 * vb + 2]};
   }
+  const int si[3] = {s0, s1, s2}, sj[3] = {t0, t1, t2};
   // Jacobians and the trial normal of the un-permuted triangles
   auto jac_normal = [](const R3<R>* p, R3<R>* n) {
     const R e1x = p[1].x - p[0].x, e1y = p[1].y - p[0].y, e1z = p[1].z - p[0].z;
@@ -452,14 +457,14 @@ __global__ void __launch_bounds__(128)
     if (lane == e) {
       out_re = (float)(vr * R(v_scale));
       out_im = (float)(vi * R(v_scale));
-      out_row = si[pi[ii]];
-      out_col = sj[pj[jj]];
+      out_row = pick3(s0, s1, s2, pi_[ii]);
+      out_col = pick3(t0, t1, t2, pj_[jj]);
     }
     if (lane == 9 + e) {
       out_re = (float)(kr * R(k_scale));
       out_im = (float)(ki * R(k_scale));
-      out_row = si[pi[ii]];
-      out_col = sj[pj[jj]];
+      out_row = pick3(s0, s1, s2, pi_[ii]);
+      out_col = pick3(t0, t1, t2, pj_[jj]);
     }
   }
   const size_t nv = (size_t)g.nv;
@@ -468,7 +473,7 @@ __global__ void __launch_bounds__(128)
     float add_re = out_re;
     if (NCOMMON == 3 && mass_coeff != 0.f) {
       // P1 mass block of a coincident pair (integrand.h:257-278): area * sum_q w_q phi_a phi_b
-      const int e = lane - 9, a = pi[e / 3], b = pj[e % 3];
+      const int e = lane - 9, a = pick3(pm.i0, pm.i1, pm.i2, e / 3), b = pick3(pm.j0, pm.j1, pm.j2, e % 3);
       double m = 0.0;
 #pragma unroll
       for (int q = 0; q < 6; q++) m += tri6_w(q) * tri6_phi(q, a) * tri6_phi(q, b);

@@ -8,7 +8,7 @@ boundary matrices, the identity, the two listener potential matrices and
 triangle2vertex, with the reference's own preprocess (solver.py:40-58) for
 the normals/curls it passes in.
 
-Usage:  python tests/golden/make_golden.py   (writes tests/golden/reference_*.npz)
+Usage:  python tests/golden/make_golden.py [out_dir]   (default: tests/golden/reference_*.npz)
 """
 from __future__ import annotations
 
@@ -53,7 +53,7 @@ def reference_preprocess(torch, vertices, triangles):
     return n.contiguous(), curls.contiguous()
 
 
-def main():
+def main(out_dir=HERE):
     import torch
 
     from oracle import build_ref
@@ -81,10 +81,10 @@ def main():
             out[f"k{ki}_single_potential"] = ref.single_boundary_potential(vt, tt, pts, float(k)).cpu().numpy()
             out[f"k{ki}_double_potential"] = ref.double_boundary_potential(vt, tt, pts, float(k)).cpu().numpy()
         torch.cuda.synchronize()
-        path = os.path.join(HERE, f"reference_{name}.npz")
+        path = os.path.join(out_dir, f"reference_{name}.npz")
         np.savez_compressed(path, **out)
         print("wrote", path, os.path.getsize(path), "bytes")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE)

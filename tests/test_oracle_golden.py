@@ -1,0 +1,66 @@
+"""The FP64 CPU oracle pinned against the reference's own src/bem kernels.
+
+tests/golden/reference_*.npz hold outputs of every binding of the reference
+extension (bind.cu:178-223), produced on a B200 by tests/golden/make_golden.py
+from the unmodified reference sources.  The reference computes in FP32 with
+atomics, so agreement is at FP32 rounding level (relative Frobenius).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FILES = sorted(glob.glob(os.path.join(HERE, "golden", "reference_*.npz")))
+LAYERS = ["single", "double", "adjointdouble", "hypersingular", "bm_lhs", "bm_rhs"]
+SUFFIXES = ["", "_approx", "_approx_1"]
+TOL = 2e-5
+
+
+def relfro(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module", params=FILES, ids=[os.path.basename(f) for f in FILES])
+def golden(request):
+    return dict(np.load(request.param))
+
+
+def test_fixtures_present():
+    assert len(FILES) >= 2
+
+
+@pytest.mark.parametrize("layer", LAYERS)
+@pytest.mark.parametrize("suffix", SUFFIXES)
+def test_boundary_matrices(golden, layer, suffix):
+    v, t = golden["vertices"], golden["triangles"]
+    for ki, k in enumerate(golden["ks"]):
+        ref = golden[f"k{ki}_{layer}{suffix}"]
+        assert relfro(O.boundary_matrix(layer, v, t, k, approx=suffix), ref) <= TOL, (layer, suffix, k)
+
+
+def test_identity_and_potentials(golden):
+    v, t = golden["vertices"], golden["triangles"]
+    assert relfro(O.identity_matrix(v, t), golden["identity"]) <= 1e-6
+    for ki, k in enumerate(golden["ks"]):
+        for lay in ("single", "double"):
+            ref = golden[f"k{ki}_{lay}_potential"]
+            assert relfro(O.potential_matrix(lay, v, t, golden["points"], k), ref) <= TOL
+
+
+def test_triangle2vertex(golden):
+    t = golden["triangles"]
+    out = O.triangle2vertex(golden["vertices"].shape[0], t, golden["t2v_in"])
+    assert relfro(out, golden["t2v_out"]) <= 1e-6
+
+
+def test_curls_match_reference_preprocess(golden):
+    """Surface curls used by hypersingular / Burton-Miller (solver.py:40-58)."""
+    v, t = golden["vertices"].astype(np.float64), golden["triangles"]
+    p0, p1, p2 = v[t[:, 0]], v[t[:, 1]], v[t[:, 2]]
+    n = np.cross(p1 - p0, p2 - p0)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    assert np.abs(n - golden["normals"]).max() < 1e-6
