@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Benchmark: BEM assemble + solve + evaluate, seconds per problem at 20k triangles.
+
+Workload (one "problem" = one step): icosphere subdivision 5 (N = 10 242 P1
+unknowns, T = 20 480 triangles), radius 0.15 m with axes scaled by seeded
+U[0.7, 1.3], k at 4 kHz, 8 smoothed complex Gaussian Neumann fields, 256
+listeners on a 0.5 m sphere.  A step builds the mesh geometry, assembles V
+and 0.5 I - K (fused), forms -V g, solves the exterior-Neumann CBIE for all 8
+right-hand sides to rtol 1e-6 (FP64 refinement) and evaluates the listener
+pressures.  Inputs are synthetic (seeded); the matrices (839 MB each) exceed
+the 126 MB L2, so no extra L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank solves its own replica ("replicas only":
+the path has no data exchange); times are the max over ranks.
+``--impl reference`` times the FP64 CPU restatement of the reference's
+algorithm (the reference has no CPU implementation of its own) on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "assemble+solve+eval s/problem @20k tris (icosphere s5, 8 RHS, 4 kHz, 256 listeners), 1 B200"
+WORKLOAD = ("icosphere s5 N=10242 T=20480, r=0.15 m axes*U[0.7,1.3] (seed 1), k=2pi*4000/343, "
+            "8 smoothed complex Gaussian Neumann RHS (seed 2), 256 listeners r=0.5 m (seed 0), CBIE rtol 1e-6")
+F_VK = 63.0  # FP32 flops per regular quadrature-point pair, fused V+K (algorithmic count)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3", "bf16"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison timing")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--validate", action="store_true", help="also compare against the FP64 oracle (minutes)")
+    ap.add_argument("--kernel-case", choices=["assemble", "solve", "eval"], default=None,
+                    help="profiling case: one stage on an icosphere of --subdiv, after one warm-up launch")
+    ap.add_argument("--subdiv", type=int, default=4)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+def workload():
+    from neuralat_b200.bem import meshes as M
+
+    w = M.precision_large(m=8)
+    return (w["vertices"].astype(np.float32), w["triangles"].astype(np.int32), float(w["k"]),
+            w["neumann"].astype(np.complex64), w["points"].astype(np.float32))
+
+
+def regular_pair_evals(triangles) -> float:
+    """36 x (ordered triangle pairs sharing no vertex)."""
+    t = np.asarray(triangles)
+    nt = t.shape[0]
+    nv = int(t.max()) + 1
+    star = [[] for _ in range(nv)]
+    for i, tri in enumerate(t):
+        for a in tri:
+            star[a].append(i)
+    touching = 0
+    for i, tri in enumerate(t):
+        touching += len(set(star[tri[0]]) | set(star[tri[1]]) | set(star[tri[2]]))
+    return 36.0 * (nt * nt - touching)
+
+
+def fp32_peak_tflops(sm_max_mhz=None):
+    import torch
+
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    mhz = sm_max_mhz or 1965.0
+    return props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(v, t, k, g, pts, budget_s=20.0):
+    """FP64 CPU restatement (oracle) timed on a bounded sample, extrapolated to
+    one full problem: assembly of sampled rows of V and K, a dense complex128
+    LU solve of a smaller system (scaled by n^3), listener evaluation for a
+    subset of listeners."""
+    from oracle import oracle as O
+
+    O.build()
+    nv, nt = v.shape[0], t.shape[0]
+    v64 = v.astype(np.float64)
+    rows = np.linspace(0, nv - 1, 48).astype(np.int32)
+    mask = np.zeros(nv, bool)
+    mask[rows] = True
+    frac_tris = float(np.any(mask[t], axis=1).sum()) / nt
+    t0 = time.perf_counter()
+    O.boundary_matrix("single", v64, t, k, rows=rows)
+    O.boundary_matrix("double", v64, t, k, rows=rows)
+    t_asm = (time.perf_counter() - t0) / frac_tris
+    ns = 2048
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((ns, ns)) + 1j * rng.standard_normal((ns, ns))
+    B = rng.standard_normal((ns, g.shape[1])) + 1j * rng.standard_normal((ns, g.shape[1]))
+    t0 = time.perf_counter()
+    np.linalg.solve(A, B)
+    t_solve = (time.perf_counter() - t0) * (nv / ns) ** 3
+    pp = pts[:8]
+    t0 = time.perf_counter()
+    O.potential_matrix("single", v64, t, pp, k)
+    O.potential_matrix("double", v64, t, pp, k)
+    t_eval = (time.perf_counter() - t0) * pts.shape[0] / pp.shape[0]
+    total = t_asm + t_solve + t_eval
+    return {
+        "value": total, "unit": "s/problem", "cores": int(O.num_threads()), "kind": "port",
+        "sample": (f"FP64 oracle: V+K rows of {rows.size} vertices ({frac_tris:.4f} of test triangles) "
+                   f"extrapolated; complex128 LU {ns}x{ns} x{g.shape[1]} RHS scaled by (N/{ns})^3; "
+                   f"{pp.shape[0]} of {pts.shape[0]} listeners scaled"),
+        "stages_s": {"assemble": t_asm, "solve": t_solve, "eval": t_eval},
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    v, t, k, g, pts = workload()
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(v, t, k, g, pts)
+    cb = None
+    for _ in range(args.steps):
+        cb = cpu_baseline(v, t, k, g, pts)
+        vals.append(cb["value"])
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s/problem", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "s/problem", "cores": cb["cores"], "kind": cb["kind"],
+                         "sample": cb["sample"]},
+        "e2e": {"value": value, "unit": "s/problem", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from neuralat_b200 import _lib as L
+    from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
+    from neuralat_b200.bem.solver import _stream, _vp
+
+    lib = L.lib()
+    v, t, k, g, pts = workload()
+    dev = torch.device("cuda", local)
+    v_d = torch.from_numpy(v).to(dev)
+    t_d = torch.from_numpy(t).to(dev)
+    g_d = torch.from_numpy(g).to(dev)
+    p_d = torch.from_numpy(pts).to(dev)
+    n_eval = regular_pair_evals(t)
+    stream = torch.cuda.current_stream(dev)
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    stage_names = ["geometry", "assemble", "rhs", "solve", "eval"]
+
+    def step(record=None, info=None):
+        e0 = ev()
+        s = BEM_Solver(v_d, t_d)
+        e1 = ev()
+        V, A = s.assemble_vk(k)
+        e2 = ev()
+        rhs = -cmatmul(V, g_d)
+        del V
+        e3 = ev()
+        u = gmres(A, rhs, rtol=1e-6, precision=args.precision, info=info)
+        e4 = ev()
+        p = s.boundary2potential(k, g_d, u, p_d)
+        e5 = ev()
+        if record is not None:
+            record.append((e0, e1, e2, e3, e4, e5))
+        return u, p
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    # ---- warm-up --------------------------------------------------------------
+    info = {}
+    for _ in range(max(args.warmup, 0)):
+        step(info=info)
+    barrier()
+
+    # ---- timed region (device-resident inputs) --------------------------------
+    rec = []
+    infos = []
+    with ClockSampler(local) as clk:
+        barrier()
+        l0 = lib.bem_kernel_launches()
+        t_start = ev()
+        for _ in range(args.steps):
+            inf = {}
+            step(rec, inf)
+            infos.append(inf)
+        t_end = ev()
+        barrier()
+        l1 = lib.bem_kernel_launches()
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end))
+    ms_per_step = total_ms / args.steps
+    value = (ms_per_step / 1e3) / world  # whole-job s/problem: world replicas in parallel
+    stages = {n: float(np.mean([r[i].elapsed_time(r[i + 1]) for r in rec])) for i, n in enumerate(stage_names)}
+    asm_ms = stages["assemble"]
+
+    # ---- end to end through the public API from host buffers -------------------
+    v_h = torch.from_numpy(v).pin_memory()
+    t_h = torch.from_numpy(t).pin_memory()
+    g_h = torch.from_numpy(g).pin_memory()
+    p_h = torch.from_numpy(pts).pin_memory()
+    h2d = sum(x.numel() * x.element_size() for x in (v_h, t_h, g_h, p_h))
+    d2h = pts.shape[0] * g.shape[1] * 8
+    barrier()
+    e_s = ev()
+    for _ in range(args.steps):
+        vd = v_h.to(dev, non_blocking=True)
+        td = t_h.to(dev, non_blocking=True)
+        gd = g_h.to(dev, non_blocking=True)
+        pd = p_h.to(dev, non_blocking=True)
+        s = BEM_Solver(vd, td)
+        _, p = s.solve_and_evaluate(k, gd, pd, precision=args.precision, rtol=1e-6)
+        p.cpu()
+    e_e = ev()
+    barrier()
+    e2e_ms = max_over_ranks(e_s.elapsed_time(e_e)) / args.steps
+
+    # ---- plain FP32 form (reference-shaped pipeline on our kernels) ------------
+    plain = None
+    if not args.no_plain and rank == 0:
+        def plain_step():
+            s = BEM_Solver(v_d, t_d)
+            I = s.identity_matrix()
+            V = s.assemble_boundary_matrix(k, "single")
+            K = s.assemble_boundary_matrix(k, "double")
+            A = (0.5 * I - K).contiguous()
+            del I, K
+            rhs = -cmatmul(V, g_d)
+            del V
+            us = [gmres(A, rhs[:, j].contiguous(), rtol=1e-6, precision="fp32") for j in range(rhs.shape[1])]
+            u = torch.stack(us, dim=1)
+            del A
+            S = s.potential_matrix(k, p_d, "single")
+            D = s.potential_matrix(k, p_d, "double")
+            return -cmatmul(S, g_d) + cmatmul(D, u)
+
+        plain_step()
+        torch.cuda.synchronize()
+        ps = ev()
+        nplain = 2
+        for _ in range(nplain):
+            plain_step()
+        pe = ev()
+        torch.cuda.synchronize()
+        plain = {"s_per_problem": ps.elapsed_time(pe) / nplain / 1e3, "steps": nplain,
+                 "form": "separate V, K, M assembly; explicit 0.5M-K; one FP32 single-RHS GMRES per RHS; "
+                         "explicit S, D potential matrices"}
+
+    # ---- roofline of the dominant kernel (fused regular V+K assembly) ----------
+    clocks = clk.summary()
+    peak = fp32_peak_tflops(clocks.get("sm_max_mhz"))
+    achieved = F_VK * n_eval / (asm_ms / 1e3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None,
+                "kernel": "bem_boundary_matrices_vk (regular_vk_kernel + singular + memset), 63 flop x "
+                          f"{n_eval:.4e} regular quadrature-point pairs per launch; peak = nominal FP32 "
+                          "(SMs x 128 FMA x 2 x max SM clock), no measured FP32 peak available"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(v, t, k, g, pts)
+        cpu = {kk: cb[kk] for kk in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        it = infos[-1] if infos else {}
+        line = {
+            "metric": METRIC, "value": value, "unit": "s/problem", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"f32 assembly + {args.precision} matvec + f64 refinement",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (two 839 MB matrices per step)"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_ms / 1e3 / world, "unit": "s/problem", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(l1 - l0),
+            "clocks": clocks,
+            "stages_ms": stages,
+            "solver": {kk: it.get(kk) for kk in ("iterations", "refinements", "matvecs", "rel_residual", "status")},
+            "plain_fp32": plain,
+            "speedup_vs_plain_fp32": (plain["s_per_problem"] / (ms_per_step / 1e3)) if plain else None,
+        }
+        if args.validate:
+            line["validation"] = validate(v, t, k, g, pts, dev, args.precision)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def validate(v, t, k, g, pts, dev, precision):
+    """Listener-pressure error of the GPU path against the FP64 oracle (minutes)."""
+    import torch
+
+    from neuralat_b200.bem import BEM_Solver
+    from oracle import oracle as O
+
+    s = BEM_Solver(torch.from_numpy(v).to(dev), torch.from_numpy(t).to(dev))
+    _, p = s.solve_and_evaluate(k, torch.from_numpy(g).to(dev), torch.from_numpy(pts).to(dev), precision=precision,
+                                rtol=1e-6)
+    p = p.cpu().numpy()
+    u_ref = O.cbie_solve(v, t, k, g)
+    p_ref = O.boundary2potential(v, t, k, g, u_ref, pts)
+    err = np.linalg.norm(p - p_ref, axis=0) / np.linalg.norm(p_ref, axis=0)
+    return {"listener_rel_err_per_rhs": err.tolist(), "max": float(err.max())}
+
+
+def run_kernel_case(args):
+    """One stage of the path on a smaller mesh (for ncu captures): warm-up once, then run once."""
+    import torch
+
+    from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
+    from neuralat_b200.bem import meshes as M
+
+    v, t = M.icosphere(args.subdiv, 0.15)
+    v = (v * np.random.default_rng(1).uniform(0.7, 1.3, size=3)).astype(np.float32)
+    k = M.wavenumber(4000.0)
+    g = torch.from_numpy(M.smoothed_gaussian_field(v.shape[0], t, 8, seed=2).astype(np.complex64)).cuda()
+    pts = torch.from_numpy(M.sphere_points(256, 0.5, seed=0).astype(np.float32)).cuda()
+    s = BEM_Solver(v, t)
+    V, A = s.assemble_vk(k)
+    rhs = -cmatmul(V, g)
+    for _ in range(2):
+        if args.kernel_case == "assemble":
+            s.assemble_vk(k)
+        elif args.kernel_case == "solve":
+            gmres(A, rhs, rtol=1e-6, precision=args.precision)
+        else:
+            s.boundary2potential(k, g, rhs, pts)
+    torch.cuda.synchronize()
+    print(f"kernel case {args.kernel_case} subdiv {args.subdiv} N={v.shape[0]} T={t.shape[0]} ok")
+
+
+def main():
+    args = parse()
+    if args.kernel_case:
+        run_kernel_case(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

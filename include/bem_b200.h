@@ -73,6 +73,9 @@ enum {
 const char* bem_status_string(int status);
 /* Library version string (static). */
 const char* bem_version(void);
+/* Number of kernels this library has launched in this process (host-side
+ * counter, incremented at every launch site). */
+unsigned long long bem_kernel_launches(void);
 
 /* ------------------------------------------------------------------------
  * Geometry.  Replaces the per-call mesh handling of bind.cu:49-66 and the

@@ -31,7 +31,7 @@ PREC_FP32, PREC_BF16X3, PREC_BF16 = range(3)
 
 # every symbol include/bem_b200.h declares
 EXPORTED = (
-    "bem_status_string", "bem_version",
+    "bem_status_string", "bem_version", "bem_kernel_launches",
     "bem_geometry_bytes", "bem_geometry_build", "bem_geometry_normals",
     "bem_boundary_matrix", "bem_boundary_matrices_vk", "bem_identity_matrix", "bem_triangle2vertex",
     "bem_potential_matrix", "bem_boundary2potential_scratch_bytes", "bem_boundary2potential",
@@ -91,6 +91,7 @@ def lib():
     sigs = {
         "bem_status_string": ([i], ctypes.c_char_p),
         "bem_version": ([], ctypes.c_char_p),
+        "bem_kernel_launches": ([], ctypes.c_ulonglong),
         "bem_geometry_bytes": ([vp, i, vp, i, P(sz), vp], i),
         "bem_geometry_build": ([vp, i, vp, i, vp, sz, vp], i),
         "bem_geometry_normals": ([vp, vp, vp, vp], i),

@@ -527,8 +527,8 @@ int launch_regular(const GeomView& g, float k, float2* V, float2* K, float v_sca
   chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
   const int n_chunks = (g.ntiles + chunk - 1) / chunk;
   const int n_items = n_groups * n_chunks;
-  regular_vk_kernel<DO_V, DO_K><<<grid < n_items ? grid : n_items, kRegThreads, smem, s>>>(
-      g, k, V, K, v_scale, k_scale, chunk, n_chunks, n_items);
+  (regular_vk_kernel<DO_V, DO_K><<<grid < n_items ? grid : n_items, kRegThreads, smem, s>>>(
+      g, k, V, K, v_scale, k_scale, chunk, n_chunks, n_items), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
@@ -537,14 +537,14 @@ template <bool DO_V, bool DO_K>
 int launch_singular(const GeomView& g, float k, float2* V, float2* K, float v_scale, float k_scale, float mass_coeff,
                     cudaStream_t s) {
   const int wpb = 4;  // warps per block
-  singular_vk_kernel<double, 3, DO_V, DO_K><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
-      g, nullptr, g.nt, k, V, K, v_scale, k_scale, mass_coeff);
+  (singular_vk_kernel<double, 3, DO_V, DO_K><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+      g, nullptr, g.nt, k, V, K, v_scale, k_scale, mass_coeff), count_launch());
   if (g.n_edge)
-    singular_vk_kernel<float, 2, DO_V, DO_K><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
-        g, g.edge_pairs, g.n_edge, k, V, K, v_scale, k_scale, 0.f);
+    (singular_vk_kernel<float, 2, DO_V, DO_K><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+        g, g.edge_pairs, g.n_edge, k, V, K, v_scale, k_scale, 0.f), count_launch());
   if (g.n_vert)
-    singular_vk_kernel<float, 1, DO_V, DO_K><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
-        g, g.vert_pairs, g.n_vert, k, V, K, v_scale, k_scale, 0.f);
+    (singular_vk_kernel<float, 1, DO_V, DO_K><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(
+        g, g.vert_pairs, g.n_vert, k, V, K, v_scale, k_scale, 0.f), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
@@ -574,7 +574,7 @@ int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_
 
 int assemble_mass(const GeomView& g, float2* M, float coeff, bool zero, cudaStream_t s) {
   if (zero) BEM_CUDA_TRY(cudaMemsetAsync(M, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
-  mass_kernel<<<(g.nt + 127) / 128, 128, 0, s>>>(g, M, coeff);
+  (mass_kernel<<<(g.nt + 127) / 128, 128, 0, s>>>(g, M, coeff), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }

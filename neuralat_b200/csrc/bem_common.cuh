@@ -127,6 +127,11 @@ __device__ __forceinline__ void atomic_add_c64(float2* p, float re, float im) {
 
 }  // namespace bemb
 
+namespace bemb {
+// process-wide count of kernel launches issued by this library (host side)
+void count_launch();
+}  // namespace bemb
+
 // error-checking helper for host code inside the library
 #define BEM_CUDA_TRY(expr)                          \
   do {                                              \

@@ -1,5 +1,6 @@
 // extern "C" entry points for assembly, plus status strings.
 
+#include <atomic>
 #include <cmath>
 
 #include "bem_common.cuh"
@@ -12,7 +13,14 @@ int assemble_generic(const GeomView& g, int layer, int order, float k, const flo
                      float2* out, cudaStream_t s);
 }  // namespace bemb
 
+namespace bemb {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace bemb
+
 using namespace bemb;
+
+extern "C" unsigned long long bem_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 extern "C" const char* bem_status_string(int status) {
   switch (status) {

@@ -336,10 +336,10 @@ extern "C" int bem_geometry_build(const float* vertices, int nv, const int* tria
   if (h.n_vert) std::memcpy(stage.data() + h.off_vert_pairs, g.vert_pairs.data(), sizeof(int2) * h.n_vert);
   BEM_CUDA_TRY(cudaMemcpyAsync(geom, stage.data(), stage.size(), cudaMemcpyHostToDevice, s));
   char* b = (char*)geom;
-  geom_records_kernel<<<(nt + 127) / 128, 128, 0, s>>>(
+  (geom_records_kernel<<<(nt + 127) / 128, 128, 0, s>>>(
       nt, (const float*)(b + h.off_vertices), (const int*)(b + h.off_triangles), (const int*)(b + h.off_perm),
       (TriRec*)(b + h.off_trirec), (TriRec*)(b + h.off_trirec_orig), (float*)(b + h.off_normals),
-      (float*)(b + h.off_curls));
+      (float*)(b + h.off_curls)), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   BEM_CUDA_TRY(cudaStreamSynchronize(s));  // staging buffer is pageable host memory
   cache_put(geom, h);

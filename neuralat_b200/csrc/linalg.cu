@@ -148,14 +148,14 @@ int launch_cmatmul(const float2* A, int n, const typename C2<T>::type* X, int ld
                    int ldy, const float2* B, int ldb, double* norm2, const int* skip, cudaStream_t s) {
   const int rb = (n + kMMRows - 1) / kMMRows;
   if (m == 1) {
-    cmatmul_kernel<T, 1, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip);
+    (cmatmul_kernel<T, 1, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
   } else if (m == 2) {
-    cmatmul_kernel<T, 2, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip);
+    (cmatmul_kernel<T, 2, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
   } else if (m <= 4) {
-    cmatmul_kernel<T, 4, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip);
+    (cmatmul_kernel<T, 4, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
   } else {
-    cmatmul_kernel<T, 8, MODE><<<dim3(rb, (m + 7) / 8), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2,
-                                                                          skip);
+    (cmatmul_kernel<T, 8, MODE><<<dim3(rb, (m + 7) / 8), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2,
+                                                                          skip), count_launch());
   }
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
@@ -684,8 +684,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
 
   BEM_CUDA_TRY(cudaMemsetAsync(P.bnorm2, 0, sizeof(double) * m, s));
   BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
-  gm_bnorm_kernel<<<gv, 256, 0, s>>>(P, (const float2*)B);
-  gm_init_x_kernel<<<gv, 256, 0, s>>>(P, (const float2*)X, use_x0);
+  (gm_bnorm_kernel<<<gv, 256, 0, s>>>(P, (const float2*)B), count_launch());
+  (gm_init_x_kernel<<<gv, 256, 0, s>>>(P, (const float2*)X, use_x0), count_launch());
   BEM_CUDA_TRY(cudaMemcpyAsync(hb.data(), P.bnorm2, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
 
   int total_iters = 0, matvecs = 0, refinements = 0;
@@ -700,7 +700,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       if (rc) return rc;
       matvecs++;
     } else {
-      gm_copy_b_kernel<<<gv, 256, 0, s>>>(P, (const float2*)B, rnorm2);
+      (gm_copy_b_kernel<<<gv, 256, 0, s>>>(P, (const float2*)B, rnorm2), count_launch());
     }
     BEM_CUDA_TRY(cudaMemcpyAsync(hres.data(), rnorm2, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
     BEM_CUDA_TRY(cudaStreamSynchronize(s));
@@ -732,28 +732,28 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     while (total_iters < params->max_iters) {
       BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
       if (!first_cycle) {
-        gm_pack_d_kernel<<<gv, 256, 0, s>>>(P);
+        (gm_pack_d_kernel<<<gv, 256, 0, s>>>(P), count_launch());
         BEM_CUDA_TRY(cudaMemsetAsync(&P.st->skip, 0, sizeof(int), s));
         if ((rc = inner_matvec())) return rc;
         matvecs++;
       }
-      gm_start_vec_kernel<<<gv, 256, 0, s>>>(P, first_cycle ? 0 : 1);
+      (gm_start_vec_kernel<<<gv, 256, 0, s>>>(P, first_cycle ? 0 : 1), count_launch());
       // absolute inner target: inner_rtol * ||r_out|| but never below rtol * ||b|| / 2
-      gm_start_scalar_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P, rnorm2, inner_rtol, 0.5 * params->rtol);
-      gm_start_norm_kernel<<<gv, 256, 0, s>>>(P);
+      (gm_start_scalar_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P, rnorm2, inner_rtol, 0.5 * params->rtol), count_launch());
+      (gm_start_norm_kernel<<<gv, 256, 0, s>>>(P), count_launch());
       first_cycle = false;
       int it = 0;
       bool cycle_done = false;
       hflag->k = -1;  // no in-cycle snapshot yet (no copy is in flight here)
       hflag->any_active = 1;
       while (it < R && total_iters < params->max_iters) {
-        gm_pack_kernel<<<gv, 256, 0, s>>>(P);
+        (gm_pack_kernel<<<gv, 256, 0, s>>>(P), count_launch());
         if ((rc = inner_matvec())) return rc;
-        gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 0);
-        gm_update_kernel<<<gv, 256, 0, s>>>(P, 0);
-        gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 1);
-        gm_update_kernel<<<gv, 256, 0, s>>>(P, 1);
-        gm_finalize_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P);
+        (gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 0), count_launch());
+        (gm_update_kernel<<<gv, 256, 0, s>>>(P, 0), count_launch());
+        (gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 1), count_launch());
+        (gm_update_kernel<<<gv, 256, 0, s>>>(P, 1), count_launch());
+        (gm_finalize_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P), count_launch());
         BEM_CUDA_TRY(cudaGetLastError());
         it++;
         total_iters++;
@@ -765,8 +765,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
         BEM_CUDA_TRY(cudaEventRecord(ev, s));
         if (cycle_done) break;
       }
-      gm_solve_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P);
-      gm_xupdate_kernel<<<gv, 256, 0, s>>>(P);
+      (gm_solve_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P), count_launch());
+      (gm_xupdate_kernel<<<gv, 256, 0, s>>>(P), count_launch());
       BEM_CUDA_TRY(cudaEventSynchronize(ev));
       // converged when no column is active at the end of the cycle with
       // resid <= tol (columns that stopped at the restart length restart)
@@ -779,10 +779,10 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
         if (hres[c] > htol[c]) all = false;
       if (all) break;
     }
-    gm_accept_kernel<<<gv, 256, 0, s>>>(P);
+    (gm_accept_kernel<<<gv, 256, 0, s>>>(P), count_launch());
     x_nonzero = true;
   }
-  gm_store_x_kernel<<<gv, 256, 0, s>>>(P, (float2*)X);
+  (gm_store_x_kernel<<<gv, 256, 0, s>>>(P, (float2*)X), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   BEM_CUDA_TRY(cudaStreamSynchronize(s));
   if (info) {

@@ -192,9 +192,9 @@ extern "C" int bem_potential_matrix(const void* geom, int layer, const float* po
   BEM_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)np * g.nv, s));
   dim3 grid((g.nt + 127) / 128, np);
   if (layer == BEM_SINGLE_LAYER)
-    potential_matrix_kernel<BEM_SINGLE_LAYER><<<grid, 128, 0, s>>>(g, points, np, k, (float2*)out);
+    (potential_matrix_kernel<BEM_SINGLE_LAYER><<<grid, 128, 0, s>>>(g, points, np, k, (float2*)out), count_launch());
   else
-    potential_matrix_kernel<BEM_DOUBLE_LAYER><<<grid, 128, 0, s>>>(g, points, np, k, (float2*)out);
+    (potential_matrix_kernel<BEM_DOUBLE_LAYER><<<grid, 128, 0, s>>>(g, points, np, k, (float2*)out), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
@@ -217,8 +217,8 @@ extern "C" int bem_boundary2potential(const void* geom, const float* points, int
   float2* dn = (float2*)scratch;
   float2* dd = dn + (size_t)g.nt * 6 * nrhs;
   const long long total = (long long)g.nt * 6 * nrhs;
-  b2p_density_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, (const float2*)neumann,
-                                                                      (const float2*)dirichlet, nrhs, dn, dd);
+  (b2p_density_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, (const float2*)neumann,
+                                                                      (const float2*)dirichlet, nrhs, dn, dd), count_launch());
   BEM_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)np * nrhs, s));
   const int nq = 6 * g.nt;
   const int ptiles = (np + 31) / 32;
@@ -231,8 +231,8 @@ extern "C" int bem_boundary2potential(const void* geom, const float* points, int
   chunk = chunk < 256 ? 256 : chunk;
   nchunks = (nq + chunk - 1) / chunk;
   for (int r0 = 0; r0 < nrhs; r0 += kB2PRhs) {
-    b2p_eval_kernel<<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, r0, chunk,
-                                                                   (float2*)out);
+    (b2p_eval_kernel<<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, r0, chunk,
+                                                                   (float2*)out), count_launch());
   }
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
@@ -247,8 +247,8 @@ extern "C" int bem_triangle2vertex(const void* geom, const void* tri_values, voi
   cudaStream_t s = (cudaStream_t)stream;
   BEM_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)g.nv, s));
   BEM_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)g.nv, s));
-  t2v_scatter_kernel<<<(g.nt + 255) / 256, 256, 0, s>>>(g, (const float2*)tri_values, (float2*)out, counts);
-  t2v_divide_kernel<<<(g.nv + 255) / 256, 256, 0, s>>>(g.nv, (float2*)out, counts);
+  (t2v_scatter_kernel<<<(g.nt + 255) / 256, 256, 0, s>>>(g, (const float2*)tri_values, (float2*)out, counts), count_launch());
+  (t2v_divide_kernel<<<(g.nv + 255) / 256, 256, 0, s>>>(g.nv, (float2*)out, counts), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }

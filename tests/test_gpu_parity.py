@@ -174,18 +174,23 @@ def test_monopole_known_answer(solvers):
 
 
 def test_solve_linear_equation_bicgstab_and_gmres(solvers):
+    """Default stopping test as the reference: ||r||^2 < tol ||b||^2 (tol 1e-10)."""
     s = solvers["s2_ellipsoid"]
     k = 30.0
     v, t = _mesh("s2_ellipsoid")
     g = torch.from_numpy(M.smoothed_gaussian_field(v.shape[0], t, 1, seed=9)[:, 0].astype(np.complex64)).cuda()
     V, lhs = s.assemble_vk(k)
     rhs = -cmatmul(V, g)
-    x_g = solve_linear_equation(lhs, rhs)
-    x_b = solve_linear_equation(lhs, rhs, solver="bicgstab")
-    x_c = solve_linear_equation(lambda x: cmatmul(lhs, x), rhs)
-    ref = np.linalg.solve(lhs.cpu().numpy().astype(np.complex128), rhs.cpu().numpy().astype(np.complex128))
-    for x in (x_g, x_b, x_c):
-        assert relfro(x.cpu().numpy(), ref) <= 5e-5
+    A = lhs.cpu().numpy().astype(np.complex128)
+    b = rhs.cpu().numpy().astype(np.complex128)
+    ref = np.linalg.solve(A, b)
+    for kw in ({}, {"solver": "bicgstab"}):
+        x = solve_linear_equation(lhs, rhs, **kw).cpu().numpy()
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.5e-5
+    x_c = solve_linear_equation(lambda x: cmatmul(lhs, x), rhs).cpu().numpy()
+    assert np.linalg.norm(b - A @ x_c) / np.linalg.norm(b) <= 1.5e-5
+    x_t = solve_linear_equation(lhs, rhs, tol=1e-14).cpu().numpy()
+    assert relfro(x_t, ref) <= 1e-5
 
 
 def test_triangle2vertex():
