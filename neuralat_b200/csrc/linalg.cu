@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(kMMThreads)
                    double* __restrict__ norm2, const int* __restrict__ skip) {
   typedef typename C2<T>::type CT;
   if (skip && *skip) return;
-  __shared__ CT xs[kMMColTile][MR];
+  __shared__ CT xs[MR][kMMColTile];  // [rhs][column]: lanes read consecutive columns
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int row0 = blockIdx.x * kMMRows + warp * kMMRowsPerWarp;
   const int s0 = blockIdx.y * MR;
@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kMMThreads)
       v.x = T(0);
       v.y = T(0);
       if (c0 + c < n && s < ms) v = X[(size_t)(c0 + c) * ldx + s0 + s];
-      xs[c][s] = v;
+      xs[s][c] = v;
     }
     __syncthreads();
 #pragma unroll
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kMMThreads)
       }
 #pragma unroll
       for (int s = 0; s < MR; s++) {
-        const CT x = xs[c][s];
+        const CT x = xs[s][c];
 #pragma unroll
         for (int r = 0; r < kMMRowsPerWarp; r++) {
           const T ar = (T)a[r].x, ai = (T)a[r].y;
@@ -169,11 +169,14 @@ struct GmState {
   int any_active;  // 0 when every column has converged (matvec early-out)
   int skip;        // == !any_active, read by the matvec kernel
   int pad;
+  int any_count;   // scratch counters of gm_finalize_kernel (zero between launches)
+  int done_blocks;
+  int pad2[2];
 };
 
 struct GmPtrs {
   int n, m, R;
-  double2* Vb;     // [m][R+1][n]
+  float2* Vb;      // [m][R+1][n]  Krylov basis, complex64 storage
   double2* H;      // [m][R][R+1]  column k, rows 0..k+1
   double* cs;      // [m][R]
   double2* sn;     // [m][R]
@@ -203,18 +206,18 @@ __global__ void gm_pack_kernel(GmPtrs P) {
   const int s = blockIdx.y;
   if (i >= P.n) return;
   const int k = P.st->k;
-  double2* vk = P.Vb + ((size_t)s * (P.R + 1) + k) * P.n;
+  float2* vk = P.Vb + ((size_t)s * (P.R + 1) + k) * P.n;
   if (P.active[s]) {
-    double2 v;
+    float2 v;
     if (k > 0) {
       const double inv = P.winv[s];
       const double2 ww = P.w[(size_t)s * P.n + i];
-      v = make_double2(ww.x * inv, ww.y * inv);
+      v = make_float2((float)(ww.x * inv), (float)(ww.y * inv));
       vk[i] = v;
     } else {
       v = vk[i];
     }
-    P.X[(size_t)i * P.m + s] = make_float2((float)v.x, (float)v.y);
+    P.X[(size_t)i * P.m + s] = v;
   } else {
     P.X[(size_t)i * P.m + s] = make_float2(0.f, 0.f);
   }
@@ -225,7 +228,7 @@ __global__ void gm_dots_kernel(GmPtrs P, int pass) {
   const int l = blockIdx.x, s = blockIdx.y;
   const int k = P.st->k;
   if (l > k || !P.active[s]) return;
-  const double2* v = P.Vb + ((size_t)s * (P.R + 1) + l) * P.n;
+  const float2* v = P.Vb + ((size_t)s * (P.R + 1) + l) * P.n;
   double re = 0.0, im = 0.0;
   for (int i = threadIdx.x; i < P.n; i += blockDim.x) {
     double2 src;
@@ -235,7 +238,8 @@ __global__ void gm_dots_kernel(GmPtrs P, int pass) {
     } else {
       src = P.w[(size_t)s * P.n + i];
     }
-    const double2 t = cmulc(v[i], src);
+    const float2 vv = v[i];
+    const double2 t = cmulc(make_double2(vv.x, vv.y), src);
     re += t.x;
     im += t.y;
   }
@@ -279,9 +283,10 @@ __global__ void gm_update_kernel(GmPtrs P, int pass) {
     } else {
       acc = P.w[(size_t)s * P.n + i];
     }
-    const double2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
+    const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
     for (int l = 0; l <= k; l++) {
-      const double2 t = cmul(v[(size_t)l * P.n], hs[l]);
+      const float2 vv = v[(size_t)l * P.n];
+      const double2 t = cmul(make_double2(vv.x, vv.y), hs[l]);
       acc.x -= t.x;
       acc.y -= t.y;
     }
@@ -295,77 +300,100 @@ __global__ void gm_update_kernel(GmPtrs P, int pass) {
   }
 }
 
-// Hessenberg column, Givens rotations, residual estimate, convergence; one
-// thread per column; thread 0 then advances k.
-__global__ void gm_finalize_kernel(GmPtrs P) {
-  const int s = threadIdx.x;
+// Hessenberg column, Givens rotations, residual estimate, convergence.  One
+// warp per column: the lanes stage the new column and the previous rotations
+// in shared memory, lane 0 applies the rotations (inherently sequential); the
+// last block to finish advances k.  One block per kFinWarps columns.
+constexpr int kFinWarps = 4;  // 40 KB of static shared memory
+constexpr int kMaxRestart = 256;
+__global__ void __launch_bounds__(32 * kFinWarps) gm_finalize_kernel(GmPtrs P, int* __restrict__ any_count,
+                                                                     int* __restrict__ done_blocks) {
+  __shared__ double2 hcol[kFinWarps][kMaxRestart + 1];
+  __shared__ double csv[kFinWarps][kMaxRestart];
+  __shared__ double2 snv[kFinWarps][kMaxRestart];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int s = blockIdx.x * kFinWarps + wl;
   const int k = P.st->k;
-  __shared__ int any;
-  if (s == 0) any = 0;
-  __syncthreads();
   if (s < P.m && P.active[s]) {
-    double2* Hk = P.H + ((size_t)s * P.R + k) * (P.R + 1);
     const double2* h0 = P.h + ((size_t)0 * P.m + s) * (P.R + 1);
     const double2* h1 = P.h + ((size_t)1 * P.m + s) * (P.R + 1);
-    for (int l = 0; l <= k; l++) Hk[l] = make_double2(h0[l].x + h1[l].x, h0[l].y + h1[l].y);
+    for (int l = lane; l <= k; l += 32) {
+      hcol[wl][l] = make_double2(h0[l].x + h1[l].x, h0[l].y + h1[l].y);
+      if (l < k) {
+        csv[wl][l] = P.cs[s * P.R + l];
+        snv[wl][l] = P.sn[s * P.R + l];
+      }
+    }
+    __syncwarp();
+    double2* Hk = P.H + ((size_t)s * P.R + k) * (P.R + 1);
     const double hn = sqrt(P.norm2[s]);
-    P.winv[s] = hn > 0.0 ? 1.0 / hn : 0.0;
-    Hk[k + 1] = make_double2(hn, 0.0);
-    // apply previous rotations
-    for (int l = 0; l < k; l++) {
-      const double c = P.cs[s * P.R + l];
-      const double2 sn = P.sn[s * P.R + l];
-      const double2 a = Hk[l], b = Hk[l + 1];
-      const double2 sb = cmul(sn, b);
-      const double2 csa = make_double2(-sn.x, sn.y);  // -conj(sn)
-      const double2 t = cmul(csa, a);
-      Hk[l] = make_double2(c * a.x + sb.x, c * a.y + sb.y);
-      Hk[l + 1] = make_double2(t.x + c * b.x, t.y + c * b.y);
+    if (lane == 0) {
+      double2* hc = hcol[wl];
+      hc[k + 1] = make_double2(hn, 0.0);
+      for (int l = 0; l < k; l++) {
+        const double c = csv[wl][l];
+        const double2 sn = snv[wl][l];
+        const double2 a = hc[l], b = hc[l + 1];
+        const double2 sb = cmul(sn, b);
+        const double2 t = cmul(make_double2(-sn.x, sn.y), a);  // -conj(sn) a
+        hc[l] = make_double2(c * a.x + sb.x, c * a.y + sb.y);
+        hc[l + 1] = make_double2(t.x + c * b.x, t.y + c * b.y);
+      }
+      const double2 a = hc[k], b = hc[k + 1];
+      const double na = sqrt(a.x * a.x + a.y * a.y), nb = sqrt(b.x * b.x + b.y * b.y);
+      const double rho = sqrt(na * na + nb * nb);
+      double c;
+      double2 sn;
+      if (rho == 0.0) {
+        c = 1.0;
+        sn = make_double2(0.0, 0.0);
+      } else if (na == 0.0) {
+        c = 0.0;
+        sn = make_double2(b.x / nb, -b.y / nb);  // conj(b)/|b|
+        hc[k] = make_double2(nb, 0.0);
+      } else {
+        c = na / rho;
+        const double2 ph = make_double2(a.x / na, a.y / na);
+        sn = cmul(ph, make_double2(b.x / rho, -b.y / rho));
+        hc[k] = make_double2(ph.x * rho, ph.y * rho);
+      }
+      hc[k + 1] = make_double2(0.0, 0.0);
+      P.cs[s * P.R + k] = c;
+      P.sn[s * P.R + k] = sn;
+      double2* gs = P.g + (size_t)s * (P.R + 1);
+      const double2 gk = gs[k];
+      gs[k + 1] = cmul(make_double2(-sn.x, sn.y), gk);
+      gs[k] = make_double2(c * gk.x, c * gk.y);
+      const double res = sqrt(gs[k + 1].x * gs[k + 1].x + gs[k + 1].y * gs[k + 1].y);
+      P.resid[s] = res;
+      P.kend[s] = k + 1;
+      P.winv[s] = hn > 0.0 ? 1.0 / hn : 0.0;
+      const bool breakdown = !(hn > 1e-300) || !(hn > 1e-14 * rho);
+      if (res <= P.tol[s] || breakdown || k + 1 >= P.R) {
+        P.active[s] = 0;
+      } else {
+        atomicAdd(any_count, 1);
+      }
     }
-    const double2 a = Hk[k], b = Hk[k + 1];
-    const double na = sqrt(a.x * a.x + a.y * a.y), nb = sqrt(b.x * b.x + b.y * b.y);
-    const double rho = sqrt(na * na + nb * nb);
-    double c;
-    double2 sn;
-    if (rho == 0.0) {
-      c = 1.0;
-      sn = make_double2(0.0, 0.0);
-    } else if (na == 0.0) {
-      c = 0.0;
-      sn = make_double2(b.x / nb, -b.y / nb);  // conj(b)/|b|
-      Hk[k] = make_double2(nb, 0.0);
-    } else {
-      c = na / rho;
-      const double2 ph = make_double2(a.x / na, a.y / na);
-      const double2 bc = make_double2(b.x / rho, -b.y / rho);
-      sn = cmul(ph, bc);
-      Hk[k] = make_double2(ph.x * rho, ph.y * rho);
-    }
-    Hk[k + 1] = make_double2(0.0, 0.0);
-    P.cs[s * P.R + k] = c;
-    P.sn[s * P.R + k] = sn;
-    double2* gs = P.g + (size_t)s * (P.R + 1);
-    const double2 gk = gs[k];
-    const double2 msc = make_double2(-sn.x, sn.y);  // -conj(sn)
-    gs[k + 1] = cmul(msc, gk);
-    gs[k] = make_double2(c * gk.x, c * gk.y);
-    const double res = sqrt(gs[k + 1].x * gs[k + 1].x + gs[k + 1].y * gs[k + 1].y);
-    P.resid[s] = res;
-    P.kend[s] = k + 1;
-    const bool breakdown = !(hn > 1e-300) || !(hn > 1e-14 * rho);
-    if (res <= P.tol[s] || breakdown || k + 1 >= P.R) {
-      P.active[s] = 0;
-    } else {
-      atomicAdd(&any, 1);
-    }
+    __syncwarp();
+    for (int l = lane; l <= k + 1; l += 32) Hk[l] = hcol[wl][l];
   }
+  if (s < P.m && lane == 0) P.norm2[s] = 0.0;
+  // the last block to finish publishes k + 1 and the activity flag
   __syncthreads();
-  if (s == 0) {
-    P.st->k = k + 1;
-    P.st->any_active = any;
-    P.st->skip = any ? 0 : 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int done = atomicAdd(done_blocks, 1);
+    if (done == (int)gridDim.x - 1) {
+      __threadfence();
+      const int any = atomicAdd(any_count, 0);
+      P.st->k = k + 1;
+      P.st->any_active = any;
+      P.st->skip = any ? 0 : 1;
+      *any_count = 0;
+      *done_blocks = 0;
+    }
   }
-  if (s < P.m) P.norm2[s] = 0.0;
 }
 
 // back substitution H y = g, then d_s += V y  (grid: rows x columns)
@@ -396,9 +424,10 @@ __global__ void gm_xupdate_kernel(GmPtrs P) {
   const int kk = P.kend[s];
   const double2* y = (const double2*)(P.y) + (size_t)s * P.R;
   double2 acc = P.d[(size_t)s * P.n + i];
-  const double2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
+  const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
   for (int l = 0; l < kk; l++) {
-    const double2 t = cmul(v[(size_t)l * P.n], y[l]);
+    const float2 vv = v[(size_t)l * P.n];
+    const double2 t = cmul(make_double2(vv.x, vv.y), y[l]);
     acc.x += t.x;
     acc.y += t.y;
   }
@@ -461,7 +490,7 @@ __global__ void gm_start_norm_kernel(GmPtrs P) {
   const double b = P.beta[s];
   const double inv = b > 0.0 ? 1.0 / b : 0.0;
   const double2 w = P.w[(size_t)s * P.n + i];
-  P.Vb[(size_t)s * (P.R + 1) * P.n + i] = make_double2(w.x * inv, w.y * inv);
+  P.Vb[(size_t)s * (P.R + 1) * P.n + i] = make_float2((float)(w.x * inv), (float)(w.y * inv));
 }
 
 // X = float(d) (for r_out - A_lp d), or X = 0
@@ -550,7 +579,7 @@ Layout layout(int n, int m, int R, int precision) {
     return r;
   };
   L.st = take(sizeof(GmState));
-  L.Vb = take(sizeof(double2) * (size_t)m * (R + 1) * n);
+  L.Vb = take(sizeof(float2) * (size_t)m * (R + 1) * n);
   L.H = take(sizeof(double2) * (size_t)m * R * (R + 1));
   L.cs = take(sizeof(double) * (size_t)m * R);
   L.sn = take(sizeof(double2) * (size_t)m * R);
@@ -578,7 +607,7 @@ Layout layout(int n, int m, int R, int precision) {
 }
 
 bool params_ok(const bem_solver_params* p) {
-  return p && p->restart >= 1 && p->restart <= 255 && p->max_iters >= 1 && p->max_refine >= 1 && p->rtol >= 0.0 &&
+  return p && p->restart >= 1 && p->restart < kMaxRestart && p->max_iters >= 1 && p->max_refine >= 1 && p->rtol >= 0.0 &&
          (p->precision == BEM_PREC_FP32 || p->precision == BEM_PREC_BF16X3 || p->precision == BEM_PREC_BF16);
 }
 
@@ -640,7 +669,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   P.n = n;
   P.m = m;
   P.R = R;
-  P.Vb = (double2*)(w + L.Vb);
+  P.Vb = (float2*)(w + L.Vb);
   P.H = (double2*)(w + L.H);
   P.cs = (double*)(w + L.cs);
   P.sn = (double2*)(w + L.sn);
@@ -682,6 +711,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   if (rc) return rc;
   std::vector<double> hres(m), hb(m);
 
+  BEM_CUDA_TRY(cudaMemsetAsync(P.st, 0, sizeof(GmState), s));
   BEM_CUDA_TRY(cudaMemsetAsync(P.bnorm2, 0, sizeof(double) * m, s));
   BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
   (gm_bnorm_kernel<<<gv, 256, 0, s>>>(P, (const float2*)B), count_launch());
@@ -753,7 +783,9 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
         (gm_update_kernel<<<gv, 256, 0, s>>>(P, 0), count_launch());
         (gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 1), count_launch());
         (gm_update_kernel<<<gv, 256, 0, s>>>(P, 1), count_launch());
-        (gm_finalize_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P), count_launch());
+        (gm_finalize_kernel<<<(m + kFinWarps - 1) / kFinWarps, 32 * kFinWarps, 0, s>>>(P, &P.st->any_count,
+                                                                                      &P.st->done_blocks),
+         count_launch());
         BEM_CUDA_TRY(cudaGetLastError());
         it++;
         total_iters++;

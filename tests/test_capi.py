@@ -44,7 +44,7 @@ def test_host_side_sizes():
                        inner_rtol=1e-3)
     n, m = 1000, 4
     b = lib.bem_gmres_workspace_bytes(n, m, ctypes.byref(p))
-    assert b > 16 * m * 31 * n
+    assert b > 8 * m * 31 * n  # complex64 Krylov basis of restart + 1 vectors per column
     p.restart = 0
     assert lib.bem_gmres_workspace_bytes(n, m, ctypes.byref(p)) == 0
     assert lib.bem_boundary2potential_scratch_bytes(100, 3) == 2 * 8 * 100 * 6 * 3
