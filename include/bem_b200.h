@@ -173,6 +173,21 @@ typedef struct bem_solver_info {
   double rel_residual; /* max over columns of ||b - A x|| / ||b|| (FP64, FP32 A) */
 } bem_solver_info;
 
+/* Tensor-core operator (tcgen05): the complex64 matrix A is split into bf16
+ * planes once (bem_tc_operator_prepare), after which bem_tc_matmul computes
+ * Y = A X for m <= 128 right-hand sides with FP32 accumulation in tensor
+ * memory.  precision: BEM_PREC_BF16X3 (A and X split hi/lo, three products)
+ * or BEM_PREC_BF16 (A in bf16, X split, two products).  No counterpart in the
+ * reference (it multiplies with cuBLAS through torch). */
+size_t bem_tc_operator_bytes(int n, int m, int precision);
+int bem_tc_operator_prepare(const void* A, int n, int precision, void* workspace, size_t workspace_bytes,
+                            bem_stream_t stream);
+int bem_tc_matmul(const void* workspace, size_t workspace_bytes, int n, int precision, const void* X, int m,
+                  void* Y, bem_stream_t stream);
+/* BEM_OK, or BEM_ERR_CUDA if a tensor-core kernel on this workspace gave up
+ * a bounded wait (synchronises `stream`). */
+int bem_tc_status(const void* workspace, bem_stream_t stream);
+
 /* Workspace bytes for bem_gmres_solve (n unknowns, m right-hand sides). */
 size_t bem_gmres_workspace_bytes(int n, int m, const bem_solver_params* params);
 

@@ -36,6 +36,7 @@ EXPORTED = (
     "bem_boundary_matrix", "bem_boundary_matrices_vk", "bem_identity_matrix", "bem_triangle2vertex",
     "bem_potential_matrix", "bem_boundary2potential_scratch_bytes", "bem_boundary2potential",
     "bem_cmatmul", "bem_gmres_workspace_bytes", "bem_gmres_solve",
+    "bem_tc_operator_bytes", "bem_tc_operator_prepare", "bem_tc_matmul", "bem_tc_status",
 )
 
 
@@ -105,6 +106,10 @@ def lib():
         "bem_cmatmul": ([vp, i, vp, i, vp, vp], i),
         "bem_gmres_workspace_bytes": ([i, i, P(SolverParams)], sz),
         "bem_gmres_solve": ([vp, i, vp, i, vp, i, P(SolverParams), vp, sz, P(SolverInfo), vp], i),
+        "bem_tc_operator_bytes": ([i, i, i], sz),
+        "bem_tc_operator_prepare": ([vp, i, i, vp, sz, vp], i),
+        "bem_tc_matmul": ([vp, sz, i, i, vp, i, vp, vp], i),
+        "bem_tc_status": ([vp, vp], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)

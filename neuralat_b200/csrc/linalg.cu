@@ -26,7 +26,9 @@ namespace bemb {
 
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
-int tc_matvec(const void* ws, int n, int precision, const float2* X, int m, float2* Y, cudaStream_t s);
+int tc_matvec(const void* ws, int n, int precision, const float2* X, int m, float2* Y, const int* skip,
+              cudaStream_t s);
+int tc_error(const void* ws, int* err_host, cudaStream_t s);
 size_t tc_workspace_bytes(int n, int m, int precision);
 
 namespace {
@@ -659,7 +661,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
                                bem_solver_info* info, bem_stream_t stream) {
   if (info) std::memset(info, 0, sizeof(*info));
   if (n <= 0 || m <= 0 || !A || !B || !X || !params_ok(params)) return BEM_ERR_INVALID_ARGUMENT;
-  if (m > 1024) return BEM_ERR_UNSUPPORTED;
+  if (m > 1024 || (params->precision != BEM_PREC_FP32 && m > 128)) return BEM_ERR_UNSUPPORTED;
   const int R = params->restart;
   const Layout L = layout(n, m, R, params->precision);
   if (!workspace || workspace_bytes < L.total) return BEM_ERR_WORKSPACE;
@@ -701,7 +703,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   auto inner_matvec = [&]() -> int {
     if (prec == BEM_PREC_FP32)
       return launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, &P.st->skip, s);
-    return tc_matvec(tcws, n, prec, P.X, m, P.Y, s);
+    return tc_matvec(tcws, n, prec, P.X, m, P.Y, &P.st->skip, s);
   };
 
   const dim3 gv((n + 255) / 256, m);
@@ -817,6 +819,10 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   (gm_store_x_kernel<<<gv, 256, 0, s>>>(P, (float2*)X), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (prec != BEM_PREC_FP32) {
+    int tc_err = 0;
+    if (tc_error(tcws, &tc_err, s) != BEM_OK || tc_err) status = BEM_ERR_CUDA;
+  }
   if (info) {
     info->status = status;
     info->iterations = total_iters;

@@ -1,0 +1,73 @@
+"""Tensor-core (tcgen05) complex matvec and the mixed-precision solve.
+
+bem_tc_matmul against an FP64 numpy product; GMRES with the bf16 operators
+(FP64 refinement against the FP32 matrix) against the FP32-operator solve.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from neuralat_b200 import _lib as L
+from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
+from neuralat_b200.bem import meshes as M
+from neuralat_b200.bem.solver import _stream, _vp
+
+pytestmark = pytest.mark.gpu
+
+
+def tc_matmul(A, X, precision):
+    lib = L.lib()
+    n, m = A.shape[0], X.shape[1]
+    nbytes = int(lib.bem_tc_operator_bytes(n, m, precision))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    L.check(lib.bem_tc_operator_prepare(_vp(A), n, precision, _vp(ws), nbytes, _stream()))
+    Y = torch.empty_like(X)
+    L.check(lib.bem_tc_matmul(_vp(ws), nbytes, n, precision, _vp(X), m, _vp(Y), _stream()))
+    L.check(lib.bem_tc_status(_vp(ws), _stream()))
+    return Y
+
+
+@pytest.mark.parametrize("n,m", [(1000, 8), (517, 3), (129, 1), (300, 16), (640, 37), (256, 64), (200, 128)])
+@pytest.mark.parametrize("precision,tol", [(L.PREC_BF16X3, 5e-5), (L.PREC_BF16, 1e-2)])
+def test_tc_matmul_vs_fp64(n, m, precision, tol):
+    rng = np.random.default_rng(n + m)
+    A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    X = (rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))).astype(np.complex64)
+    Y = tc_matmul(torch.from_numpy(A).cuda(), torch.from_numpy(X).cuda(), precision).cpu().numpy()
+    ref = A.astype(np.complex128) @ X.astype(np.complex128)
+    err = np.linalg.norm(Y - ref) / np.linalg.norm(ref)
+    assert err <= tol, err
+
+
+def test_tc_matmul_repeat_is_deterministic_enough():
+    rng = np.random.default_rng(5)
+    n, m = 800, 8
+    A = torch.from_numpy((rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)).cuda()
+    X = torch.from_numpy((rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))).astype(np.complex64)).cuda()
+    y1 = tc_matmul(A, X, L.PREC_BF16X3)
+    y2 = tc_matmul(A, X, L.PREC_BF16X3)
+    assert torch.allclose(y1, y2, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
+def test_mixed_precision_cbie_matches_fp32(precision):
+    v, t = M.icosphere(3, 0.15)
+    v = (v * np.array([1.2, 0.8, 1.0])).astype(np.float32)
+    k = M.wavenumber(4000.0)
+    g = torch.from_numpy(M.smoothed_gaussian_field(v.shape[0], t, 8, seed=2).astype(np.complex64)).cuda()
+    s = BEM_Solver(v, t)
+    V, A = s.assemble_vk(k)
+    rhs = -cmatmul(V, g)
+    i32, imx = {}, {}
+    x32 = gmres(A, rhs, rtol=1e-6, precision="fp32", info=i32)
+    xmx = gmres(A, rhs, rtol=1e-6, precision=precision, info=imx)
+    assert i32["status"] == L.BEM_OK and imx["status"] == L.BEM_OK, (i32, imx)
+    assert imx["rel_residual"] <= 1e-6
+    Ad = A.cpu().numpy().astype(np.complex128)
+    b = rhs.cpu().numpy().astype(np.complex128)
+    ref = np.linalg.solve(Ad, b)
+    for x in (x32, xmx):
+        xx = x.cpu().numpy()
+        assert np.linalg.norm(xx - ref) / np.linalg.norm(ref) <= 2e-5
