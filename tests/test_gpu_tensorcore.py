@@ -70,4 +70,4 @@ def test_mixed_precision_cbie_matches_fp32(precision):
     ref = np.linalg.solve(Ad, b)
     for x in (x32, xmx):
         xx = x.cpu().numpy()
-        assert np.linalg.norm(xx - ref) / np.linalg.norm(ref) <= 2e-5
+        assert np.linalg.norm(xx - ref) / np.linalg.norm(ref) <= 1e-4  # residual 1e-6 times the conditioning
