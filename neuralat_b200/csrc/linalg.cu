@@ -173,7 +173,8 @@ struct GmState {
   int pad;
   int any_count;   // scratch counters of gm_finalize_kernel (zero between launches)
   int done_blocks;
-  int pad2[2];
+  int act_count;   // columns active when the step started (scratch)
+  int iters_done;  // Arnoldi steps executed with at least one active column
 };
 
 struct GmPtrs {
@@ -316,6 +317,7 @@ __global__ void __launch_bounds__(32 * kFinWarps) gm_finalize_kernel(GmPtrs P, i
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int s = blockIdx.x * kFinWarps + wl;
   const int k = P.st->k;
+  if (s < P.m && P.active[s] && lane == 0) atomicAdd(&P.st->act_count, 1);
   if (s < P.m && P.active[s]) {
     const double2* h0 = P.h + ((size_t)0 * P.m + s) * (P.R + 1);
     const double2* h1 = P.h + ((size_t)1 * P.m + s) * (P.R + 1);
@@ -389,6 +391,8 @@ __global__ void __launch_bounds__(32 * kFinWarps) gm_finalize_kernel(GmPtrs P, i
     if (done == (int)gridDim.x - 1) {
       __threadfence();
       const int any = atomicAdd(any_count, 0);
+      if (atomicAdd(&P.st->act_count, 0) > 0) P.st->iters_done += 1;
+      P.st->act_count = 0;
       P.st->k = k + 1;
       P.st->any_active = any;
       P.st->skip = any ? 0 : 1;
@@ -613,24 +617,30 @@ bool params_ok(const bem_solver_params* p) {
          (p->precision == BEM_PREC_FP32 || p->precision == BEM_PREC_BF16X3 || p->precision == BEM_PREC_BF16);
 }
 
-// pinned host mirror of the convergence flag, one per host thread
-struct HostFlag {
-  GmState* h = nullptr;
-  cudaEvent_t ev = nullptr;
-  ~HostFlag() {
-    if (h) cudaFreeHost(h);
-    if (ev) cudaEventDestroy(ev);
+// Pinned host snapshots of the solver state, one per Arnoldi step in a ring,
+// each with an event.  The host runs at most kLookahead steps ahead of the
+// GPU: it blocks on the event of step it - kLookahead (the GPU still has that
+// many steps queued) and stops enqueueing once a snapshot shows every column
+// converged, so at most kLookahead no-op steps follow convergence.
+constexpr int kRing = 8;
+constexpr int kLookahead = 4;
+struct HostRing {
+  GmState* snap = nullptr;
+  cudaEvent_t ev[kRing] = {};
+  ~HostRing() {
+    if (snap) cudaFreeHost(snap);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
   }
 };
-thread_local HostFlag t_flag;
+thread_local HostRing t_ring;
 
-int host_flag(GmState** h, cudaEvent_t* ev) {
-  if (!t_flag.h) {
-    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_flag.h, sizeof(GmState), cudaHostAllocDefault));
-    BEM_CUDA_TRY(cudaEventCreateWithFlags(&t_flag.ev, cudaEventDisableTiming));
+int host_ring(HostRing** r) {
+  if (!t_ring.snap) {
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_ring.snap, sizeof(GmState) * kRing, cudaHostAllocDefault));
+    for (auto& e : t_ring.ev) BEM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
-  *h = t_flag.h;
-  *ev = t_flag.ev;
+  *r = &t_ring;
   return BEM_OK;
 }
 
@@ -707,9 +717,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   };
 
   const dim3 gv((n + 255) / 256, m);
-  GmState* hflag;
-  cudaEvent_t ev;
-  int rc = host_flag(&hflag, &ev);
+  HostRing* ring;
+  int rc = host_ring(&ring);
   if (rc) return rc;
   std::vector<double> hres(m), hb(m);
 
@@ -776,8 +785,6 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       first_cycle = false;
       int it = 0;
       bool cycle_done = false;
-      hflag->k = -1;  // no in-cycle snapshot yet (no copy is in flight here)
-      hflag->any_active = 1;
       while (it < R && total_iters < params->max_iters) {
         (gm_pack_kernel<<<gv, 256, 0, s>>>(P), count_launch());
         if ((rc = inner_matvec())) return rc;
@@ -789,19 +796,19 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
                                                                                       &P.st->done_blocks),
          count_launch());
         BEM_CUDA_TRY(cudaGetLastError());
+        BEM_CUDA_TRY(cudaMemcpyAsync(&ring->snap[it % kRing], P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+        BEM_CUDA_TRY(cudaEventRecord(ring->ev[it % kRing], s));
         it++;
         total_iters++;
-        matvecs++;
-        // look at the newest completed snapshot without stalling the GPU;
-        // steps enqueued after convergence are no-ops on the device
-        if (cudaEventQuery(ev) == cudaSuccess && hflag->k >= 0 && hflag->any_active == 0) cycle_done = true;
-        BEM_CUDA_TRY(cudaMemcpyAsync(hflag, P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));
-        BEM_CUDA_TRY(cudaEventRecord(ev, s));
+        if (it > kLookahead) {
+          const int old = (it - 1 - kLookahead) % kRing;
+          BEM_CUDA_TRY(cudaEventSynchronize(ring->ev[old]));
+          if (ring->snap[old].any_active == 0) cycle_done = true;
+        }
         if (cycle_done) break;
       }
       (gm_solve_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P), count_launch());
       (gm_xupdate_kernel<<<gv, 256, 0, s>>>(P), count_launch());
-      BEM_CUDA_TRY(cudaEventSynchronize(ev));
       // converged when no column is active at the end of the cycle with
       // resid <= tol (columns that stopped at the restart length restart)
       BEM_CUDA_TRY(cudaMemcpyAsync(hres.data(), P.resid, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
@@ -823,9 +830,13 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int tc_err = 0;
     if (tc_error(tcws, &tc_err, s) != BEM_OK || tc_err) status = BEM_ERR_CUDA;
   }
+  GmState fin;
+  BEM_CUDA_TRY(cudaMemcpy(&fin, P.st, sizeof(GmState), cudaMemcpyDeviceToHost));
+  (void)total_iters;  // steps enqueued; fin.iters_done counts the executed ones
+  matvecs += fin.iters_done;
   if (info) {
     info->status = status;
-    info->iterations = total_iters;
+    info->iterations = fin.iters_done;
     info->refinements = refinements;
     info->matvecs = matvecs;
     info->rel_residual = max_rel;
