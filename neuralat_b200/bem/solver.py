@@ -110,7 +110,7 @@ class SolveInfo(dict):
     pass
 
 
-def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_iters=1000, restart=200,
+def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_iters=1000, restart=120,
           precision="fp32", max_refine=None, inner_rtol=None, info: dict | None = None, raise_on_failure=False):
     """Device GMRES (+ FP64 refinement) for complex64 A and b of shape (n,) or (n, m)."""
     check_tensor(A, torch.complex64)
@@ -146,7 +146,7 @@ def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_
 
 
 def solve_linear_equation(A_func, b, x=None, nsteps=500, tol=1e-10, atol=1e-16, *, solver="gmres",
-                          precision="fp32", restart=200, info: dict | None = None):
+                          precision="fp32", restart=120, info: dict | None = None):
     """Solve A x = b (solver.py:61-66).
 
     ``A_func`` is a complex64 (n, n) tensor or a callable x -> A x.  Stops when
@@ -215,7 +215,7 @@ class BEM_Solver:
         return out
 
     # ---- boundary integral equations -------------------------------------
-    def CBIE(self, k, neumann, *, precision="fp32", solver="gmres", rtol=1e-5, restart=200, max_iters=1000,
+    def CBIE(self, k, neumann, *, precision="fp32", solver="gmres", rtol=1e-5, restart=120, max_iters=1000,
              info: dict | None = None):
         """Exterior Neumann CBIE (solver.py:97-104): (0.5 I - K) u = -V g."""
         V, lhs = self.assemble_vk(k)
@@ -291,7 +291,7 @@ class BEM_Solver:
         return self._b2p(k, neumann, dirichlet, points)
 
     # ---- the whole path ------------------------------------------------------
-    def solve_and_evaluate(self, k, neumann, points, *, precision="bf16x3", rtol=1e-6, restart=200, max_iters=1000,
+    def solve_and_evaluate(self, k, neumann, points, *, precision="bf16x3", rtol=1e-6, restart=120, max_iters=1000,
                            info: dict | None = None):
         """Assemble (fused V, 0.5 I - K), solve the CBIE for every column of
         ``neumann`` and evaluate the listener pressures.  Returns (u, p)."""

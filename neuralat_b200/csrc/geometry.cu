@@ -43,15 +43,42 @@ struct HostGeom {
   GeomHeader hdr{};
 };
 
+int analyse_host(HostGeom& g);
+
+// The most recent analysis of this host thread: bem_geometry_bytes followed by
+// bem_geometry_build on an unchanged mesh analyses it once.
+thread_local HostGeom t_last;
+thread_local bool t_last_valid = false;
+
 int analyse(const float* d_vertices, int nv, const int* d_triangles, int nt, cudaStream_t s, HostGeom& g) {
   if (nv <= 0 || nt <= 0 || !d_vertices || !d_triangles) return BEM_ERR_INVALID_ARGUMENT;
+  std::vector<float> vh(3 * (size_t)nv);
+  std::vector<int> th(3 * (size_t)nt);
+  BEM_CUDA_TRY(cudaMemcpyAsync(vh.data(), d_vertices, sizeof(float) * 3 * nv, cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaMemcpyAsync(th.data(), d_triangles, sizeof(int) * 3 * nt, cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (t_last_valid && t_last.nv == nv && t_last.nt == nt &&
+      std::memcmp(t_last.vertices.data(), vh.data(), vh.size() * sizeof(float)) == 0 &&
+      std::memcmp(t_last.triangles.data(), th.data(), th.size() * sizeof(int)) == 0) {
+    g = t_last;
+    return BEM_OK;
+  }
+  g = HostGeom{};
   g.nv = nv;
   g.nt = nt;
-  g.vertices.resize(3 * (size_t)nv);
-  g.triangles.resize(3 * (size_t)nt);
-  BEM_CUDA_TRY(cudaMemcpyAsync(g.vertices.data(), d_vertices, sizeof(float) * 3 * nv, cudaMemcpyDeviceToHost, s));
-  BEM_CUDA_TRY(cudaMemcpyAsync(g.triangles.data(), d_triangles, sizeof(int) * 3 * nt, cudaMemcpyDeviceToHost, s));
-  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  g.vertices.swap(vh);
+  g.triangles.swap(th);
+  t_last_valid = false;
+  const int rc = analyse_host(g);
+  if (rc == BEM_OK) {
+    t_last = g;
+    t_last_valid = true;
+  }
+  return rc;
+}
+
+int analyse_host(HostGeom& g) {
+  const int nv = g.nv, nt = g.nt;
 
   for (size_t i = 0; i < g.vertices.size(); i++)
     if (!std::isfinite(g.vertices[i])) return BEM_ERR_NONFINITE;

@@ -52,9 +52,13 @@ struct C2<double> {
 };
 
 constexpr int kMMThreads = 256;
-constexpr int kMMRowsPerWarp = 4;
-constexpr int kMMRows = kMMRowsPerWarp * (kMMThreads / 32);  // 32
 constexpr int kMMColTile = 128;
+// rows per warp: 4 in FP32 (X tile reused 4x), 2 in FP64 (register budget)
+template <typename T>
+struct MMRows {
+  static constexpr int kPerWarp = sizeof(T) == 4 ? 4 : 2;
+  static constexpr int kPerBlock = kPerWarp * (kMMThreads / 32);
+};
 
 // MODE 0: Y[i, s] = sum_j A[i, j] X[j, s]
 // MODE 1: Y[i, s] = B[i, s] - sum_j A[i, j] X[j, s], norm2[s] += |Y[i,s]|^2
@@ -65,6 +69,8 @@ __global__ void __launch_bounds__(kMMThreads)
                    int m, typename C2<T>::type* __restrict__ Y, int ldy, const float2* __restrict__ B, int ldb,
                    double* __restrict__ norm2, const int* __restrict__ skip) {
   typedef typename C2<T>::type CT;
+  constexpr int kMMRowsPerWarp = MMRows<T>::kPerWarp;
+  constexpr int kMMRows = MMRows<T>::kPerBlock;
   if (skip && *skip) return;
   __shared__ CT xs[MR][kMMColTile];  // [rhs][column]: lanes read consecutive columns
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -148,7 +154,7 @@ __global__ void __launch_bounds__(kMMThreads)
 template <typename T, int MODE>
 int launch_cmatmul(const float2* A, int n, const typename C2<T>::type* X, int ldx, int m, typename C2<T>::type* Y,
                    int ldy, const float2* B, int ldb, double* norm2, const int* skip, cudaStream_t s) {
-  const int rb = (n + kMMRows - 1) / kMMRows;
+  const int rb = (n + MMRows<T>::kPerBlock - 1) / MMRows<T>::kPerBlock;
   if (m == 1) {
     (cmatmul_kernel<T, 1, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
   } else if (m == 2) {
@@ -402,24 +408,34 @@ __global__ void __launch_bounds__(32 * kFinWarps) gm_finalize_kernel(GmPtrs P, i
   }
 }
 
-// back substitution H y = g, then d_s += V y  (grid: rows x columns)
-__global__ void gm_solve_kernel(GmPtrs P) {
-  const int s = threadIdx.x;
+// Back substitution H y = g on the Givens-reduced Hessenberg matrix, one
+// warp per column, column-oriented: y_j = g_j / H_jj, then the lanes update
+// g_0..g_{j-1} -= y_j H_{0..j-1, j} (column j of H is contiguous).
+constexpr int kSolveWarps = 4;
+__global__ void __launch_bounds__(32 * kSolveWarps) gm_solve_kernel(GmPtrs P) {
+  __shared__ double2 gsh[kSolveWarps][kMaxRestart + 1];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int s = blockIdx.x * kSolveWarps + wl;
   if (s >= P.m) return;
   const int kk = P.kend[s];
-  double2* y = (double2*)(P.y) + (size_t)s * P.R;
   const double2* gs = P.g + (size_t)s * (P.R + 1);
-  for (int l = kk - 1; l >= 0; l--) {
-    double2 acc = gs[l];
-    for (int j = l + 1; j < kk; j++) {
-      const double2 t = cmul(P.H[((size_t)s * P.R + j) * (P.R + 1) + l], y[j]);
-      acc.x -= t.x;
-      acc.y -= t.y;
-    }
-    const double2 hd = P.H[((size_t)s * P.R + l) * (P.R + 1) + l];
+  double2* y = (double2*)(P.y) + (size_t)s * P.R;
+  for (int l = lane; l < kk; l += 32) gsh[wl][l] = gs[l];
+  __syncwarp();
+  for (int j = kk - 1; j >= 0; j--) {
+    const double2* Hj = P.H + ((size_t)s * P.R + j) * (P.R + 1);  // column j, rows 0..j
+    const double2 hd = Hj[j];
     const double den = hd.x * hd.x + hd.y * hd.y;
-    y[l] = den > 0.0 ? make_double2((acc.x * hd.x + acc.y * hd.y) / den, (acc.y * hd.x - acc.x * hd.y) / den)
-                     : make_double2(0.0, 0.0);
+    const double2 gj = gsh[wl][j];
+    const double2 yj = den > 0.0 ? make_double2((gj.x * hd.x + gj.y * hd.y) / den, (gj.y * hd.x - gj.x * hd.y) / den)
+                                 : make_double2(0.0, 0.0);
+    if (lane == 0) y[j] = yj;
+    for (int l = lane; l < j; l += 32) {
+      const double2 t = cmul(Hj[l], yj);
+      gsh[wl][l].x -= t.x;
+      gsh[wl][l].y -= t.y;
+    }
+    __syncwarp();
   }
 }
 
@@ -807,7 +823,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
         }
         if (cycle_done) break;
       }
-      (gm_solve_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P), count_launch());
+      (gm_solve_kernel<<<(m + kSolveWarps - 1) / kSolveWarps, 32 * kSolveWarps, 0, s>>>(P), count_launch());
       (gm_xupdate_kernel<<<gv, 256, 0, s>>>(P), count_launch());
       // converged when no column is active at the end of the cycle with
       // resid <= tol (columns that stopped at the restart length restart)

@@ -110,6 +110,23 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Same, with an L2 eviction-priority policy (used to stream the matrix
+// evict-first so that the small, re-read Krylov basis stays in L2).
+__device__ __forceinline__ void tma_load_2d_hint(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar,
+                                                 uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, "
+      "%3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
 // Shared-memory matrix descriptor: K-major tile with 128-byte swizzle, rows
 // of 128 bytes, 8-row core groups 1024 bytes apart (SBO), sm100 version 1.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
@@ -212,13 +229,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---------------- TMA producer ----------------
     int stage = 0;
     uint32_t phase = 0;
+    const uint64_t stream_policy = l2_evict_first_policy();
     for (long long u = u0; u < u1; u++) {
       const int rb = (int)(u / p.n_kb), kb = (int)(u % p.n_kb);
       if (!mbar_wait(&empty[stage], phase ^ 1u, p.err)) break;
       unsigned char* st = base + stage * S::kStageBytes;
       mbar_expect_tx(&full[stage], S::kStageBytes);
-      tma_load_2d(st, &tmAh, kb * kBK, rb * kBM, &full[stage]);
-      if (X3) tma_load_2d(st + S::kABytes, &tmAl, kb * kBK, rb * kBM, &full[stage]);
+      tma_load_2d_hint(st, &tmAh, kb * kBK, rb * kBM, &full[stage], stream_policy);
+      if (X3) tma_load_2d_hint(st + S::kABytes, &tmAl, kb * kBK, rb * kBM, &full[stage], stream_policy);
       unsigned char* bst = st + (X3 ? 2 : 1) * S::kABytes;
       tma_load_2d(bst, &tmBh, kb * kBK, 0, &full[stage]);
       tma_load_2d(bst + S::kBBytes, &tmBl, kb * kBK, 0, &full[stage]);
