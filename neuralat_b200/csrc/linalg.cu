@@ -238,30 +238,42 @@ __global__ void gm_dots_kernel(GmPtrs P, int pass) {
   const int k = P.st->k;
   if (l > k || !P.active[s]) return;
   const float2* v = P.Vb + ((size_t)s * (P.R + 1) + l) * P.n;
-  double re = 0.0, im = 0.0;
-  for (int i = threadIdx.x; i < P.n; i += blockDim.x) {
-    double2 src;
-    if (pass == 0) {
-      const float2 y = P.Y[(size_t)i * P.m + s];
-      src = make_double2(y.x, y.y);
-    } else {
-      src = P.w[(size_t)s * P.n + i];
+  // four independent accumulators so the loads of consecutive strides overlap
+  double re[4] = {0.0, 0.0, 0.0, 0.0}, im[4] = {0.0, 0.0, 0.0, 0.0};
+  const int stride = blockDim.x;
+  for (int i0 = threadIdx.x; i0 < P.n; i0 += 4 * stride) {
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = i0 + u * stride;
+      if (i < P.n) {
+        double2 src;
+        if (pass == 0) {
+          const float2 y = P.Y[(size_t)i * P.m + s];
+          src = make_double2(y.x, y.y);
+        } else {
+          src = P.w[(size_t)s * P.n + i];
+        }
+        const float2 vv = v[i];
+        const double2 t = cmulc(make_double2(vv.x, vv.y), src);
+        re[u] += t.x;
+        im[u] += t.y;
+      }
     }
-    const float2 vv = v[i];
-    const double2 t = cmulc(make_double2(vv.x, vv.y), src);
-    re += t.x;
-    im += t.y;
   }
+  double re_ = (re[0] + re[1]) + (re[2] + re[3]);
+  double im_ = (im[0] + im[1]) + (im[2] + im[3]);
+  double& re_out = re_;
+  double& im_out = im_;
   __shared__ double sr[32], si[32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    re += __shfl_xor_sync(0xffffffffu, re, o);
-    im += __shfl_xor_sync(0xffffffffu, im, o);
+    re_out += __shfl_xor_sync(0xffffffffu, re_out, o);
+    im_out += __shfl_xor_sync(0xffffffffu, im_out, o);
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
-    sr[warp] = re;
-    si[warp] = im;
+    sr[warp] = re_out;
+    si[warp] = im_out;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -293,12 +305,31 @@ __global__ void gm_update_kernel(GmPtrs P, int pass) {
       acc = P.w[(size_t)s * P.n + i];
     }
     const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
-    for (int l = 0; l <= k; l++) {
+    // batches of 8 independent loads, two accumulators
+    double2 acc2 = make_double2(0.0, 0.0);
+    int l = 0;
+    for (; l + 8 <= k + 1; l += 8) {
+      float2 vv[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) vv[u] = v[(size_t)(l + u) * P.n];
+#pragma unroll
+      for (int u = 0; u < 8; u += 2) {
+        const double2 t0 = cmul(make_double2(vv[u].x, vv[u].y), hs[l + u]);
+        const double2 t1 = cmul(make_double2(vv[u + 1].x, vv[u + 1].y), hs[l + u + 1]);
+        acc.x -= t0.x;
+        acc.y -= t0.y;
+        acc2.x -= t1.x;
+        acc2.y -= t1.y;
+      }
+    }
+    for (; l <= k; l++) {
       const float2 vv = v[(size_t)l * P.n];
       const double2 t = cmul(make_double2(vv.x, vv.y), hs[l]);
       acc.x -= t.x;
       acc.y -= t.y;
     }
+    acc.x += acc2.x;
+    acc.y += acc2.y;
     P.w[(size_t)s * P.n + i] = acc;
     n2 = acc.x * acc.x + acc.y * acc.y;
   }
