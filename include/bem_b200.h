@@ -138,6 +138,22 @@ int bem_boundary2potential(const void* geom, const float* points, int np, float 
                            const void* dirichlet, int nrhs, void* out, void* scratch,
                            size_t scratch_bytes, bem_stream_t stream);
 
+/* Listener evaluation for callers that cannot allocate device memory (for
+ * example a real-time audio or rendering loop, where an allocation may block
+ * and synchronise the device past the callback deadline, or a C plug-in with
+ * no device allocator of its own).  Same result as bem_boundary2potential, no
+ * scratch argument: the densities live in a fixed 16 MiB array of the
+ * library's own device memory, reserved on every GPU that loads the library.
+ * Limit: 6 * nt * nrhs <= bem_boundary2potential_noalloc_max() (2^20), else
+ * BEM_ERR_WORKSPACE before any work.  The first call on a device (with it
+ * current) looks up the array's address; make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Calls no cudaMalloc/cudaFree.
+ * No counterpart in the reference, which allocates its outputs with torch. */
+long long bem_boundary2potential_noalloc_max(void);
+int bem_boundary2potential_noalloc(const void* geom, const float* points, int np, float k, const void* neumann,
+                                   const void* dirichlet, int nrhs, void* out, bem_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * Dense complex linear algebra.
  * ---------------------------------------------------------------------- */

@@ -37,6 +37,7 @@ EXPORTED = (
     "bem_potential_matrix", "bem_boundary2potential_scratch_bytes", "bem_boundary2potential",
     "bem_cmatmul", "bem_gmres_workspace_bytes", "bem_gmres_solve",
     "bem_tc_operator_bytes", "bem_tc_operator_prepare", "bem_tc_matmul", "bem_tc_status",
+    "bem_boundary2potential_noalloc_max", "bem_boundary2potential_noalloc",
 )
 
 
@@ -110,6 +111,8 @@ def lib():
         "bem_tc_operator_prepare": ([vp, i, i, vp, sz, vp], i),
         "bem_tc_matmul": ([vp, sz, i, i, vp, i, vp, vp], i),
         "bem_tc_status": ([vp, vp], i),
+        "bem_boundary2potential_noalloc_max": ([], ctypes.c_longlong),
+        "bem_boundary2potential_noalloc": ([vp, vp, i, f, vp, vp, i, vp, vp], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)

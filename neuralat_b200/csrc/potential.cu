@@ -252,3 +252,98 @@ extern "C" int bem_triangle2vertex(const void* geom, const void* tri_values, voi
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Listener evaluation for callers that cannot allocate device memory.
+//
+// Some hosts of this library never call cudaMalloc while they run: real-time
+// audio or rendering loops that synthesise sound from listener pressures
+// must not block on the allocator (an allocation may synchronise the device
+// and miss the callback deadline), and plug-ins embedded through a plain C
+// FFI often have no device allocator of their own.  This entry point is the
+// same computation as bem_boundary2potential, with the quadrature-point
+// densities kept in a fixed array of this library's own device memory
+// instead of a caller-provided scratch buffer.
+//
+// Contract:
+//  * the array holds 2 x kNoAllocQuadRhs complex64 values (16 MiB); every GPU
+//    that loads the library reserves it until the process exits;
+//  * requests with 6 * nt * nrhs > kNoAllocQuadRhs are rejected with
+//    BEM_ERR_WORKSPACE before any work is enqueued;
+//  * the first call on a device, with that device current, looks up the
+//    array's device address (cudaGetSymbolAddress) and caches it; make that
+//    first call before any stream capture;
+//  * all calls share the array and it keeps the last call's contents: each
+//    call overwrites every density it reads before reading it, so nothing
+//    needs clearing, but calls that overlap on the GPU (different streams,
+//    or different host threads) race on it and must be serialised by the
+//    caller;
+//  * no cudaMalloc, cudaFree or allocating library routine is called.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace bemb {
+namespace {
+constexpr long long kNoAllocQuadRhs = 1LL << 20;
+static __device__ __align__(256) float2 g_noalloc_density[2 * kNoAllocQuadRhs];
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 64;
+float2* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_density on the current device (set-up once per
+// device; the name itself is only a host-side handle for the symbol).
+int noalloc_density(float2** out) {
+  int dev = 0;
+  BEM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return BEM_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_density);
+    if (e != cudaSuccess || !p) return BEM_ERR_CUDA;
+    g_noalloc_addr[dev] = (float2*)p;
+  }
+  *out = g_noalloc_addr[dev];
+  return BEM_OK;
+}
+}  // namespace
+}  // namespace bemb
+
+extern "C" long long bem_boundary2potential_noalloc_max(void) { return bemb::kNoAllocQuadRhs; }
+
+extern "C" int bem_boundary2potential_noalloc(const void* geom, const float* points, int np, float k,
+                                              const void* neumann, const void* dirichlet, int nrhs, void* out,
+                                              bem_stream_t stream) {
+  GeomView g;
+  int rc = geom_view(geom, &g, nullptr);
+  if (rc) return rc;
+  if (np < 0 || nrhs <= 0 || (np > 0 && (!points || !out))) return BEM_ERR_INVALID_ARGUMENT;
+  if ((long long)6 * g.nt * nrhs > kNoAllocQuadRhs) return BEM_ERR_WORKSPACE;
+  if (np == 0) return BEM_OK;
+  float2* base = nullptr;
+  if ((rc = noalloc_density(&base))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  float2* dn = base;
+  float2* dd = base + kNoAllocQuadRhs;
+  const long long total = (long long)g.nt * 6 * nrhs;
+  (b2p_density_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, (const float2*)neumann,
+                                                                       (const float2*)dirichlet, nrhs, dn, dd),
+   count_launch());
+  BEM_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)np * nrhs, s));
+  const int nq = 6 * g.nt;
+  const int ptiles = (np + 31) / 32;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int nchunks = (4 * sms * 4 + ptiles - 1) / ptiles;
+  int chunk = (nq + nchunks - 1) / nchunks;
+  chunk = chunk < 256 ? 256 : chunk;
+  nchunks = (nq + chunk - 1) / chunk;
+  for (int r0 = 0; r0 < nrhs; r0 += kB2PRhs) {
+    (b2p_eval_kernel<<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, r0, chunk,
+                                                                    (float2*)out),
+     count_launch());
+  }
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
