@@ -164,6 +164,26 @@ int bem_boundary2potential_noalloc(const void* geom, const float* points, int np
  * (src/bem/solver.py:103,147; BiCGSTAB.py:52,68,73). */
 int bem_cmatmul(const void* A, int n, const void* X, int m, void* Y, bem_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Adjoint (differentiation).  No counterpart in the reference, which has no
+ * gradients; these serve the hand-written adjoint of the listener pressures
+ * p = -S g + D u, (1/2 M - K) u = -V g.
+ * ---------------------------------------------------------------------- */
+
+/* Y = A^H X for an n x n complex64 A and m columns (Y overwritten). */
+int bem_cmatmul_adjoint(const void* A, int n, const void* X, int m, void* Y, bem_stream_t stream);
+/* out = conj(A)^T (n x n complex64, out != A). */
+int bem_conj_transpose(const void* A, int n, void* out, bem_stream_t stream);
+/* out_s = S^H pbar, out_d = D^H pbar (each nv complex64, either may be NULL)
+ * for np listener weights pbar (complex64). */
+int bem_boundary2potential_adjoint(const void* geom, const float* points, int np, float k, const void* pbar,
+                                   void* out_s, void* out_d, bem_stream_t stream);
+/* grad (nv x 3 float64, overwritten) = d/dx Re[ -pbar^H S g + pbar^H D u
+ *   - lambda^H V g - 1/2 lambda^H M u + lambda^H K u ] with the vectors held
+ * fixed (lambda, g = neumann, u = dirichlet: nv complex64; pbar: np). */
+int bem_vertex_gradient(const void* geom, float k, const void* lambda, const void* neumann, const void* dirichlet,
+                        const float* points, int np, const void* pbar, double* grad, bem_stream_t stream);
+
 /* Solver precision of the dense operator. */
 enum {
   BEM_PREC_FP32 = 0,   /* complex64 CUDA-core matvec */

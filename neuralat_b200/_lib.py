@@ -38,6 +38,7 @@ EXPORTED = (
     "bem_cmatmul", "bem_gmres_workspace_bytes", "bem_gmres_solve",
     "bem_tc_operator_bytes", "bem_tc_operator_prepare", "bem_tc_matmul", "bem_tc_status",
     "bem_boundary2potential_noalloc_max", "bem_boundary2potential_noalloc",
+    "bem_cmatmul_adjoint", "bem_conj_transpose", "bem_boundary2potential_adjoint", "bem_vertex_gradient",
 )
 
 
@@ -113,6 +114,10 @@ def lib():
         "bem_tc_status": ([vp, vp], i),
         "bem_boundary2potential_noalloc_max": ([], ctypes.c_longlong),
         "bem_boundary2potential_noalloc": ([vp, vp, i, f, vp, vp, i, vp, vp], i),
+        "bem_cmatmul_adjoint": ([vp, i, vp, i, vp, vp], i),
+        "bem_conj_transpose": ([vp, i, vp, vp], i),
+        "bem_boundary2potential_adjoint": ([vp, vp, i, f, vp, vp, vp, vp], i),
+        "bem_vertex_gradient": ([vp, f, vp, vp, vp, vp, i, vp, vp, vp], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)
