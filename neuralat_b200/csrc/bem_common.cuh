@@ -130,6 +130,8 @@ __device__ __forceinline__ void atomic_add_c64(float2* p, float re, float im) {
 namespace bemb {
 // process-wide count of kernel launches issued by this library (host side)
 void count_launch();
+void count_launches(unsigned long long n);
+unsigned long long launch_count();
 }  // namespace bemb
 
 // error-checking helper for host code inside the library

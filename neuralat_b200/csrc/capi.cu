@@ -16,6 +16,8 @@ int assemble_generic(const GeomView& g, int layer, int order, float k, const flo
 namespace bemb {
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace bemb
 
 using namespace bemb;

@@ -18,6 +18,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "bem_common.cuh"
@@ -232,57 +233,80 @@ __global__ void gm_pack_kernel(GmPtrs P) {
   }
 }
 
-// h[pass][s][l] = <V[s][l], src_s>, l <= k.  Block per (l, s).
-__global__ void gm_dots_kernel(GmPtrs P, int pass) {
-  const int l = blockIdx.x, s = blockIdx.y;
+// w_s = double(Y[:, s]) for active columns (Y is (n, m) row-major; w is
+// column-major, so both Gram-Schmidt passes read contiguous vectors).
+__global__ void gm_y2w_kernel(GmPtrs P) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)P.n * P.m) return;
+  const int i = (int)(idx / P.m), s = (int)(idx - (long long)i * P.m);
+  if (!P.active[s]) return;
+  const float2 y = P.Y[idx];
+  P.w[(size_t)s * P.n + i] = make_double2(y.x, y.y);
+}
+
+// h[pass][s][l] += <V[s][l], w_s> over one chunk of rows, for a group of
+// kDotL basis vectors: every thread keeps 8 rows of w in registers and issues
+// 8 x kDotL independent loads; partial sums reach h through FP64 atomics
+// (h is zeroed at the start of a cycle and after each use).
+constexpr int kDotThreads = 256;
+constexpr int kDotRowsPerThread = 8;
+constexpr int kDotRows = kDotThreads * kDotRowsPerThread;  // 2048
+constexpr int kDotL = 8;
+__global__ void __launch_bounds__(kDotThreads) gm_dots_kernel(GmPtrs P, int pass) {
+  const int s = blockIdx.z;
+  if (!P.active[s]) return;
   const int k = P.st->k;
-  if (l > k || !P.active[s]) return;
-  const float2* v = P.Vb + ((size_t)s * (P.R + 1) + l) * P.n;
-  // four independent accumulators so the loads of consecutive strides overlap
-  double re[4] = {0.0, 0.0, 0.0, 0.0}, im[4] = {0.0, 0.0, 0.0, 0.0};
-  const int stride = blockDim.x;
-  for (int i0 = threadIdx.x; i0 < P.n; i0 += 4 * stride) {
+  const int l0 = blockIdx.y * kDotL;
+  if (l0 > k) return;
+  const int nl = min(kDotL, k + 1 - l0);
+  const int row0 = blockIdx.x * kDotRows;
+  double2 src[kDotRowsPerThread];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int i = i0 + u * stride;
-      if (i < P.n) {
-        double2 src;
-        if (pass == 0) {
-          const float2 y = P.Y[(size_t)i * P.m + s];
-          src = make_double2(y.x, y.y);
-        } else {
-          src = P.w[(size_t)s * P.n + i];
+  for (int u = 0; u < kDotRowsPerThread; u++) {
+    const int i = row0 + threadIdx.x + u * kDotThreads;
+    src[u] = i < P.n ? P.w[(size_t)s * P.n + i] : make_double2(0.0, 0.0);
+  }
+  double re[kDotL], im[kDotL];
+#pragma unroll
+  for (int ll = 0; ll < kDotL; ll++) {
+    re[ll] = 0.0;
+    im[ll] = 0.0;
+    if (ll < nl) {
+      const float2* v = P.Vb + ((size_t)s * (P.R + 1) + l0 + ll) * P.n;
+#pragma unroll
+      for (int u = 0; u < kDotRowsPerThread; u++) {
+        const int i = row0 + threadIdx.x + u * kDotThreads;
+        if (i < P.n) {
+          const float2 vv = v[i];
+          re[ll] += (double)vv.x * src[u].x + (double)vv.y * src[u].y;  // conj(v) w
+          im[ll] += (double)vv.x * src[u].y - (double)vv.y * src[u].x;
         }
-        const float2 vv = v[i];
-        const double2 t = cmulc(make_double2(vv.x, vv.y), src);
-        re[u] += t.x;
-        im[u] += t.y;
       }
     }
   }
-  double re_ = (re[0] + re[1]) + (re[2] + re[3]);
-  double im_ = (im[0] + im[1]) + (im[2] + im[3]);
-  double& re_out = re_;
-  double& im_out = im_;
-  __shared__ double sr[32], si[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    re_out += __shfl_xor_sync(0xffffffffu, re_out, o);
-    im_out += __shfl_xor_sync(0xffffffffu, im_out, o);
-  }
+  __shared__ double red[kDotThreads / 32][kDotL][2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    sr[warp] = re_out;
-    si[warp] = im_out;
+#pragma unroll
+  for (int ll = 0; ll < kDotL; ll++) {
+    double a = re[ll], b = im[ll];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      red[warp][ll][0] = a;
+      red[warp][ll][1] = b;
+    }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
-      a += sr[w];
-      b += si[w];
-    }
-    P.h[((size_t)pass * P.m + s) * (P.R + 1) + l] = make_double2(a, b);
+  if (threadIdx.x < 2 * nl) {
+    const int ll = threadIdx.x >> 1, c = threadIdx.x & 1;
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kDotThreads / 32; w++) t += red[w][ll][c];
+    double* h = (double*)(P.h + ((size_t)pass * P.m + s) * (P.R + 1) + l0 + ll);
+    atomicAdd(h + c, t);
   }
 }
 
@@ -297,13 +321,7 @@ __global__ void gm_update_kernel(GmPtrs P, int pass) {
   __syncthreads();
   double n2 = 0.0;
   if (i < P.n) {
-    double2 acc;
-    if (pass == 0) {
-      const float2 y = P.Y[(size_t)i * P.m + s];
-      acc = make_double2(y.x, y.y);
-    } else {
-      acc = P.w[(size_t)s * P.n + i];
-    }
+    double2 acc = P.w[(size_t)s * P.n + i];
     const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
     // batches of 8 independent loads, two accumulators
     double2 acc2 = make_double2(0.0, 0.0);
@@ -418,6 +436,12 @@ __global__ void __launch_bounds__(32 * kFinWarps) gm_finalize_kernel(GmPtrs P, i
     }
     __syncwarp();
     for (int l = lane; l <= k + 1; l += 32) Hk[l] = hcol[wl][l];
+    double2* h0w = P.h + ((size_t)0 * P.m + s) * (P.R + 1);
+    double2* h1w = P.h + ((size_t)1 * P.m + s) * (P.R + 1);
+    for (int l = lane; l <= k; l += 32) {
+      h0w[l] = make_double2(0.0, 0.0);
+      h1w[l] = make_double2(0.0, 0.0);
+    }
   }
   if (s < P.m && lane == 0) P.norm2[s] = 0.0;
   // the last block to finish publishes k + 1 and the activity flag
@@ -682,6 +706,30 @@ struct HostRing {
 };
 thread_local HostRing t_ring;
 
+// One Arnoldi step (every kernel reads the step index from device memory) is
+// captured once per solve on a private stream and replayed with one graph
+// launch per step on the caller's stream.
+thread_local cudaStream_t t_capture_stream = nullptr;
+
+int capture_graph(const std::function<int(cudaStream_t)>& body, cudaGraphExec_t* exec, unsigned long long* nkern) {
+  if (!t_capture_stream) BEM_CUDA_TRY(cudaStreamCreateWithFlags(&t_capture_stream, cudaStreamNonBlocking));
+  const unsigned long long l0 = launch_count();
+  BEM_CUDA_TRY(cudaStreamBeginCapture(t_capture_stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = body(t_capture_stream);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(t_capture_stream, &graph);
+  if (rc != BEM_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return rc != BEM_OK ? rc : BEM_ERR_CUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) return BEM_ERR_CUDA;
+  *nkern = launch_count() - l0;
+  return BEM_OK;
+}
+
 int host_ring(HostRing** r) {
   if (!t_ring.snap) {
     BEM_CUDA_TRY(cudaHostAlloc((void**)&t_ring.snap, sizeof(GmState) * kRing, cudaHostAllocDefault));
@@ -757,13 +805,33 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int rc = tc_operator_prepare((const float2*)A, n, prec, tcws, s);
     if (rc) return rc;
   }
-  auto inner_matvec = [&]() -> int {
+  auto inner_matvec_on = [&](cudaStream_t st) -> int {
     if (prec == BEM_PREC_FP32)
-      return launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, &P.st->skip, s);
-    return tc_matvec(tcws, n, prec, P.X, m, P.Y, &P.st->skip, s);
+      return launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, &P.st->skip, st);
+    return tc_matvec(tcws, n, prec, P.X, m, P.Y, &P.st->skip, st);
   };
+  auto inner_matvec = [&]() -> int { return inner_matvec_on(s); };
 
   const dim3 gv((n + 255) / 256, m);
+  const dim3 dots_grid((n + kDotRows - 1) / kDotRows, (R + 1 + kDotL - 1) / kDotL, m);
+  auto arnoldi_step = [&](cudaStream_t st) -> int {
+    (gm_pack_kernel<<<gv, 256, 0, st>>>(P), count_launch());
+    int r2 = inner_matvec_on(st);
+    if (r2) return r2;
+    (gm_y2w_kernel<<<(unsigned)(((long long)n * m + 255) / 256), 256, 0, st>>>(P), count_launch());
+    (gm_dots_kernel<<<dots_grid, kDotThreads, 0, st>>>(P, 0), count_launch());
+    (gm_update_kernel<<<gv, 256, 0, st>>>(P, 0), count_launch());
+    (gm_dots_kernel<<<dots_grid, kDotThreads, 0, st>>>(P, 1), count_launch());
+    (gm_update_kernel<<<gv, 256, 0, st>>>(P, 1), count_launch());
+    (gm_finalize_kernel<<<(m + kFinWarps - 1) / kFinWarps, 32 * kFinWarps, 0, st>>>(P, &P.st->any_count,
+                                                                                   &P.st->done_blocks),
+     count_launch());
+    BEM_CUDA_TRY(cudaGetLastError());
+    return BEM_OK;
+  };
+  cudaGraphExec_t step_exec = nullptr;
+  unsigned long long step_kernels = 0;
+  bool step_direct_done = false;  // the first step runs uncaptured (sets kernel attributes)
   HostRing* ring;
   int rc = host_ring(&ring);
   if (rc) return rc;
@@ -825,6 +893,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
         if ((rc = inner_matvec())) return rc;
         matvecs++;
       }
+      BEM_CUDA_TRY(cudaMemsetAsync(P.h, 0, sizeof(double2) * 2 * (size_t)m * (R + 1), s));
       (gm_start_vec_kernel<<<gv, 256, 0, s>>>(P, first_cycle ? 0 : 1), count_launch());
       // absolute inner target: inner_rtol * ||r_out|| but never below rtol * ||b|| / 2
       (gm_start_scalar_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P, rnorm2, inner_rtol, 0.5 * params->rtol), count_launch());
@@ -833,16 +902,16 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       int it = 0;
       bool cycle_done = false;
       while (it < R && total_iters < params->max_iters) {
-        (gm_pack_kernel<<<gv, 256, 0, s>>>(P), count_launch());
-        if ((rc = inner_matvec())) return rc;
-        (gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 0), count_launch());
-        (gm_update_kernel<<<gv, 256, 0, s>>>(P, 0), count_launch());
-        (gm_dots_kernel<<<dim3(R + 1, m), 256, 0, s>>>(P, 1), count_launch());
-        (gm_update_kernel<<<gv, 256, 0, s>>>(P, 1), count_launch());
-        (gm_finalize_kernel<<<(m + kFinWarps - 1) / kFinWarps, 32 * kFinWarps, 0, s>>>(P, &P.st->any_count,
-                                                                                      &P.st->done_blocks),
-         count_launch());
-        BEM_CUDA_TRY(cudaGetLastError());
+        if (!step_direct_done || !step_exec) {
+          if ((rc = arnoldi_step(s))) return rc;
+          if (!step_direct_done) {
+            step_direct_done = true;
+            if (capture_graph(arnoldi_step, &step_exec, &step_kernels) != BEM_OK) step_exec = nullptr;
+          }
+        } else {
+          BEM_CUDA_TRY(cudaGraphLaunch(step_exec, s));
+          count_launches(step_kernels);
+        }
         BEM_CUDA_TRY(cudaMemcpyAsync(&ring->snap[it % kRing], P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));
         BEM_CUDA_TRY(cudaEventRecord(ring->ev[it % kRing], s));
         it++;
@@ -877,6 +946,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int tc_err = 0;
     if (tc_error(tcws, &tc_err, s) != BEM_OK || tc_err) status = BEM_ERR_CUDA;
   }
+  if (step_exec) cudaGraphExecDestroy(step_exec);
   GmState fin;
   BEM_CUDA_TRY(cudaMemcpy(&fin, P.st, sizeof(GmState), cudaMemcpyDeviceToHost));
   (void)total_iters;  // steps enqueued; fin.iters_done counts the executed ones
