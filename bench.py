@@ -54,6 +54,11 @@ def parse():
     ap.add_argument("--kernel-case", choices=["assemble", "solve", "eval"], default=None,
                     help="profiling case: one stage on an icosphere of --subdiv, after one warm-up launch")
     ap.add_argument("--subdiv", type=int, default=4)
+    ap.add_argument("--batch-case", action="store_true",
+                    help="batching workload: meshes x wavenumbers through the batch runner vs one at a time")
+    ap.add_argument("--batch-meshes", type=int, default=16)
+    ap.add_argument("--batch-k", type=int, default=4)
+    ap.add_argument("--batch-max-subdiv", type=int, default=4)
     return ap.parse_args()
 
 
@@ -433,9 +438,64 @@ def run_kernel_case(args):
     print(f"kernel case {args.kernel_case} subdiv {args.subdiv} N={v.shape[0]} T={t.shape[0]} ok")
 
 
+def run_batch_case(args):
+    """Meshes of subdivision U{2..max} x log-uniform frequencies x 16 RHS x 512
+    listeners: the batch runner (one batched assembly launch family per wave,
+    concurrent solves on worker streams, autotuned launch shape) against the
+    same problems solved one at a time through ``BEM_Solver``."""
+    import torch
+
+    from neuralat_b200.bem import BEM_Solver, autotune
+    from neuralat_b200.bem import meshes as M
+    from neuralat_b200.bem.batch import BatchRunner
+
+    probs, pts = M.batching(n_meshes=args.batch_meshes, n_k=args.batch_k, n_rhs=16,
+                            max_subdiv=args.batch_max_subdiv)
+    meshes = [(p["vertices"].astype(np.float32), p["triangles"].astype(np.int32)) for p in probs]
+    ks = [p["ks"] for p in probs]
+    gs = [p["neumann"].astype(np.complex64) for p in probs]
+    nprob = sum(len(x) for x in ks)
+    pts_d = torch.from_numpy(pts.astype(np.float32)).cuda()
+
+    def one_at_a_time():
+        out = []
+        for (v, t), kk, g in zip(meshes, ks, gs):
+            s = BEM_Solver(v, t)
+            gd = torch.from_numpy(g).cuda()
+            for k in kk:
+                _, p = s.solve_and_evaluate(k, gd, pts_d, precision=args.precision, rtol=1e-6)
+                out.append(p)
+        torch.cuda.synchronize()
+        return out
+
+    tuned = autotune.tune_assembly([BEM_Solver(v, t) for v, t in meshes[:8]], [k[0] for k in ks[:8]], repeats=2)
+    runner = BatchRunner(workers=4, precision=args.precision, rtol=1e-6)
+    runner.run(meshes[:2], [k[:1] for k in ks[:2]], gs[:2], pts)  # warm-up
+    one_at_a_time()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    one_at_a_time()
+    t_seq = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res = runner.run(meshes, ks, gs, pts)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    line = {
+        "case": "batching", "problems": nprob, "meshes": len(meshes),
+        "vertices": sorted({int(m[0].shape[0]) for m in meshes}), "rhs": 16, "listeners": int(pts.shape[0]),
+        "precision": args.precision, "tuning": {k: tuned[k] for k in ("chunk", "ctas_per_sm")},
+        "one_at_a_time_problems_per_s": nprob / t_seq, "batched_problems_per_s": nprob / t_batch,
+        "speedup": t_seq / t_batch,
+        "max_rel_residual": max(i.get("rel_residual", 0.0) for i in res.info),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.kernel_case:
+    if args.batch_case:
+        run_batch_case(args)
+    elif args.kernel_case:
         run_kernel_case(args)
     elif args.impl == "reference":
         run_reference(args)

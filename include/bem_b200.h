@@ -114,6 +114,32 @@ int bem_boundary_matrix(const void* geom, int layer, int order, float k, const f
 int bem_boundary_matrices_vk(const void* geom, float k, void* v_out, void* k_out, float mass_coeff,
                              float k_coeff, bem_stream_t stream);
 
+/* Batched fused assembly: many problems (meshes of any size, each with its
+ * own wavenumber) in one persistent launch whose CTAs drain a single queue of
+ * (problem, 32 test triangles, trial-tile chunk) work items, plus one launch
+ * per touching-pair type over all problems.  `problems` is a HOST array;
+ * every v_out / k_out must be non-NULL (nv x nv complex64, overwritten with V
+ * and mass_coeff M + k_coeff K).  Workspace: bem_batch_workspace_bytes.
+ * No counterpart in the reference (one mesh, one wavenumber per call). */
+typedef struct bem_batch_problem {
+  const void* geom; /* built geometry */
+  float k;          /* wavenumber */
+  void* v_out;
+  void* k_out;
+} bem_batch_problem;
+size_t bem_batch_workspace_bytes(int nproblems);
+int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, float mass_coeff, float k_coeff,
+                          void* workspace, size_t workspace_bytes, bem_stream_t stream);
+
+/* Launch-shape knobs of the assembly kernels, set by the autotuner
+ * (0 = automatic).  Process-wide. */
+enum {
+  BEM_TUNE_ASSEMBLY_CHUNK = 1,      /* trial tiles (16 triangles) per work item */
+  BEM_TUNE_ASSEMBLY_CTAS_PER_SM = 2 /* persistent CTAs per SM (<= occupancy limit) */
+};
+int bem_set_tuning(int key, int value);
+int bem_get_tuning(int key);
+
 /* Dense P1 mass matrix (bind.cu:10-21), overwriting out. */
 int bem_identity_matrix(const void* geom, void* out, bem_stream_t stream);
 

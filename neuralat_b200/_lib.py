@@ -39,6 +39,7 @@ EXPORTED = (
     "bem_tc_operator_bytes", "bem_tc_operator_prepare", "bem_tc_matmul", "bem_tc_status",
     "bem_boundary2potential_noalloc_max", "bem_boundary2potential_noalloc",
     "bem_cmatmul_adjoint", "bem_conj_transpose", "bem_boundary2potential_adjoint", "bem_vertex_gradient",
+    "bem_batch_workspace_bytes", "bem_batch_matrices_vk", "bem_set_tuning", "bem_get_tuning",
 )
 
 
@@ -47,6 +48,14 @@ class BEMError(RuntimeError):
         self.status = int(status)
         msg = _status_string(self.status)
         super().__init__(f"{what}: {msg} (status {self.status})" if what else f"{msg} (status {self.status})")
+
+
+TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM = 1, 2
+
+
+class BatchProblem(ctypes.Structure):
+    _fields_ = [("geom", ctypes.c_void_p), ("k", ctypes.c_float), ("v_out", ctypes.c_void_p),
+                ("k_out", ctypes.c_void_p)]
 
 
 class SolverParams(ctypes.Structure):
@@ -118,6 +127,10 @@ def lib():
         "bem_conj_transpose": ([vp, i, vp, vp], i),
         "bem_boundary2potential_adjoint": ([vp, vp, i, f, vp, vp, vp, vp], i),
         "bem_vertex_gradient": ([vp, f, vp, vp, vp, vp, i, vp, vp, vp], i),
+        "bem_batch_workspace_bytes": ([i], sz),
+        "bem_batch_matrices_vk": ([P(BatchProblem), i, f, f, vp, sz, vp], i),
+        "bem_set_tuning": ([i, i], i),
+        "bem_get_tuning": ([i], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)

@@ -26,12 +26,18 @@
 //     pair over a precomputed pair list (no O(T^2) adjacency scan).
 
 #include <cmath>
+#include <cstring>
 
 #include "bem_common.cuh"
 
 namespace bemb {
 
 int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
+
+namespace {
+extern int g_tune_chunk;
+extern int g_tune_ctas_per_sm;
+}  // namespace
 
 namespace {
 
@@ -134,18 +140,15 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes
 
 // Work item = (group of 32 test triangles = 2 tiles) x (chunk of `chunk`
 // trial tiles).  Items are dealt round-robin to a persistent grid.
+// One work item: test group `grp` (32 triangles = 2 tiles) against the trial
+// tiles [ch * chunk, ch * chunk + chunk).
 template <bool DO_V, bool DO_K>
-__global__ void __launch_bounds__(kRegThreads, 2)
-    regular_vk_kernel(GeomView g, float k, float2* __restrict__ V, float2* __restrict__ K, float v_scale,
-                      float k_scale, int chunk, int n_chunks, int n_items) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  RegSmem<DO_V, DO_K>& sm = *reinterpret_cast<RegSmem<DO_V, DO_K>*>(smem_raw);
+__device__ __forceinline__ void regular_item(RegSmem<DO_V, DO_K>& sm, const GeomView& g, float k,
+                                             float2* __restrict__ V, float2* __restrict__ K, float v_scale,
+                                             float k_scale, int grp, int ch, int chunk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nt = g.nt, nv = g.nv;
-
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int grp = item / n_chunks;
-    const int ch = item - grp * n_chunks;
+  {
     const int tile0 = 2 * grp;
     const bool has_t1 = tile0 + 1 < g.ntiles;
 
@@ -229,6 +232,19 @@ __global__ void __launch_bounds__(kRegThreads, 2)
         if (DO_K) atomicAdd(&K[idx], acc_k);
       }
     }
+  }
+}
+
+// Single problem: items dealt round-robin to a persistent grid.
+template <bool DO_V, bool DO_K>
+__global__ void __launch_bounds__(kRegThreads, 2)
+    regular_vk_kernel(GeomView g, float k, float2* __restrict__ V, float2* __restrict__ K, float v_scale,
+                      float k_scale, int chunk, int n_chunks, int n_items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RegSmem<DO_V, DO_K>& sm = *reinterpret_cast<RegSmem<DO_V, DO_K>*>(smem_raw);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int grp = item / n_chunks;
+    regular_item<DO_V, DO_K>(sm, g, k, V, K, v_scale, k_scale, grp, item - grp * n_chunks, chunk);
   }
 }
 
@@ -383,14 +399,10 @@ __device__ __forceinline__ R warp_sum(R x) {
 
 // NCOMMON = 3: pairs (i, i), i = pair index; otherwise pairs from the list.
 template <typename R, int NCOMMON, bool DO_V, bool DO_K>
-__global__ void __launch_bounds__(128)
-    singular_vk_kernel(GeomView g, const int2* __restrict__ pairs, int npairs, float k, float2* __restrict__ V,
-                       float2* __restrict__ K, float v_scale, float k_scale, float mass_coeff) {
+__device__ __forceinline__ void singular_pair(const GeomView& g, int ti, int tj, float k, float2* __restrict__ V,
+                                              float2* __restrict__ K, float v_scale, float k_scale,
+                                              float mass_coeff) {
   const int lane = threadIdx.x & 31;
-  const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (pair >= npairs) return;
-  const int ti = NCOMMON == 3 ? pair : pairs[pair].x;
-  const int tj = NCOMMON == 3 ? pair : pairs[pair].y;
   const int s0 = g.triangles[3 * ti], s1 = g.triangles[3 * ti + 1], s2 = g.triangles[3 * ti + 2];
   const int t0 = g.triangles[3 * tj], t1 = g.triangles[3 * tj + 1], t2 = g.triangles[3 * tj + 2];
   const Perm pm = reorder_pair<NCOMMON>(s0, s1, s2, t0, t1, t2);
@@ -483,6 +495,94 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+template <typename R, int NCOMMON, bool DO_V, bool DO_K>
+__global__ void __launch_bounds__(128)
+    singular_vk_kernel(GeomView g, const int2* __restrict__ pairs, int npairs, float k, float2* __restrict__ V,
+                       float2* __restrict__ K, float v_scale, float k_scale, float mass_coeff) {
+  const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pair >= npairs) return;
+  const int ti = NCOMMON == 3 ? pair : pairs[pair].x;
+  const int tj = NCOMMON == 3 ? pair : pairs[pair].y;
+  singular_pair<R, NCOMMON, DO_V, DO_K>(g, ti, tj, k, V, K, v_scale, k_scale, mass_coeff);
+}
+
+// ---------------------------------------------------------------------------
+// Batched assembly: many problems (meshes of uneven size, wavenumbers) in one
+// persistent launch.  Regular work items of all problems form one queue that
+// CTAs drain with an atomic counter (dynamic load balance); touching pairs of
+// all problems are concatenated per type.
+// ---------------------------------------------------------------------------
+struct BatchProblem {
+  GeomView g;
+  float k;
+  int chunk, n_chunks;
+  float2* V;
+  float2* K;
+  long long item_begin;   // prefix sum of regular items
+  long long pair_begin[3];  // prefix sums of coincident / edge / vertex pairs
+};
+
+struct BatchHeader {
+  unsigned long long next_item;  // queue head (zeroed before each launch)
+  int nproblems;
+  int pad;
+  long long total_items;
+  long long total_pairs[3];
+};
+
+__device__ __forceinline__ int find_problem(const BatchProblem* probs, int np, long long x, int which) {
+  int lo = 0, hi = np - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long b = which < 0 ? probs[mid].item_begin : probs[mid].pair_begin[which];
+    if (b <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kRegThreads, 2)
+    regular_vk_batch_kernel(BatchHeader* __restrict__ hdr, const BatchProblem* __restrict__ probs, float v_scale,
+                            float k_scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RegSmem<true, true>& sm = *reinterpret_cast<RegSmem<true, true>*>(smem_raw);
+  __shared__ long long s_item;
+  const int np = hdr->nproblems;
+  const long long total = hdr->total_items;
+  for (;;) {
+    __syncthreads();  // everyone has read s_item of the previous round
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(&hdr->next_item, 1ull);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= total) break;
+    const int pi = find_problem(probs, np, item, -1);
+    const BatchProblem& P = probs[pi];
+    const int local = (int)(item - P.item_begin);
+    const int grp = local / P.n_chunks;
+    regular_item<true, true>(sm, P.g, P.k, P.V, P.K, v_scale, k_scale, grp, local - grp * P.n_chunks, P.chunk);
+  }
+}
+
+template <typename R, int NCOMMON>
+__global__ void __launch_bounds__(128)
+    singular_vk_batch_kernel(const BatchHeader* __restrict__ hdr, const BatchProblem* __restrict__ probs,
+                             float v_scale, float k_scale, float mass_coeff) {
+  const int which = NCOMMON == 3 ? 0 : (NCOMMON == 2 ? 1 : 2);
+  const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pair >= hdr->total_pairs[which]) return;
+  const int pi = find_problem(probs, hdr->nproblems, pair, which);
+  const BatchProblem& P = probs[pi];
+  const int local = (int)(pair - P.pair_begin[which]);
+  int ti = local, tj = local;
+  if (NCOMMON == 2) {
+    ti = P.g.edge_pairs[local].x;
+    tj = P.g.edge_pairs[local].y;
+  } else if (NCOMMON == 1) {
+    ti = P.g.vert_pairs[local].x;
+    tj = P.g.vert_pairs[local].y;
+  }
+  singular_pair<R, NCOMMON, true, true>(P.g, ti, tj, P.k, P.V, P.K, v_scale, k_scale, mass_coeff);
+}
+
 // Dense P1 mass matrix, one thread per triangle (bind.cu:10-21).
 __global__ void mass_kernel(GeomView g, float2* __restrict__ M, float coeff) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -521,10 +621,12 @@ int launch_regular(const GeomView& g, float k, float2* V, float2* K, float v_sca
   const int n_groups = (g.nt + kTestTris - 1) / kTestTris;
   int occ = 0;
   BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_vk_kernel<DO_V, DO_K>, kRegThreads, smem));
+  if (g_tune_ctas_per_sm > 0 && g_tune_ctas_per_sm < occ) occ = g_tune_ctas_per_sm;
   const int grid = sm_count() * (occ > 0 ? occ : 1);
   // chunk of trial tiles per work item: enough items to balance the grid
   int chunk = (int)((long long)n_groups * g.ntiles / (8LL * grid));
   chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
+  if (g_tune_chunk > 0) chunk = g_tune_chunk;
   const int n_chunks = (g.ntiles + chunk - 1) / chunk;
   const int n_items = n_groups * n_chunks;
   (regular_vk_kernel<DO_V, DO_K><<<grid < n_items ? grid : n_items, kRegThreads, smem, s>>>(
@@ -575,6 +677,134 @@ int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_
 int assemble_mass(const GeomView& g, float2* M, float coeff, bool zero, cudaStream_t s) {
   if (zero) BEM_CUDA_TRY(cudaMemsetAsync(M, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
   (mass_kernel<<<(g.nt + 127) / 128, 128, 0, s>>>(g, M, coeff), count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+}  // namespace bemb
+
+// ---------------------------------------------------------------------------
+// Batched assembly host side and tuning knobs.
+// ---------------------------------------------------------------------------
+#include <vector>
+
+namespace bemb {
+
+namespace {
+int g_tune_chunk = 0;        // trial tiles per regular work item (0: automatic)
+int g_tune_ctas_per_sm = 0;  // persistent CTAs per SM (0: occupancy limit)
+
+struct PinnedStage {
+  void* buf = nullptr;
+  size_t cap = 0;
+  cudaEvent_t ev = nullptr;
+  ~PinnedStage() {
+    if (buf) cudaFreeHost(buf);
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+thread_local PinnedStage t_stage;
+
+inline size_t al256b(size_t x) { return (x + 255) / 256 * 256; }
+}  // namespace
+
+int set_tuning(int key, int value) {
+  if (value < 0) return BEM_ERR_INVALID_ARGUMENT;
+  switch (key) {
+    case BEM_TUNE_ASSEMBLY_CHUNK: g_tune_chunk = value; return BEM_OK;
+    case BEM_TUNE_ASSEMBLY_CTAS_PER_SM: g_tune_ctas_per_sm = value; return BEM_OK;
+  }
+  return BEM_ERR_INVALID_ARGUMENT;
+}
+
+int get_tuning(int key) {
+  switch (key) {
+    case BEM_TUNE_ASSEMBLY_CHUNK: return g_tune_chunk;
+    case BEM_TUNE_ASSEMBLY_CTAS_PER_SM: return g_tune_ctas_per_sm;
+  }
+  return -1;
+}
+
+size_t batch_workspace_bytes(int np) {
+  return al256b(sizeof(BatchHeader)) + al256b(sizeof(BatchProblem) * (size_t)(np > 0 ? np : 1));
+}
+
+int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs, float2* const* Ks, int np,
+                      float mass_coeff, float k_coeff, void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (np <= 0) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ws || ws_bytes < batch_workspace_bytes(np)) return BEM_ERR_WORKSPACE;
+  const int smem = (int)sizeof(RegSmem<true, true>);
+  static bool attr = false;
+  if (!attr) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(regular_vk_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  // host descriptors
+  const size_t hbytes = al256b(sizeof(BatchHeader)), pbytes = sizeof(BatchProblem) * (size_t)np;
+  if (!t_stage.ev) BEM_CUDA_TRY(cudaEventCreateWithFlags(&t_stage.ev, cudaEventDisableTiming));
+  BEM_CUDA_TRY(cudaEventSynchronize(t_stage.ev));  // previous upload from the staging buffer is done
+  if (t_stage.cap < hbytes + pbytes) {
+    if (t_stage.buf) cudaFreeHost(t_stage.buf);
+    t_stage.cap = 2 * (hbytes + pbytes);
+    BEM_CUDA_TRY(cudaHostAlloc(&t_stage.buf, t_stage.cap, cudaHostAllocDefault));
+  }
+  BatchHeader* hh = (BatchHeader*)t_stage.buf;
+  BatchProblem* hp = (BatchProblem*)((char*)t_stage.buf + hbytes);
+  std::memset(hh, 0, sizeof(BatchHeader));
+  hh->nproblems = np;
+  long long items = 0, pairs[3] = {0, 0, 0};
+  const size_t elem = sizeof(float2);
+  for (int p = 0; p < np; p++) {
+    const GeomView& g = views[p];
+    if (!Vs[p] || !Ks[p]) return BEM_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(ks[p])) return BEM_ERR_NONFINITE;
+    BEM_CUDA_TRY(cudaMemsetAsync(Vs[p], 0, elem * (size_t)g.nv * g.nv, s));
+    BEM_CUDA_TRY(cudaMemsetAsync(Ks[p], 0, elem * (size_t)g.nv * g.nv, s));
+    BatchProblem& P = hp[p];
+    P.g = g;
+    P.k = ks[p];
+    int chunk = g_tune_chunk > 0 ? g_tune_chunk : (g.ntiles / 4 < 1 ? 1 : (g.ntiles / 4 > 32 ? 32 : g.ntiles / 4));
+    P.chunk = chunk;
+    P.n_chunks = (g.ntiles + chunk - 1) / chunk;
+    P.V = Vs[p];
+    P.K = Ks[p];
+    P.item_begin = items;
+    items += (long long)((g.nt + kTestTris - 1) / kTestTris) * P.n_chunks;
+    P.pair_begin[0] = pairs[0];
+    P.pair_begin[1] = pairs[1];
+    P.pair_begin[2] = pairs[2];
+    pairs[0] += g.nt;
+    pairs[1] += g.n_edge;
+    pairs[2] += g.n_vert;
+  }
+  hh->total_items = items;
+  for (int t = 0; t < 3; t++) hh->total_pairs[t] = pairs[t];
+  BatchHeader* dh = (BatchHeader*)ws;
+  BatchProblem* dp = (BatchProblem*)((char*)ws + hbytes);
+  BEM_CUDA_TRY(cudaMemcpyAsync(ws, t_stage.buf, hbytes + pbytes, cudaMemcpyHostToDevice, s));
+  BEM_CUDA_TRY(cudaEventRecord(t_stage.ev, s));
+  const float v_scale = kInv4Pi, k_scale = -kInv4Pi * k_coeff;
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_vk_batch_kernel, kRegThreads, smem));
+  if (g_tune_ctas_per_sm > 0 && g_tune_ctas_per_sm < occ) occ = g_tune_ctas_per_sm;
+  const long long grid = (long long)sm_count() * (occ > 0 ? occ : 1);
+  if (items > 0)
+    (regular_vk_batch_kernel<<<(unsigned)(grid < items ? grid : items), kRegThreads, smem, s>>>(dh, dp, v_scale,
+                                                                                                k_scale),
+     count_launch());
+  const int wpb = 4;
+  if (pairs[0])
+    (singular_vk_batch_kernel<double, 3><<<(unsigned)((pairs[0] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(
+         dh, dp, v_scale, k_scale, mass_coeff),
+     count_launch());
+  if (pairs[1])
+    (singular_vk_batch_kernel<float, 2><<<(unsigned)((pairs[1] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(
+         dh, dp, v_scale, k_scale, mass_coeff),
+     count_launch());
+  if (pairs[2])
+    (singular_vk_batch_kernel<float, 1><<<(unsigned)((pairs[2] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(
+         dh, dp, v_scale, k_scale, mass_coeff),
+     count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }

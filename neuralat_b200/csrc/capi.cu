@@ -2,6 +2,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <vector>
 
 #include "bem_common.cuh"
 
@@ -11,6 +12,11 @@ int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_
 int assemble_mass(const GeomView& g, float2* M, float coeff, bool zero, cudaStream_t s);
 int assemble_generic(const GeomView& g, int layer, int order, float k, const float* normals, const float* curls,
                      float2* out, cudaStream_t s);
+int set_tuning(int key, int value);
+int get_tuning(int key);
+size_t batch_workspace_bytes(int np);
+int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs, float2* const* Ks, int np,
+                      float mass_coeff, float k_coeff, void* ws, size_t ws_bytes, cudaStream_t s);
 }  // namespace bemb
 
 namespace bemb {
@@ -74,4 +80,25 @@ extern "C" int bem_identity_matrix(const void* geom, void* out, bem_stream_t str
   if (rc) return rc;
   if (!out) return BEM_ERR_INVALID_ARGUMENT;
   return assemble_mass(g, (float2*)out, 1.f, true, (cudaStream_t)stream);
+}
+
+extern "C" int bem_set_tuning(int key, int value) { return set_tuning(key, value); }
+extern "C" int bem_get_tuning(int key) { return get_tuning(key); }
+extern "C" size_t bem_batch_workspace_bytes(int nproblems) { return batch_workspace_bytes(nproblems); }
+
+extern "C" int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, float mass_coeff, float k_coeff,
+                                     void* workspace, size_t workspace_bytes, bem_stream_t stream) {
+  if (!problems || nproblems <= 0) return BEM_ERR_INVALID_ARGUMENT;
+  std::vector<GeomView> views(nproblems);
+  std::vector<float> ks(nproblems);
+  std::vector<float2*> Vs(nproblems), Ks(nproblems);
+  for (int p = 0; p < nproblems; p++) {
+    int rc = geom_view(problems[p].geom, &views[p], nullptr);
+    if (rc) return rc;
+    ks[p] = problems[p].k;
+    Vs[p] = (float2*)problems[p].v_out;
+    Ks[p] = (float2*)problems[p].k_out;
+  }
+  return assemble_vk_batch(views.data(), ks.data(), Vs.data(), Ks.data(), nproblems, mass_coeff, k_coeff, workspace,
+                           workspace_bytes, (cudaStream_t)stream);
 }

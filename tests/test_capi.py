@@ -67,3 +67,22 @@ def test_no_cpu_fallback_without_device():
     nbytes = ctypes.c_size_t(0)
     st = lib.bem_geometry_bytes(ctypes.c_void_p(16), 3, ctypes.c_void_p(16), 1, ctypes.byref(nbytes), None)
     assert st == L.BEM_ERR_CUDA
+
+
+def test_tuning_knobs_and_batch_sizes():
+    lib = L.lib()
+    assert lib.bem_get_tuning(L.TUNE_ASSEMBLY_CHUNK) == 0
+    assert lib.bem_set_tuning(L.TUNE_ASSEMBLY_CHUNK, 4) == L.BEM_OK
+    assert lib.bem_get_tuning(L.TUNE_ASSEMBLY_CHUNK) == 4
+    assert lib.bem_set_tuning(L.TUNE_ASSEMBLY_CTAS_PER_SM, 1) == L.BEM_OK
+    assert lib.bem_get_tuning(L.TUNE_ASSEMBLY_CTAS_PER_SM) == 1
+    assert lib.bem_set_tuning(99, 1) == L.BEM_ERR_INVALID_ARGUMENT
+    assert lib.bem_set_tuning(L.TUNE_ASSEMBLY_CHUNK, -1) == L.BEM_ERR_INVALID_ARGUMENT
+    assert lib.bem_get_tuning(99) == -1
+    for key in (L.TUNE_ASSEMBLY_CHUNK, L.TUNE_ASSEMBLY_CTAS_PER_SM):
+        assert lib.bem_set_tuning(key, 0) == L.BEM_OK
+    assert lib.bem_batch_workspace_bytes(1) >= 256
+    assert lib.bem_batch_workspace_bytes(1000) > lib.bem_batch_workspace_bytes(10)
+    assert lib.bem_batch_matrices_vk(None, 1, 0.5, -1.0, None, 0, None) == L.BEM_ERR_INVALID_ARGUMENT
+    probs = (L.BatchProblem * 1)()
+    assert lib.bem_batch_matrices_vk(probs, 0, 0.5, -1.0, None, 0, None) == L.BEM_ERR_INVALID_ARGUMENT
