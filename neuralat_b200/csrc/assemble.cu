@@ -25,6 +25,7 @@
 //     separate Sauter-Schwab kernels (coincident pairs in FP64), one warp per
 //     pair over a precomputed pair list (no O(T^2) adjacency scan).
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -613,10 +614,10 @@ int sm_count() {
 template <bool DO_V, bool DO_K>
 int launch_regular(const GeomView& g, float k, float2* V, float2* K, float v_scale, float k_scale, cudaStream_t s) {
   const int smem = (int)sizeof(RegSmem<DO_V, DO_K>);
-  static bool attr_set = false;
-  if (!attr_set) {
+  static std::atomic<bool> attr_set{false};
+  if (!attr_set.load(std::memory_order_acquire)) {
     BEM_CUDA_TRY(cudaFuncSetAttribute(regular_vk_kernel<DO_V, DO_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr_set = true;
+    attr_set.store(true, std::memory_order_release);
   }
   const int n_groups = (g.nt + kTestTris - 1) / kTestTris;
   int occ = 0;
@@ -734,10 +735,10 @@ int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs,
   if (np <= 0) return BEM_ERR_INVALID_ARGUMENT;
   if (!ws || ws_bytes < batch_workspace_bytes(np)) return BEM_ERR_WORKSPACE;
   const int smem = (int)sizeof(RegSmem<true, true>);
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<bool> attr{false};
+  if (!attr.load(std::memory_order_acquire)) {
     BEM_CUDA_TRY(cudaFuncSetAttribute(regular_vk_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
+    attr.store(true, std::memory_order_release);
   }
   // host descriptors
   const size_t hbytes = al256b(sizeof(BatchHeader)), pbytes = sizeof(BatchProblem) * (size_t)np;

@@ -19,6 +19,7 @@
 // pairs in FP64), with one output and the quadrature points computed from the
 // vertices for any rule.
 
+#include <atomic>
 #include <cmath>
 
 #include "bem_common.cuh"
@@ -445,11 +446,11 @@ template <int LAYER, int TN>
 int launch_regular_generic(const GeomView& g, float k, const float* normals, const float* curls, float2* out,
                            cudaStream_t s) {
   const int smem = (int)sizeof(GenSmem);
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<bool> attr{false};
+  if (!attr.load(std::memory_order_acquire)) {
     BEM_CUDA_TRY(cudaFuncSetAttribute(regular_generic_kernel<LAYER, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
-    attr = true;
+    attr.store(true, std::memory_order_release);
   }
   int dev = 0, sms = 148, occ = 1;
   cudaGetDevice(&dev);

@@ -21,6 +21,7 @@
 // mbarrier wait is bounded in time; on expiry the kernel raises an error flag
 // and unwinds instead of spinning.
 
+#include <atomic>
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -379,15 +380,17 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+EncodeTiledFn lookup_encode_fn() {
+  void* ptr = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    return (EncodeTiledFn)ptr;
+  return nullptr;
+}
+
 EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* ptr = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)ptr;
-  }
+  static const EncodeTiledFn fn = lookup_encode_fn();  // initialised once, thread-safe
   return fn;
 }
 
@@ -438,10 +441,10 @@ TcLayout tc_layout(int n, int m, int precision) {
 template <int NB, bool X3>
 int launch_tc(const TcLayout& L, char* ws, int n, const int* skip, float* Y, int m2, cudaStream_t s) {
   using S = TcSmem<NB, X3>;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<bool> attr{false};
+  if (!attr.load(std::memory_order_acquire)) {
     BEM_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NB, X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
-    attr = true;
+    attr.store(true, std::memory_order_release);
   }
   CUtensorMap mah, mal, mbh, mbl;
   int rc;
