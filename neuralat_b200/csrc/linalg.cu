@@ -16,29 +16,35 @@
 //    without stalling the GPU.  Outer FP64 iterative refinement
 //    r = b - A x against the FP32 matrix.
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
 #include <vector>
 
+#include <cooperative_groups.h>
+#include <cuda_bf16.h>
+
+#include "async_copy.cuh"
 #include "bem_common.cuh"
 
 namespace bemb {
 
+namespace cg = cooperative_groups;
+
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
-int tc_matvec(const void* ws, int n, int precision, const float2* X, int m, float2* Y, const int* skip,
+int tc_matvec(const void* ws, int n, int precision, const float2* X, int m, float2* Y, const int* active,
               cudaStream_t s);
 int tc_error(const void* ws, int* err_host, cudaStream_t s);
 size_t tc_workspace_bytes(int n, int m, int precision);
+int tc_b_planes(void* ws, int n, int m, int precision, __nv_bfloat16** bh, __nv_bfloat16** bl, int* ldb, int* nb);
+int tc_gemm(const void* ws, int n, int precision, int m, float2* Y, const int* active, cudaStream_t s);
 
 namespace {
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // conj(a) * b
-  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
 }
 
 template <typename T>
@@ -68,11 +74,15 @@ template <typename T, int MR, int MODE>
 __global__ void __launch_bounds__(kMMThreads)
     cmatmul_kernel(const float2* __restrict__ A, int n, const typename C2<T>::type* __restrict__ X, int ldx,
                    int m, typename C2<T>::type* __restrict__ Y, int ldy, const float2* __restrict__ B, int ldb,
-                   double* __restrict__ norm2, const int* __restrict__ skip) {
+                   double* __restrict__ norm2, const int* __restrict__ active) {
   typedef typename C2<T>::type CT;
   constexpr int kMMRowsPerWarp = MMRows<T>::kPerWarp;
   constexpr int kMMRows = MMRows<T>::kPerBlock;
-  if (skip && *skip) return;
+  if (active) {  // GMRES: nothing to do once every column has converged
+    int any = 0;
+    for (int c = 0; c < m; c++) any |= active[c];
+    if (!any) return;
+  }
   __shared__ CT xs[MR][kMMColTile];  // [rhs][column]: lanes read consecutive columns
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int row0 = blockIdx.x * kMMRows + warp * kMMRowsPerWarp;
@@ -154,17 +164,17 @@ __global__ void __launch_bounds__(kMMThreads)
 
 template <typename T, int MODE>
 int launch_cmatmul(const float2* A, int n, const typename C2<T>::type* X, int ldx, int m, typename C2<T>::type* Y,
-                   int ldy, const float2* B, int ldb, double* norm2, const int* skip, cudaStream_t s) {
+                   int ldy, const float2* B, int ldb, double* norm2, const int* active, cudaStream_t s) {
   const int rb = (n + MMRows<T>::kPerBlock - 1) / MMRows<T>::kPerBlock;
   if (m == 1) {
-    (cmatmul_kernel<T, 1, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
+    (cmatmul_kernel<T, 1, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, active), count_launch());
   } else if (m == 2) {
-    (cmatmul_kernel<T, 2, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
+    (cmatmul_kernel<T, 2, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, active), count_launch());
   } else if (m <= 4) {
-    (cmatmul_kernel<T, 4, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, skip), count_launch());
+    (cmatmul_kernel<T, 4, MODE><<<dim3(rb, 1), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2, active), count_launch());
   } else {
     (cmatmul_kernel<T, 8, MODE><<<dim3(rb, (m + 7) / 8), kMMThreads, 0, s>>>(A, n, X, ldx, m, Y, ldy, B, ldb, norm2,
-                                                                          skip), count_launch());
+                                                                          active), count_launch());
   }
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
@@ -174,24 +184,25 @@ int launch_cmatmul(const float2* A, int n, const typename C2<T>::type* X, int ld
 // GMRES state and kernels
 // ---------------------------------------------------------------------------
 struct GmState {
-  int k;           // Arnoldi step inside the current cycle (same for all active columns)
-  int any_active;  // 0 when every column has converged (matvec early-out)
-  int skip;        // == !any_active, read by the matvec kernel
-  int pad;
-  int any_count;   // scratch counters of gm_finalize_kernel (zero between launches)
-  int done_blocks;
-  int act_count;   // columns active when the step started (scratch)
-  int iters_done;  // Arnoldi steps executed with at least one active column
+  int err;  // a bounded wait of gm_arnoldi_kernel expired
+  int pad[3];
 };
+
+// Host-mapped ring of per-step column activity (kSnapRing steps x m ints),
+// written by the Arnoldi kernel and read by the host after the step's event.
+constexpr int kSnapRing = 8;
 
 struct GmPtrs {
   int n, m, R;
-  float2* Vb;      // [m][R+1][n]  Krylov basis, complex64 storage
+  int ldv;         // basis row stride (n rounded up to even: 16-byte pairs)
+  int ldb;         // row stride of the tensor-core B planes
+  float2* Vb;      // [m][R+1][ldv]  orthonormal Krylov basis, complex64 storage
+  __nv_bfloat16* bh;  // tensor-core B planes (hi, lo) of the matvec operand, or NULL (FP32 matvec on X)
+  __nv_bfloat16* bl;
   double2* H;      // [m][R][R+1]  column k, rows 0..k+1
   double* cs;      // [m][R]
   double2* sn;     // [m][R]
   double2* g;      // [m][R+1]
-  double2* h;      // [2][m][R+1]  dots of the two CGS passes
   double2* w;      // [m][n]
   double2* d;      // [m][n]  inner correction
   double2* x;      // [n][m]  solution (FP64)
@@ -199,267 +210,454 @@ struct GmPtrs {
   float2* X;       // [n][m]  matvec input
   float2* Y;       // [n][m]  matvec output
   double* norm2;   // [m]  |w|^2 accumulator of the current step
-  double* winv;    // [m]  1 / h_{k+1,k} of the previous step
   double* beta;    // [m]
   double* tol;     // [m] inner absolute tolerance
   double* resid;   // [m]
   int* active;     // [m]
   int* kend;       // [m]  basis size used by each column in this cycle
+  int* kcol;       // [m]  Arnoldi step of each column inside the current cycle
+  int* colstep;    // [m]  Arnoldi launches so far in this solve (snapshot slot)
+  int* snap;       // device view of the host-mapped activity ring
   double* y;       // [m][R]
   GmState* st;
   double* bnorm2;  // [m]
 };
 
-// X[:, s] = float(V[s][k]) after normalising w into V[s][k] (k > 0).
-__global__ void gm_pack_kernel(GmPtrs P) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y;
-  if (i >= P.n) return;
-  const int k = P.st->k;
-  float2* vk = P.Vb + ((size_t)s * (P.R + 1) + k) * P.n;
-  if (P.active[s]) {
-    float2 v;
-    if (k > 0) {
-      const double inv = P.winv[s];
-      const double2 ww = P.w[(size_t)s * P.n + i];
-      v = make_float2((float)(ww.x * inv), (float)(ww.y * inv));
-      vk[i] = v;
-    } else {
-      v = vk[i];
+// ---------------------------------------------------------------------------
+// Arnoldi step = the matvec plus ONE launch of gm_arnoldi_kernel.
+//
+// A thread-block cluster (up to 16 CTAs) owns one right-hand-side column;
+// its CTAs split the unknowns and keep their slice of w in shared memory for
+// the whole step:
+//   w = Y (Y cleared for the next accumulating matvec)
+//   h1 = V^H w                 classical Gram-Schmidt, FP64 sums
+//   w' = w - V h1;  h2 = V^H w'  (re-orthogonalisation, CGS2)
+//   w'' = w' - V h2;  h_{k+1,k} = |w''|
+//   v_{k+1} = w'' / h_{k+1,k} -> basis (complex64) and the next matvec operand
+//   Givens rotation of the new Hessenberg column (CTA 0 of the cluster)
+// Partial sums of each CTA are combined across the cluster through
+// distributed shared memory after a cluster barrier (no global atomics);
+// every CTA forms the same totals.  Each of the four passes streams the CTA's
+// slice of basis vectors 0..k through a ring of shared-memory stages with
+// 1-D bulk async copies (mbarrier completion, bounded waits), so the copy
+// engine keeps a whole pass in flight while the threads compute from shared
+// memory.  Threads own pairs of consecutive unknowns; per-basis-vector sums
+// are reduced with a warp reduce-scatter.  The last column to finish
+// publishes k + 1 and the activity flag for the host and the matvec.
+// ---------------------------------------------------------------------------
+constexpr int kArnConsumerWarps = 12;
+constexpr int kArnConsumers = 32 * kArnConsumerWarps;
+constexpr int kArnThreads = kArnConsumers + 32;  // + one producer warp (bulk copies)
+constexpr int kArnWarps = kArnThreads / 32;
+constexpr int kChunkMax = 8;     // basis vectors per staged chunk (<= consumer warps)
+constexpr int kRingStages = 4;   // shared-memory stages of the basis stream
+constexpr int kMaxRestart = 256;
+constexpr int kArnMaxCluster = 16;
+
+__device__ __forceinline__ const float2* vrow(const GmPtrs& P, int s, int l) {
+  return P.Vb + ((size_t)s * (P.R + 1) + l) * P.ldv;
+}
+
+// Warp reduce-scatter of NV doubles (NV a power of two, 2..32): afterwards
+// the returned value of lane L is the warp total of value L >> (5 - log2 NV).
+template <int NV>
+__device__ __forceinline__ double warp_reduce_scatter(double (&v)[NV], int lane) {
+#pragma unroll
+  for (int half = NV / 2, off = 16; half >= 1; half >>= 1, off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int j = 0; j < half; j++) {
+      const double send = upper ? v[j] : v[j + half];
+      const double keep = upper ? v[j + half] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
     }
-    P.X[(size_t)i * P.m + s] = v;
-  } else {
-    P.X[(size_t)i * P.m + s] = make_float2(0.f, 0.f);
+  }
+  double t = v[0];
+#pragma unroll
+  for (int off = 16 / NV; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+  return t;
+}
+
+// Matvec operand for unknowns j, j+1 of column s: complex64 X (FP32 matvec)
+// or the bf16 hi/lo B planes of the tensor-core GEMM (rows 2s: (re, -im),
+// 2s+1: (im, re) per unknown, as tc_pack_b_kernel writes them).  x1 is zero
+// when j+1 is the padding entry.
+__device__ __forceinline__ void store_operand(const GmPtrs& P, int j, int s, float2 x0, float2 x1) {
+  if (!P.bh) {
+    P.X[(size_t)j * P.m + s] = x0;
+    if (j + 1 < P.n) P.X[(size_t)(j + 1) * P.m + s] = x1;
+    return;
+  }
+  const float e[2][4] = {{x0.x, -x0.y, x1.x, -x1.y}, {x0.y, x0.x, x1.y, x1.x}};
+#pragma unroll
+  for (int r = 0; r < 2; r++) {
+    __align__(8) __nv_bfloat16 hi[4], lo[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      hi[q] = __float2bfloat16_rn(e[r][q]);
+      lo[q] = __float2bfloat16_rn(e[r][q] - __bfloat162float(hi[q]));
+    }
+    const size_t o = (size_t)(2 * s + r) * P.ldb + 2 * j;
+    *reinterpret_cast<uint2*>(P.bh + o) = *reinterpret_cast<const uint2*>(hi);
+    *reinterpret_cast<uint2*>(P.bl + o) = *reinterpret_cast<const uint2*>(lo);
   }
 }
 
-// w_s = double(Y[:, s]) for active columns (Y is (n, m) row-major; w is
-// column-major, so both Gram-Schmidt passes read contiguous vectors).
-__global__ void gm_y2w_kernel(GmPtrs P) {
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)P.n * P.m) return;
-  const int i = (int)(idx / P.m), s = (int)(idx - (long long)i * P.m);
-  if (!P.active[s]) return;
-  const float2 y = P.Y[idx];
-  P.w[(size_t)s * P.n + i] = make_double2(y.x, y.y);
+struct ArnSmem {
+  uint64_t full[kRingStages];     // bulk-copy completion of each ring stage
+  uint64_t empty[kRingStages];    // consumer warps done with the stage
+  double red[kArnWarps][2 * kChunkMax];
+  double part1[2 * kMaxRestart];  // this CTA's partial h1 (re, im), read by the whole cluster
+  double part2[2 * kMaxRestart];  // partial h2
+  double part3[2];                // partial |w''|^2
+  double2 c1[kMaxRestart];        // cluster totals h1, h2
+  double2 c2[kMaxRestart];
+  double2 hcol[kMaxRestart + 1];  // Givens scratch (CTA 0)
+  double2 snv[kMaxRestart];
+  double csv[kMaxRestart];
+  double hn2;
+  double tol;   // this column's inner tolerance (CTA 0)
+  double2 gk;   // g[k] of this column (CTA 0)
+};
+
+// Row li, unknowns 2p, 2p+1 of a staged chunk; the padding entry of an odd n
+// reads as zero.
+__device__ __forceinline__ float4 staged_pair(const float2* rows, int li, int units, int p, bool pad) {
+  float4 v = *reinterpret_cast<const float4*>(rows + (size_t)li * units + 2 * p);
+  if (pad) {
+    v.z = 0.f;
+    v.w = 0.f;
+  }
+  return v;
 }
 
-// h[pass][s][l] += <V[s][l], w_s> over one chunk of rows, for a group of
-// kDotL basis vectors: every thread keeps 8 rows of w in registers and issues
-// 8 x kDotL independent loads; partial sums reach h through FP64 atomics
-// (h is zeroed at the start of a cycle and after each use).
-constexpr int kDotThreads = 256;
-constexpr int kDotRowsPerThread = 8;
-constexpr int kDotRows = kDotThreads * kDotRowsPerThread;  // 2048
-constexpr int kDotL = 8;
-__global__ void __launch_bounds__(kDotThreads) gm_dots_kernel(GmPtrs P, int pass) {
-  const int s = blockIdx.z;
-  if (!P.active[s]) return;
-  const int k = P.st->k;
-  const int l0 = blockIdx.y * kDotL;
-  if (l0 > k) return;
-  const int nl = min(kDotL, k + 1 - l0);
-  const int row0 = blockIdx.x * kDotRows;
-  double2 src[kDotRowsPerThread];
-#pragma unroll
-  for (int u = 0; u < kDotRowsPerThread; u++) {
-    const int i = row0 + threadIdx.x + u * kDotThreads;
-    src[u] = i < P.n ? P.w[(size_t)s * P.n + i] : make_double2(0.0, 0.0);
+// The basis stream of one launch: every pass reads rows 0..k of this CTA's
+// slice (ucta unknowns from i0) in nch chunks of `chunk` rows; chunk c of
+// pass q is ring position g = q * nch + c, stage g % kRingStages.
+struct ArnStream {
+  const GmPtrs* P;
+  ArnSmem* S;
+  float2* ring;
+  int s, k, i0, ucta, units, chunk, nch;
+  __device__ float2* stage_rows(uint32_t g) const { return ring + (size_t)(g % kRingStages) * chunk * units; }
+  // producer (one thread): wait until the stage is free, then bulk-copy the rows
+  __device__ void produce(int pass, int c) const {
+    const uint32_t g = (uint32_t)(pass * nch + c);
+    const int st = (int)(g % kRingStages);
+    if (g >= (uint32_t)kRingStages) mbar_wait(&S->empty[st], ((g / kRingStages) - 1u) & 1u, &P->st->err);
+    const int l0 = c * chunk, nl = min(chunk, k + 1 - l0);
+    const uint32_t row_bytes = (uint32_t)ucta * 8u;
+    mbar_expect_tx(&S->full[st], row_bytes * (uint32_t)nl);
+    float2* dst = stage_rows(g);
+    for (int li = 0; li < nl; li++)
+      bulk_load(dst + (size_t)li * units, vrow(*P, s, l0 + li) + i0, row_bytes, &S->full[st]);
   }
-  double re[kDotL], im[kDotL];
+  // consumer warps: wait for the chunk's rows
+  __device__ const float2* acquire(int pass, int c) const {
+    const uint32_t g = (uint32_t)(pass * nch + c);
+    if (ucta > 0) mbar_wait(&S->full[g % kRingStages], (g / kRingStages) & 1u, &P->st->err);
+    return stage_rows(g);
+  }
+  // consumer warps: the warp is done with the chunk's stage
+  __device__ void release(int pass, int c) const {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(&S->empty[(uint32_t)(pass * nch + c) % kRingStages]);
+  }
+};
+
+// Dots pass (consumer warps): warp w reduces row l0 + w of each chunk,
+// part[2l + c] = sum over this CTA's unknowns of conj(V[l]) w.
+__device__ __forceinline__ void arn_dots(const ArnStream& T, int pass, const double2* __restrict__ wsl, int npairs,
+                                         double* part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = 0; c < T.nch; c++) {
+    const float2* rows = T.acquire(pass, c);
+    const int l0 = c * T.chunk, nl = min(T.chunk, T.k + 1 - l0);
+    if (warp < nl) {
+      double re = 0.0, im = 0.0;
+      for (int p = lane; p < npairs; p += 32) {
+        const float4 a = staged_pair(rows, warp, T.units, p, T.i0 + 2 * p + 1 >= T.P->n);
+        const double2 w0 = wsl[2 * p], w1 = wsl[2 * p + 1];
+        re += (double)a.x * w0.x + (double)a.y * w0.y + (double)a.z * w1.x + (double)a.w * w1.y;
+        im += (double)a.x * w0.y - (double)a.y * w0.x + (double)a.z * w1.y - (double)a.w * w1.x;
+      }
 #pragma unroll
-  for (int ll = 0; ll < kDotL; ll++) {
-    re[ll] = 0.0;
-    im[ll] = 0.0;
-    if (ll < nl) {
-      const float2* v = P.Vb + ((size_t)s * (P.R + 1) + l0 + ll) * P.n;
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+      }
+      if (lane == 0) {
+        part[2 * (l0 + warp)] = re;
+        part[2 * (l0 + warp) + 1] = im;
+      }
+    }
+    T.release(pass, c);
+  }
+}
+
+// Update pass (consumer threads own pairs): w -= V coef over this CTA's unknowns.
+__device__ __forceinline__ void arn_update(const ArnStream& T, int pass, const double2* __restrict__ coef,
+                                           double2* __restrict__ wsl, int npairs) {
+  for (int c = 0; c < T.nch; c++) {
+    const float2* rows = T.acquire(pass, c);
+    const int l0 = c * T.chunk, nl = min(T.chunk, T.k + 1 - l0);
+    for (int p = threadIdx.x; p < npairs; p += kArnConsumers) {
+      const bool pad = T.i0 + 2 * p + 1 >= T.P->n;
+      double2 a0 = wsl[2 * p], a1 = wsl[2 * p + 1];
 #pragma unroll
-      for (int u = 0; u < kDotRowsPerThread; u++) {
-        const int i = row0 + threadIdx.x + u * kDotThreads;
-        if (i < P.n) {
-          const float2 vv = v[i];
-          re[ll] += (double)vv.x * src[u].x + (double)vv.y * src[u].y;  // conj(v) w
-          im[ll] += (double)vv.x * src[u].y - (double)vv.y * src[u].x;
+      for (int li = 0; li < kChunkMax; li++) {
+        if (li < nl) {
+          const float4 v = staged_pair(rows, li, T.units, p, pad);
+          const double2 cc = coef[l0 + li];
+          a0.x -= (double)v.x * cc.x - (double)v.y * cc.y;
+          a0.y -= (double)v.x * cc.y + (double)v.y * cc.x;
+          a1.x -= (double)v.z * cc.x - (double)v.w * cc.y;
+          a1.y -= (double)v.z * cc.y + (double)v.w * cc.x;
         }
       }
+      wsl[2 * p] = a0;
+      wsl[2 * p + 1] = a1;
     }
-  }
-  __shared__ double red[kDotThreads / 32][kDotL][2];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int ll = 0; ll < kDotL; ll++) {
-    double a = re[ll], b = im[ll];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-    }
-    if (lane == 0) {
-      red[warp][ll][0] = a;
-      red[warp][ll][1] = b;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 2 * nl) {
-    const int ll = threadIdx.x >> 1, c = threadIdx.x & 1;
-    double t = 0.0;
-#pragma unroll
-    for (int w = 0; w < kDotThreads / 32; w++) t += red[w][ll][c];
-    double* h = (double*)(P.h + ((size_t)pass * P.m + s) * (P.R + 1) + l0 + ll);
-    atomicAdd(h + c, t);
+    T.release(pass, c);
   }
 }
 
-// w_s = src_s - sum_{l<=k} V[s][l] h[pass][s][l]; pass 1 also accumulates |w|^2.
-__global__ void gm_update_kernel(GmPtrs P, int pass) {
+// dst[t] = sum over the cluster's CTAs of src[t], t < count (after a cluster barrier).
+__device__ __forceinline__ void cluster_sum(cg::cluster_group& cluster, double* src, double* dst, int count) {
+  const int nb = (int)cluster.num_blocks();
+  for (int t = threadIdx.x; t < count; t += kArnThreads) {
+    double v[kArnMaxCluster];
+#pragma unroll
+    for (int r = 0; r < kArnMaxCluster; r++) v[r] = r < nb ? cluster.map_shared_rank(src, r)[t] : 0.0;
+    double sum = 0.0;
+#pragma unroll
+    for (int r = 0; r < kArnMaxCluster; r++) sum += v[r];
+    dst[t] = sum;
+  }
+}
+
+// One column's step record (one thread per column): the new step index
+// and whether the column is still active, the latter also into the
+// host-mapped ring slot of this launch.
+__device__ __forceinline__ void column_done(const GmPtrs& P, int s, int k_next, bool still_active) {
+  P.kcol[s] = k_next;
+  const int step = P.colstep[s];
+  P.colstep[s] = step + 1;
+  reinterpret_cast<volatile int*>(P.snap)[(step % kSnapRing) * P.m + s] = still_active ? 1 : 0;
+}
+
+// Hessenberg column k of column s (hcol = h1 + h2, hcol[k+1] = hn), the
+// previous rotations applied, the new complex Givens rotation, residual
+// estimate and convergence (one warp; lane 0 applies the rotations, which is
+// inherently sequential).  Returns on every lane whether s stays active.
+__device__ __forceinline__ bool arn_givens(const GmPtrs& P, ArnSmem& S, int s, int k, double hn) {
+  const int lane = threadIdx.x & 31;
+  for (int l = lane; l <= k; l += 32) S.hcol[l] = make_double2(S.c1[l].x + S.c2[l].x, S.c1[l].y + S.c2[l].y);
+  __syncwarp();
+  int still = 0;
+  if (lane == 0) {
+    double2* hc = S.hcol;
+    hc[k + 1] = make_double2(hn, 0.0);
+    for (int l = 0; l < k; l++) {
+      const double c = S.csv[l];
+      const double2 sn = S.snv[l];
+      const double2 a = hc[l], b = hc[l + 1];
+      const double2 sb = cmul(sn, b);
+      const double2 t = cmul(make_double2(-sn.x, sn.y), a);  // -conj(sn) a
+      hc[l] = make_double2(c * a.x + sb.x, c * a.y + sb.y);
+      hc[l + 1] = make_double2(t.x + c * b.x, t.y + c * b.y);
+    }
+    const double2 a = hc[k], b = hc[k + 1];
+    const double na = sqrt(a.x * a.x + a.y * a.y), nb = sqrt(b.x * b.x + b.y * b.y);
+    const double rho = sqrt(na * na + nb * nb);
+    double c;
+    double2 sn;
+    if (rho == 0.0) {
+      c = 1.0;
+      sn = make_double2(0.0, 0.0);
+    } else if (na == 0.0) {
+      c = 0.0;
+      sn = make_double2(b.x / nb, -b.y / nb);  // conj(b)/|b|
+      hc[k] = make_double2(nb, 0.0);
+    } else {
+      c = na / rho;
+      const double2 ph = make_double2(a.x / na, a.y / na);
+      sn = cmul(ph, make_double2(b.x / rho, -b.y / rho));
+      hc[k] = make_double2(ph.x * rho, ph.y * rho);
+    }
+    hc[k + 1] = make_double2(0.0, 0.0);
+    P.cs[s * P.R + k] = c;
+    P.sn[s * P.R + k] = sn;
+    double2* gs = P.g + (size_t)s * (P.R + 1);
+    const double2 gk = S.gk;
+    const double2 gk1 = cmul(make_double2(-sn.x, sn.y), gk);
+    gs[k + 1] = gk1;
+    gs[k] = make_double2(c * gk.x, c * gk.y);
+    const double res = sqrt(gk1.x * gk1.x + gk1.y * gk1.y);
+    P.resid[s] = res;
+    P.kend[s] = k + 1;
+    const bool breakdown = !(hn > 1e-300) || !(hn > 1e-14 * rho);
+    if (res <= S.tol || breakdown || k + 1 >= P.R) {
+      P.active[s] = 0;
+    } else {
+      still = 1;
+    }
+  }
+  __syncwarp();
+  double2* Hk = P.H + ((size_t)s * P.R + k) * (P.R + 1);
+  for (int l = lane; l <= k + 1; l += 32) Hk[l] = S.hcol[l];
+  return __shfl_sync(0xffffffffu, still, 0) != 0;
+}
+
+// Dynamic shared memory of gm_arnoldi_kernel: ArnSmem, the CTA's slice of w
+// (units complex doubles), the ring (kRingStages x chunk x units complex64).
+__host__ __device__ constexpr size_t arn_ring_offset(int units) {
+  return ((sizeof(ArnSmem) + sizeof(double2) * (size_t)units) + 127) / 128 * 128;
+}
+__host__ __device__ constexpr size_t arn_smem_bytes(int units, int chunk) {
+  return arn_ring_offset(units) + sizeof(float2) * (size_t)kRingStages * chunk * units;
+}
+
+// grid (cluster size, m), cluster (cluster size, 1, 1).  reorth != 0 adds the
+// second Gram-Schmidt pass (CGS2); without it the step is classical
+// Gram-Schmidt (enough when a cycle only reduces the residual by ~1e-3 and the
+// basis is stored in complex64).
+__global__ void __launch_bounds__(kArnThreads, 1) gm_arnoldi_kernel(GmPtrs P, int units, int chunk, int reorth) {
+  extern __shared__ __align__(128) unsigned char arn_raw[];
+  ArnSmem& S = *reinterpret_cast<ArnSmem*>(arn_raw);
+  double2* wsl = reinterpret_cast<double2*>(arn_raw + sizeof(ArnSmem));
+  float2* ring = reinterpret_cast<float2*>(arn_raw + arn_ring_offset(units));
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
   const int s = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = P.st->k;
-  if (!P.active[s]) return;
-  __shared__ double2 hs[256];
-  for (int l = threadIdx.x; l <= k; l += blockDim.x) hs[l] = P.h[((size_t)pass * P.m + s) * (P.R + 1) + l];
-  __syncthreads();
-  double n2 = 0.0;
-  if (i < P.n) {
-    double2 acc = P.w[(size_t)s * P.n + i];
-    const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
-    // batches of 8 independent loads, two accumulators
-    double2 acc2 = make_double2(0.0, 0.0);
-    int l = 0;
-    for (; l + 8 <= k + 1; l += 8) {
-      float2 vv[8];
-#pragma unroll
-      for (int u = 0; u < 8; u++) vv[u] = v[(size_t)(l + u) * P.n];
-#pragma unroll
-      for (int u = 0; u < 8; u += 2) {
-        const double2 t0 = cmul(make_double2(vv[u].x, vv[u].y), hs[l + u]);
-        const double2 t1 = cmul(make_double2(vv[u + 1].x, vv[u + 1].y), hs[l + u + 1]);
-        acc.x -= t0.x;
-        acc.y -= t0.y;
-        acc2.x -= t1.x;
-        acc2.y -= t1.y;
-      }
-    }
-    for (; l <= k; l++) {
-      const float2 vv = v[(size_t)l * P.n];
-      const double2 t = cmul(make_double2(vv.x, vv.y), hs[l]);
-      acc.x -= t.x;
-      acc.y -= t.y;
-    }
-    acc.x += acc2.x;
-    acc.y += acc2.y;
-    P.w[(size_t)s * P.n + i] = acc;
-    n2 = acc.x * acc.x + acc.y * acc.y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool producer = warp == kArnConsumerWarps;
+  const int k = P.kcol[s];
+  if (!P.active[s]) {  // uniform over the cluster: nobody waits for this column
+    if (rank == 0 && tid == 0) column_done(P, s, k, false);
+    return;
   }
-  if (pass == 1) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
-    if ((threadIdx.x & 31) == 0 && n2 != 0.0) atomicAdd(&P.norm2[s], n2);
-  }
-}
-
-// Hessenberg column, Givens rotations, residual estimate, convergence.  One
-// warp per column: the lanes stage the new column and the previous rotations
-// in shared memory, lane 0 applies the rotations (inherently sequential); the
-// last block to finish advances k.  One block per kFinWarps columns.
-constexpr int kFinWarps = 4;  // 40 KB of static shared memory
-constexpr int kMaxRestart = 256;
-__global__ void __launch_bounds__(32 * kFinWarps) gm_finalize_kernel(GmPtrs P, int* __restrict__ any_count,
-                                                                     int* __restrict__ done_blocks) {
-  __shared__ double2 hcol[kFinWarps][kMaxRestart + 1];
-  __shared__ double csv[kFinWarps][kMaxRestart];
-  __shared__ double2 snv[kFinWarps][kMaxRestart];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int s = blockIdx.x * kFinWarps + wl;
-  const int k = P.st->k;
-  if (s < P.m && P.active[s] && lane == 0) atomicAdd(&P.st->act_count, 1);
-  if (s < P.m && P.active[s]) {
-    const double2* h0 = P.h + ((size_t)0 * P.m + s) * (P.R + 1);
-    const double2* h1 = P.h + ((size_t)1 * P.m + s) * (P.R + 1);
-    for (int l = lane; l <= k; l += 32) {
-      hcol[wl][l] = make_double2(h0[l].x + h1[l].x, h0[l].y + h1[l].y);
-      if (l < k) {
-        csv[wl][l] = P.cs[s * P.R + l];
-        snv[wl][l] = P.sn[s * P.R + l];
-      }
+  const int i0 = (int)rank * units;
+  const int i1 = min(P.n, i0 + units);
+  const int npairs = i1 > i0 ? (i1 - i0 + 1) / 2 : 0;
+  ArnStream T;
+  T.P = &P;
+  T.S = &S;
+  T.ring = ring;
+  T.s = s;
+  T.k = k;
+  T.i0 = i0;
+  T.ucta = 2 * npairs;
+  T.units = units;
+  T.chunk = chunk;
+  T.nch = (k + chunk) / chunk;
+  if (tid == 0) {
+    for (int st = 0; st < kRingStages; st++) {
+      mbar_init(&S.full[st], 1);
+      mbar_init(&S.empty[st], kArnConsumerWarps);
     }
-    __syncwarp();
-    double2* Hk = P.H + ((size_t)s * P.R + k) * (P.R + 1);
-    const double hn = sqrt(P.norm2[s]);
+    mbar_init_fence();
+  }
+  if (rank == 0 && warp == 0) {  // Givens inputs, loaded while the passes run
+    for (int l = lane; l < k; l += 32) {
+      S.csv[l] = P.cs[s * P.R + l];
+      S.snv[l] = P.sn[s * P.R + l];
+    }
     if (lane == 0) {
-      double2* hc = hcol[wl];
-      hc[k + 1] = make_double2(hn, 0.0);
-      for (int l = 0; l < k; l++) {
-        const double c = csv[wl][l];
-        const double2 sn = snv[wl][l];
-        const double2 a = hc[l], b = hc[l + 1];
-        const double2 sb = cmul(sn, b);
-        const double2 t = cmul(make_double2(-sn.x, sn.y), a);  // -conj(sn) a
-        hc[l] = make_double2(c * a.x + sb.x, c * a.y + sb.y);
-        hc[l + 1] = make_double2(t.x + c * b.x, t.y + c * b.y);
-      }
-      const double2 a = hc[k], b = hc[k + 1];
-      const double na = sqrt(a.x * a.x + a.y * a.y), nb = sqrt(b.x * b.x + b.y * b.y);
-      const double rho = sqrt(na * na + nb * nb);
-      double c;
-      double2 sn;
-      if (rho == 0.0) {
-        c = 1.0;
-        sn = make_double2(0.0, 0.0);
-      } else if (na == 0.0) {
-        c = 0.0;
-        sn = make_double2(b.x / nb, -b.y / nb);  // conj(b)/|b|
-        hc[k] = make_double2(nb, 0.0);
-      } else {
-        c = na / rho;
-        const double2 ph = make_double2(a.x / na, a.y / na);
-        sn = cmul(ph, make_double2(b.x / rho, -b.y / rho));
-        hc[k] = make_double2(ph.x * rho, ph.y * rho);
-      }
-      hc[k + 1] = make_double2(0.0, 0.0);
-      P.cs[s * P.R + k] = c;
-      P.sn[s * P.R + k] = sn;
-      double2* gs = P.g + (size_t)s * (P.R + 1);
-      const double2 gk = gs[k];
-      gs[k + 1] = cmul(make_double2(-sn.x, sn.y), gk);
-      gs[k] = make_double2(c * gk.x, c * gk.y);
-      const double res = sqrt(gs[k + 1].x * gs[k + 1].x + gs[k + 1].y * gs[k + 1].y);
-      P.resid[s] = res;
-      P.kend[s] = k + 1;
-      P.winv[s] = hn > 0.0 ? 1.0 / hn : 0.0;
-      const bool breakdown = !(hn > 1e-300) || !(hn > 1e-14 * rho);
-      if (res <= P.tol[s] || breakdown || k + 1 >= P.R) {
-        P.active[s] = 0;
-      } else {
-        atomicAdd(any_count, 1);
-      }
-    }
-    __syncwarp();
-    for (int l = lane; l <= k + 1; l += 32) Hk[l] = hcol[wl][l];
-    double2* h0w = P.h + ((size_t)0 * P.m + s) * (P.R + 1);
-    double2* h1w = P.h + ((size_t)1 * P.m + s) * (P.R + 1);
-    for (int l = lane; l <= k; l += 32) {
-      h0w[l] = make_double2(0.0, 0.0);
-      h1w[l] = make_double2(0.0, 0.0);
+      S.gk = P.g[(size_t)s * (P.R + 1) + k];
+      S.tol = P.tol[s];
     }
   }
-  if (s < P.m && lane == 0) P.norm2[s] = 0.0;
-  // the last block to finish publishes k + 1 and the activity flag
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const int done = atomicAdd(done_blocks, 1);
-    if (done == (int)gridDim.x - 1) {
-      __threadfence();
-      const int any = atomicAdd(any_count, 0);
-      if (atomicAdd(&P.st->act_count, 0) > 0) P.st->iters_done += 1;
-      P.st->act_count = 0;
-      P.st->k = k + 1;
-      P.st->any_active = any;
-      P.st->skip = any ? 0 : 1;
-      *any_count = 0;
-      *done_blocks = 0;
+
+  // w = Y over this CTA's unknowns; Y = 0 for the next accumulating matvec
+  for (int p = tid; p < npairs; p += kArnThreads) {
+    const int i = i0 + 2 * p;
+    float2* y0 = P.Y + (size_t)i * P.m + s;
+    wsl[2 * p] = make_double2(y0->x, y0->y);
+    *y0 = make_float2(0.f, 0.f);
+    double2 w1 = make_double2(0.0, 0.0);
+    if (i + 1 < P.n) {
+      float2* y1 = P.Y + (size_t)(i + 1) * P.m + s;
+      w1 = make_double2(y1->x, y1->y);
+      *y1 = make_float2(0.f, 0.f);
     }
+    wsl[2 * p + 1] = w1;
+  }
+  __syncthreads();
+
+  // passes: dots h1, update; with reorth also dots h2, update.  The producer
+  // issues each pass's chunks and, before the pass boundary, the first
+  // stages of the next pass (their stages are freed within this pass).
+  const int npass = reorth ? 4 : 2;
+  int first = 0;
+  for (int pass = 0; pass < npass; pass++) {
+    const bool dots = (pass & 1) == 0;
+    double* part = pass == 0 ? S.part1 : S.part2;
+    double2* coef = pass == 1 ? S.c1 : S.c2;
+    if (producer) {
+      if (lane == 0 && T.ucta > 0) {
+        for (int c = first; c < T.nch; c++) T.produce(pass, c);
+        if (pass + 1 < npass)
+          for (int c = 0; c < min(kRingStages, T.nch); c++) T.produce(pass + 1, c);
+      }
+      first = min(kRingStages, T.nch);
+      __syncwarp();
+    } else if (dots) {
+      arn_dots(T, pass, wsl, npairs, part);
+    } else {
+      arn_update(T, pass, coef, wsl, npairs);
+    }
+    if (dots) {
+      cluster.sync();
+      cluster_sum(cluster, part, reinterpret_cast<double*>(pass == 0 ? S.c1 : S.c2), 2 * (k + 1));
+    }
+    __syncthreads();
+  }
+  if (!reorth)
+    for (int t = tid; t <= k; t += kArnThreads) S.c2[t] = make_double2(0.0, 0.0);
+  if (npairs > 0 && *(volatile int*)&P.st->err && producer && lane == 0) {
+    // a wait expired: let the copies of the last chunks land before leaving
+    const uint32_t gc = (uint32_t)(npass * T.nch);
+    for (uint32_t g = gc > kRingStages ? gc - kRingStages : 0; g < gc; g++)
+      mbar_wait_drain(&S.full[g % kRingStages], (g / kRingStages) & 1u);
+  }
+  double n2 = 0.0;
+  for (int p = tid; p < npairs; p += kArnThreads) {
+    const double2 a0 = wsl[2 * p], a1 = wsl[2 * p + 1];
+    n2 += a0.x * a0.x + a0.y * a0.y + a1.x * a1.x + a1.y * a1.y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+  if (lane == 0) S.red[warp][0] = n2;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kArnWarps; w++) t += S.red[w][0];
+    S.part3[0] = t;
+  }
+  cluster.sync();
+  if (tid == 0) {
+    double t = 0.0;
+    for (unsigned r = 0; r < cluster.num_blocks(); r++) t += cluster.map_shared_rank(S.part3, r)[0];
+    S.hn2 = t;
+  }
+  cluster.sync();  // remote reads done before any CTA leaves; publishes hn2 in the CTA
+  const double hn = sqrt(S.hn2);
+  const double inv = hn > 0.0 ? 1.0 / hn : 0.0;
+
+  // v_{k+1} and the next matvec operand
+  float2* vk1 = P.Vb + ((size_t)s * (P.R + 1) + k + 1) * P.ldv;
+  for (int p = tid; p < npairs; p += kArnThreads) {
+    const int i = i0 + 2 * p;
+    const double2 a0 = wsl[2 * p], a1 = wsl[2 * p + 1];
+    const float2 f0 = make_float2((float)(a0.x * inv), (float)(a0.y * inv));
+    const float2 f1 = i + 1 < P.n ? make_float2((float)(a1.x * inv), (float)(a1.y * inv)) : make_float2(0.f, 0.f);
+    *reinterpret_cast<float4*>(vk1 + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+    store_operand(P, i, s, f0, f1);
+  }
+  if (rank == 0 && warp == 0) {
+    const bool still = arn_givens(P, S, s, k, hn);
+    if (lane == 0) column_done(P, s, k + 1, still);
   }
 }
 
@@ -501,9 +699,9 @@ __global__ void gm_xupdate_kernel(GmPtrs P) {
   const int kk = P.kend[s];
   const double2* y = (const double2*)(P.y) + (size_t)s * P.R;
   double2 acc = P.d[(size_t)s * P.n + i];
-  const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.n + i;
+  const float2* v = P.Vb + (size_t)s * (P.R + 1) * P.ldv + i;
   for (int l = 0; l < kk; l++) {
-    const float2 vv = v[(size_t)l * P.n];
+    const float2 vv = v[(size_t)l * P.ldv];
     const double2 t = cmul(make_double2(vv.x, vv.y), y[l]);
     acc.x += t.x;
     acc.y += t.y;
@@ -533,9 +731,6 @@ __global__ void gm_start_vec_kernel(GmPtrs P, int use_y) {
 __global__ void gm_start_scalar_kernel(GmPtrs P, const double* __restrict__ outer_norm2, double inner_rtol,
                                        double floor_abs_rtol) {
   const int s = threadIdx.x;
-  __shared__ int any;
-  if (s == 0) any = 0;
-  __syncthreads();
   if (s < P.m) {
     const double beta = sqrt(P.norm2[s]);
     P.beta[s] = beta;
@@ -546,28 +741,26 @@ __global__ void gm_start_scalar_kernel(GmPtrs P, const double* __restrict__ oute
     gs[0] = make_double2(beta, 0.0);
     P.kend[s] = 0;
     P.resid[s] = beta;
-    const int act = beta > target && beta > 0.0;
-    P.active[s] = act;
-    if (act) atomicAdd(&any, 1);
+    P.active[s] = beta > target && beta > 0.0;
+    P.kcol[s] = 0;
     P.norm2[s] = 0.0;
-  }
-  __syncthreads();
-  if (s == 0) {
-    P.st->k = 0;
-    P.st->any_active = any;
-    P.st->skip = any ? 0 : 1;
   }
 }
 
-// V[s][0] = w_s / beta_s
-__global__ void gm_start_norm_kernel(GmPtrs P) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// V[s][0] = w_s / beta_s and the first matvec operand; two unknowns per thread
+constexpr int kPairThreads = 256;
+__global__ void __launch_bounds__(kPairThreads) gm_start_norm_kernel(GmPtrs P) {
+  const int i = blockIdx.x * 2 * kPairThreads + 2 * threadIdx.x;
   const int s = blockIdx.y;
   if (i >= P.n) return;
   const double b = P.beta[s];
   const double inv = b > 0.0 ? 1.0 / b : 0.0;
-  const double2 w = P.w[(size_t)s * P.n + i];
-  P.Vb[(size_t)s * (P.R + 1) * P.n + i] = make_float2((float)(w.x * inv), (float)(w.y * inv));
+  const double2 w0 = P.w[(size_t)s * P.n + i];
+  const double2 w1 = i + 1 < P.n ? P.w[(size_t)s * P.n + i + 1] : make_double2(0.0, 0.0);
+  const float2 f0 = make_float2((float)(w0.x * inv), (float)(w0.y * inv));
+  const float2 f1 = make_float2((float)(w1.x * inv), (float)(w1.y * inv));
+  *reinterpret_cast<float4*>(P.Vb + (size_t)s * (P.R + 1) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+  store_operand(P, i, s, f0, f1);
 }
 
 // X = float(d) (for r_out - A_lp d), or X = 0
@@ -643,8 +836,8 @@ __global__ void gm_store_x_kernel(GmPtrs P, float2* __restrict__ X) {
 inline size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
 struct Layout {
-  size_t Vb, H, cs, sn, g, h, w, d, x, r, X, Y, norm2, winv, rnorm2, beta, tol, resid, active, kend, y, st, bnorm2, tc,
-      total;
+  size_t Vb, H, cs, sn, g, w, d, x, r, X, Y, norm2, rnorm2, beta, tol, resid, active, kend, kcol, colstep, y, st,
+      bnorm2, tc, total;
 };
 
 Layout layout(int n, int m, int R, int precision) {
@@ -656,12 +849,11 @@ Layout layout(int n, int m, int R, int precision) {
     return r;
   };
   L.st = take(sizeof(GmState));
-  L.Vb = take(sizeof(float2) * (size_t)m * (R + 1) * n);
+  L.Vb = take(sizeof(float2) * (size_t)m * (R + 1) * (size_t)((n + 1) & ~1));
   L.H = take(sizeof(double2) * (size_t)m * R * (R + 1));
   L.cs = take(sizeof(double) * (size_t)m * R);
   L.sn = take(sizeof(double2) * (size_t)m * R);
   L.g = take(sizeof(double2) * (size_t)m * (R + 1));
-  L.h = take(sizeof(double2) * 2 * (size_t)m * (R + 1));
   L.w = take(sizeof(double2) * (size_t)m * n);
   L.d = take(sizeof(double2) * (size_t)m * n);
   L.x = take(sizeof(double2) * (size_t)m * n);
@@ -669,13 +861,14 @@ Layout layout(int n, int m, int R, int precision) {
   L.X = take(sizeof(float2) * (size_t)m * n);
   L.Y = take(sizeof(float2) * (size_t)m * n);
   L.norm2 = take(sizeof(double) * m);
-  L.winv = take(sizeof(double) * m);
   L.rnorm2 = take(sizeof(double) * m);
   L.beta = take(sizeof(double) * m);
   L.tol = take(sizeof(double) * m);
   L.resid = take(sizeof(double) * m);
   L.active = take(sizeof(int) * m);
   L.kend = take(sizeof(int) * m);
+  L.kcol = take(sizeof(int) * m);
+  L.colstep = take(sizeof(int) * m);
   L.y = take(sizeof(double2) * (size_t)m * R);
   L.bnorm2 = take(sizeof(double) * m);
   L.tc = take(precision == BEM_PREC_FP32 ? 0 : tc_workspace_bytes(n, m, precision));
@@ -688,16 +881,19 @@ bool params_ok(const bem_solver_params* p) {
          (p->precision == BEM_PREC_FP32 || p->precision == BEM_PREC_BF16X3 || p->precision == BEM_PREC_BF16);
 }
 
-// Pinned host snapshots of the solver state, one per Arnoldi step in a ring,
-// each with an event.  The host runs at most kLookahead steps ahead of the
-// GPU: it blocks on the event of step it - kLookahead (the GPU still has that
-// many steps queued) and stops enqueueing once a snapshot shows every column
-// converged, so at most kLookahead no-op steps follow convergence.
-constexpr int kRing = 8;
+// Per-step column activity in host-mapped pinned memory (kSnapRing slots of
+// m ints, written by the Arnoldi kernel) and one event per slot.  The host
+// runs at most kLookahead steps ahead of the GPU: before enqueueing step
+// j + kLookahead + 1 it waits for the event of step j and reads its slot, and
+// it stops enqueueing once a slot shows every column converged, so at most
+// kLookahead no-op steps follow convergence.  No copy is enqueued per step.
 constexpr int kLookahead = 4;
+static_assert(kLookahead < kSnapRing, "a slot is read before it is reused");
 struct HostRing {
-  GmState* snap = nullptr;
-  cudaEvent_t ev[kRing] = {};
+  int* snap = nullptr;  // [kSnapRing][cap] host view
+  int* dsnap = nullptr;  // device view
+  int cap = 0;
+  cudaEvent_t ev[kSnapRing] = {};
   ~HostRing() {
     if (snap) cudaFreeHost(snap);
     for (auto& e : ev)
@@ -730,13 +926,72 @@ int capture_graph(const std::function<int(cudaStream_t)>& body, cudaGraphExec_t*
   return BEM_OK;
 }
 
-int host_ring(HostRing** r) {
-  if (!t_ring.snap) {
-    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_ring.snap, sizeof(GmState) * kRing, cudaHostAllocDefault));
+int host_ring(int m, HostRing** r) {
+  if (!t_ring.ev[0])
     for (auto& e : t_ring.ev) BEM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (t_ring.cap < m) {
+    if (t_ring.snap) cudaFreeHost(t_ring.snap);
+    t_ring.snap = nullptr;
+    t_ring.cap = 0;
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_ring.snap, sizeof(int) * kSnapRing * (size_t)m, cudaHostAllocMapped));
+    BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_ring.dsnap, t_ring.snap, 0));
+    t_ring.cap = m;
   }
   *r = &t_ring;
   return BEM_OK;
+}
+
+// Launch shape of gm_arnoldi_kernel for n unknowns: the smallest
+// power-of-two cluster (<= 16 CTAs) whose CTAs hold at most 768 unknowns
+// each, widened while the w slice would not fit in shared memory; checked
+// against the device with cudaOccupancyMaxActiveClusters.
+struct ArnShape {
+  int cluster = 1;
+  int units = 0;
+  int chunk = 0;
+  size_t smem = 0;
+};
+
+int arnoldi_shape(int n, ArnShape* out) {
+  static std::atomic<bool> attr{false};
+  int dev = 0, smem_optin = 0;
+  BEM_CUDA_TRY(cudaGetDevice(&dev));
+  BEM_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_arnoldi_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_arnoldi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+    attr.store(true, std::memory_order_release);
+  }
+  int cl = 1;
+  while (cl < kArnMaxCluster && (long long)cl * 2 * kArnThreads < n) cl *= 2;
+  for (; cl >= 1; cl /= 2) {
+    const int units = (((n + cl - 1) / cl) + 1) & ~1;
+    int chunk = kChunkMax;
+    while (chunk > 1 && arn_smem_bytes(units, chunk) > (size_t)smem_optin) chunk--;
+    const size_t smem = arn_smem_bytes(units, chunk);
+    if (smem > (size_t)smem_optin) break;  // smaller clusters need even more
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cl, 1, 1);
+    cfg.blockDim = dim3(kArnThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, gm_arnoldi_kernel, &cfg) == cudaSuccess && nclusters > 0) {
+      out->cluster = cl;
+      out->units = units;
+      out->chunk = chunk;
+      out->smem = smem;
+      return BEM_OK;
+    }
+    cudaGetLastError();
+  }
+  return BEM_ERR_UNSUPPORTED;
 }
 
 }  // namespace
@@ -781,7 +1036,6 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   P.cs = (double*)(w + L.cs);
   P.sn = (double2*)(w + L.sn);
   P.g = (double2*)(w + L.g);
-  P.h = (double2*)(w + L.h);
   P.w = (double2*)(w + L.w);
   P.d = (double2*)(w + L.d);
   P.x = (double2*)(w + L.x);
@@ -789,12 +1043,17 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   P.X = (float2*)(w + L.X);
   P.Y = (float2*)(w + L.Y);
   P.norm2 = (double*)(w + L.norm2);
-  P.winv = (double*)(w + L.winv);
+  P.ldv = (n + 1) & ~1;
+  P.bh = nullptr;
+  P.bl = nullptr;
+  P.ldb = 0;
   P.beta = (double*)(w + L.beta);
   P.tol = (double*)(w + L.tol);
   P.resid = (double*)(w + L.resid);
   P.active = (int*)(w + L.active);
   P.kend = (int*)(w + L.kend);
+  P.kcol = (int*)(w + L.kcol);
+  P.colstep = (int*)(w + L.colstep);
   P.y = (double*)(w + L.y);
   P.st = (GmState*)(w + L.st);
   P.bnorm2 = (double*)(w + L.bnorm2);
@@ -804,28 +1063,53 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   if (prec != BEM_PREC_FP32) {
     int rc = tc_operator_prepare((const float2*)A, n, prec, tcws, s);
     if (rc) return rc;
+    int nb = 0;
+    if ((rc = tc_b_planes(tcws, n, m, prec, &P.bh, &P.bl, &P.ldb, &nb))) return rc;
+    // rows 2m..nb-1 of the B planes stay zero; the step kernels write rows < 2m
+    BEM_CUDA_TRY(cudaMemsetAsync(P.bh, 0, sizeof(__nv_bfloat16) * (size_t)nb * P.ldb, s));
+    BEM_CUDA_TRY(cudaMemsetAsync(P.bl, 0, sizeof(__nv_bfloat16) * (size_t)nb * P.ldb, s));
+  } else {
+    BEM_CUDA_TRY(cudaMemsetAsync(P.X, 0, sizeof(float2) * (size_t)n * m, s));
   }
   auto inner_matvec_on = [&](cudaStream_t st) -> int {
     if (prec == BEM_PREC_FP32)
-      return launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, &P.st->skip, st);
-    return tc_matvec(tcws, n, prec, P.X, m, P.Y, &P.st->skip, st);
+      return launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, nullptr, st);
+    return tc_matvec(tcws, n, prec, P.X, m, P.Y, nullptr, st);
   };
   auto inner_matvec = [&]() -> int { return inner_matvec_on(s); };
 
   const dim3 gv((n + 255) / 256, m);
-  const dim3 dots_grid((n + kDotRows - 1) / kDotRows, (R + 1 + kDotL - 1) / kDotL, m);
+  const dim3 pair_grid((n + 2 * kPairThreads - 1) / (2 * kPairThreads), m);
+  // re-orthogonalise (CGS2) when a cycle has to reach the full tolerance;
+  // the mixed-precision inner cycles only reduce the residual by inner_rtol
+  const int reorth = (prec == BEM_PREC_FP32 || params->inner_rtol < 1e-4) ? 1 : 0;
+  ArnShape shape;
+  {
+    int rc0 = arnoldi_shape(n, &shape);
+    if (rc0) return rc0;
+  }
+  // one Arnoldi step: the matvec reads the operand that gm_arnoldi_kernel (or
+  // gm_start_norm_kernel) wrote and accumulates into Y, which
+  // gm_arnoldi_kernel clears again after reading it
   auto arnoldi_step = [&](cudaStream_t st) -> int {
-    (gm_pack_kernel<<<gv, 256, 0, st>>>(P), count_launch());
-    int r2 = inner_matvec_on(st);
+    int r2 = prec == BEM_PREC_FP32
+                 ? launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, P.active, st)
+                 : tc_gemm(tcws, n, prec, m, P.Y, P.active, st);
     if (r2) return r2;
-    (gm_y2w_kernel<<<(unsigned)(((long long)n * m + 255) / 256), 256, 0, st>>>(P), count_launch());
-    (gm_dots_kernel<<<dots_grid, kDotThreads, 0, st>>>(P, 0), count_launch());
-    (gm_update_kernel<<<gv, 256, 0, st>>>(P, 0), count_launch());
-    (gm_dots_kernel<<<dots_grid, kDotThreads, 0, st>>>(P, 1), count_launch());
-    (gm_update_kernel<<<gv, 256, 0, st>>>(P, 1), count_launch());
-    (gm_finalize_kernel<<<(m + kFinWarps - 1) / kFinWarps, 32 * kFinWarps, 0, st>>>(P, &P.st->any_count,
-                                                                                   &P.st->done_blocks),
-     count_launch());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)shape.cluster, (unsigned)m, 1);
+    cfg.blockDim = dim3(kArnThreads, 1, 1);
+    cfg.dynamicSmemBytes = shape.smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)shape.cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_arnoldi_kernel, P, shape.units, shape.chunk, reorth));
+    count_launch();
     BEM_CUDA_TRY(cudaGetLastError());
     return BEM_OK;
   };
@@ -833,18 +1117,21 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   unsigned long long step_kernels = 0;
   bool step_direct_done = false;  // the first step runs uncaptured (sets kernel attributes)
   HostRing* ring;
-  int rc = host_ring(&ring);
+  int rc = host_ring(m, &ring);
   if (rc) return rc;
+  P.snap = ring->dsnap;
   std::vector<double> hres(m), hb(m);
 
   BEM_CUDA_TRY(cudaMemsetAsync(P.st, 0, sizeof(GmState), s));
+  BEM_CUDA_TRY(cudaMemsetAsync(P.colstep, 0, sizeof(int) * m, s));
   BEM_CUDA_TRY(cudaMemsetAsync(P.bnorm2, 0, sizeof(double) * m, s));
   BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
   (gm_bnorm_kernel<<<gv, 256, 0, s>>>(P, (const float2*)B), count_launch());
   (gm_init_x_kernel<<<gv, 256, 0, s>>>(P, (const float2*)X, use_x0), count_launch());
   BEM_CUDA_TRY(cudaMemcpyAsync(hb.data(), P.bnorm2, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
 
-  int total_iters = 0, matvecs = 0, refinements = 0;
+  int total_iters = 0, matvecs = 0, refinements = 0, iters_done = 0;
+  long long launched = 0;  // Arnoldi launches in this solve (snapshot slot = launched % kSnapRing)
   double max_rel = 0.0;
   int status = BEM_ERR_NOT_CONVERGED;
   bool x_nonzero = use_x0 != 0;
@@ -889,18 +1176,31 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
       if (!first_cycle) {
         (gm_pack_d_kernel<<<gv, 256, 0, s>>>(P), count_launch());
-        BEM_CUDA_TRY(cudaMemsetAsync(&P.st->skip, 0, sizeof(int), s));
         if ((rc = inner_matvec())) return rc;
         matvecs++;
       }
-      BEM_CUDA_TRY(cudaMemsetAsync(P.h, 0, sizeof(double2) * 2 * (size_t)m * (R + 1), s));
       (gm_start_vec_kernel<<<gv, 256, 0, s>>>(P, first_cycle ? 0 : 1), count_launch());
       // absolute inner target: inner_rtol * ||r_out|| but never below rtol * ||b|| / 2
       (gm_start_scalar_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P, rnorm2, inner_rtol, 0.5 * params->rtol), count_launch());
-      (gm_start_norm_kernel<<<gv, 256, 0, s>>>(P), count_launch());
+      BEM_CUDA_TRY(cudaMemsetAsync(P.Y, 0, sizeof(float2) * (size_t)n * m, s));
+      (gm_start_norm_kernel<<<pair_grid, kPairThreads, 0, s>>>(P), count_launch());
       first_cycle = false;
-      int it = 0;
+      int it = 0, checked = 0;
       bool cycle_done = false;
+      const long long base = launched;
+      // step j of the cycle ran with at least one active column unless an
+      // earlier step's slot already showed all converged
+      auto examine = [&](int j) -> int {
+        const int slot = (int)((base + j) % kSnapRing);
+        BEM_CUDA_TRY(cudaEventSynchronize(ring->ev[slot]));
+        if (!cycle_done) {
+          iters_done++;
+          bool any = false;
+          for (int c = 0; c < m; c++) any |= ring->snap[(size_t)slot * m + c] != 0;
+          if (!any) cycle_done = true;
+        }
+        return BEM_OK;
+      };
       while (it < R && total_iters < params->max_iters) {
         if (!step_direct_done || !step_exec) {
           if ((rc = arnoldi_step(s))) return rc;
@@ -912,17 +1212,17 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
           BEM_CUDA_TRY(cudaGraphLaunch(step_exec, s));
           count_launches(step_kernels);
         }
-        BEM_CUDA_TRY(cudaMemcpyAsync(&ring->snap[it % kRing], P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));
-        BEM_CUDA_TRY(cudaEventRecord(ring->ev[it % kRing], s));
+        BEM_CUDA_TRY(cudaEventRecord(ring->ev[launched % kSnapRing], s));
+        launched++;
         it++;
         total_iters++;
-        if (it > kLookahead) {
-          const int old = (it - 1 - kLookahead) % kRing;
-          BEM_CUDA_TRY(cudaEventSynchronize(ring->ev[old]));
-          if (ring->snap[old].any_active == 0) cycle_done = true;
+        while (checked < it - kLookahead) {
+          if ((rc = examine(checked++))) return rc;
         }
         if (cycle_done) break;
       }
+      while (checked < it)
+        if ((rc = examine(checked++))) return rc;
       (gm_solve_kernel<<<(m + kSolveWarps - 1) / kSolveWarps, 32 * kSolveWarps, 0, s>>>(P), count_launch());
       (gm_xupdate_kernel<<<gv, 256, 0, s>>>(P), count_launch());
       // converged when no column is active at the end of the cycle with
@@ -948,12 +1248,14 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   }
   if (step_exec) cudaGraphExecDestroy(step_exec);
   GmState fin;
-  BEM_CUDA_TRY(cudaMemcpy(&fin, P.st, sizeof(GmState), cudaMemcpyDeviceToHost));
-  (void)total_iters;  // steps enqueued; fin.iters_done counts the executed ones
-  matvecs += fin.iters_done;
+  BEM_CUDA_TRY(cudaMemcpyAsync(&fin, P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (fin.err) status = BEM_ERR_CUDA;  // a bounded wait in gm_arnoldi_kernel expired
+  (void)total_iters;  // steps enqueued; iters_done counts those with an active column
+  matvecs += iters_done;
   if (info) {
     info->status = status;
-    info->iterations = fin.iters_done;
+    info->iterations = iters_done;
     info->refinements = refinements;
     info->matvecs = matvecs;
     info->rel_residual = max_rel;

@@ -27,6 +27,7 @@
 
 #include <cstring>
 
+#include "async_copy.cuh"
 #include "bem_common.cuh"
 
 namespace bemb {
@@ -37,8 +38,6 @@ constexpr int kBM = 128;            // rows per tile (UMMA M)
 constexpr int kBK = 64;             // K elements per stage: one 128-byte swizzle row
 constexpr int kTcThreads = 192;     // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2..5 epilogue
 constexpr int kSmemBudget = 200 * 1024;
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
-
 struct TcArgs {
   int n;          // matrix order
   int n_rb;       // row blocks
@@ -46,61 +45,10 @@ struct TcArgs {
   long long units;  // n_rb * n_kb
   int m2;         // 2 * (right-hand sides), valid D columns
   float* Y;       // (n, m2) fp32 = (n, m) complex64
-  const int* skip;  // nonzero: nothing to do (all Krylov columns converged)
+  const int* active;  // if set: nothing to do unless some active[c] != 0, c < nact
+  int nact;
   int* err;       // set to 1 when a wait expired
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: false (and the error flag raised) if the phase did not
-// complete within kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer();
-  for (uint32_t it = 0;; it++) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0u) {
-      if (*(volatile int*)err) return false;
-      if (globaltimer() - t0 > kWaitLimitNs) {
-        atomicExch(err, 1);
-        return false;
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
 
 // 2-D tiled TMA load (no multicast) completing on `bar`.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
@@ -190,7 +138,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                    const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, TcArgs p) {
   using S = TcSmem<NB, X3>;
-  if (*p.skip) return;  // uniform: every thread reads the same flag
+  if (p.active) {  // uniform: every thread reads the same flags
+    int any = 0;
+    for (int c = 0; c < p.nact; c++) any |= p.active[c];
+    if (!any) return;
+  }
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* bars = (uint64_t*)(base + S::kStages * S::kStageBytes);
@@ -439,7 +391,7 @@ TcLayout tc_layout(int n, int m, int precision) {
 }
 
 template <int NB, bool X3>
-int launch_tc(const TcLayout& L, char* ws, int n, const int* skip, float* Y, int m2, cudaStream_t s) {
+int launch_tc(const TcLayout& L, char* ws, int n, const int* active, int nact, float* Y, int m2, cudaStream_t s) {
   using S = TcSmem<NB, X3>;
   static std::atomic<bool> attr{false};
   if (!attr.load(std::memory_order_acquire)) {
@@ -460,7 +412,8 @@ int launch_tc(const TcLayout& L, char* ws, int n, const int* skip, float* Y, int
   a.m2 = m2;
   a.Y = Y;
   a.err = (int*)(ws + L.hdr);
-  a.skip = skip ? skip : (const int*)(ws + L.hdr + 4);  // header word 1 stays zero
+  a.active = active;
+  a.nact = nact;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -488,9 +441,11 @@ int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStr
   return BEM_OK;
 }
 
-// Y = A X for m <= 128 right-hand sides; `skip` (device int, may be NULL)
-// turns the launch into a no-op when nonzero.
-int tc_matvec(const void* ws_, int n, int precision, const float2* X, int m, float2* Y, const int* skip,
+int tc_gemm(const void* ws_, int n, int precision, int m, float2* Y, const int* active, cudaStream_t s);
+
+// Y = A X for m <= 128 right-hand sides; `active` (device ints, one per
+// right-hand side, may be NULL) turns the launch into a no-op when all are 0.
+int tc_matvec(const void* ws_, int n, int precision, const float2* X, int m, float2* Y, const int* active,
               cudaStream_t s) {
   if (m <= 0 || m > 128) return BEM_ERR_UNSUPPORTED;
   char* ws = (char*)ws_;
@@ -499,14 +454,37 @@ int tc_matvec(const void* ws_, int n, int precision, const float2* X, int m, flo
                                          (__nv_bfloat16*)(ws + L.bl)),
    count_launch());
   BEM_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)n * m, s));
+  return tc_gemm(ws_, n, precision, m, Y, active, s);
+}
+
+// B operand planes, for producers that write them directly: element (j, s)
+// of X occupies columns 2j, 2j+1 of rows 2s, 2s+1 (row stride ldb), as
+// written by tc_pack_b_kernel.  Rows 2m..nb-1 must be zero.
+int tc_b_planes(void* ws_, int n, int m, int precision, __nv_bfloat16** bh, __nv_bfloat16** bl, int* ldb,
+                int* nb) {
+  if (m <= 0 || m > 128) return BEM_ERR_UNSUPPORTED;
+  char* ws = (char*)ws_;
+  const TcLayout L = tc_layout(n, m, precision);
+  *bh = (__nv_bfloat16*)(ws + L.bh);
+  *bl = (__nv_bfloat16*)(ws + L.bl);
+  *ldb = L.ld;
+  *nb = L.nb;
+  return BEM_OK;
+}
+
+// Y += A_lp B with the B planes already in the workspace.
+int tc_gemm(const void* ws_, int n, int precision, int m, float2* Y, const int* active, cudaStream_t s) {
+  if (m <= 0 || m > 128) return BEM_ERR_UNSUPPORTED;
+  char* ws = (char*)ws_;
+  const TcLayout L = tc_layout(n, m, precision);
   const bool x3 = precision == BEM_PREC_BF16X3;
   float* y = (float*)Y;
   switch (L.nb) {
-    case 16: return x3 ? launch_tc<16, true>(L, ws, n, skip, y, 2 * m, s) : launch_tc<16, false>(L, ws, n, skip, y, 2 * m, s);
-    case 32: return x3 ? launch_tc<32, true>(L, ws, n, skip, y, 2 * m, s) : launch_tc<32, false>(L, ws, n, skip, y, 2 * m, s);
-    case 64: return x3 ? launch_tc<64, true>(L, ws, n, skip, y, 2 * m, s) : launch_tc<64, false>(L, ws, n, skip, y, 2 * m, s);
-    case 128: return x3 ? launch_tc<128, true>(L, ws, n, skip, y, 2 * m, s) : launch_tc<128, false>(L, ws, n, skip, y, 2 * m, s);
-    default: return x3 ? launch_tc<256, true>(L, ws, n, skip, y, 2 * m, s) : launch_tc<256, false>(L, ws, n, skip, y, 2 * m, s);
+    case 16: return x3 ? launch_tc<16, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<16, false>(L, ws, n, active, m, y, 2 * m, s);
+    case 32: return x3 ? launch_tc<32, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<32, false>(L, ws, n, active, m, y, 2 * m, s);
+    case 64: return x3 ? launch_tc<64, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<64, false>(L, ws, n, active, m, y, 2 * m, s);
+    case 128: return x3 ? launch_tc<128, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<128, false>(L, ws, n, active, m, y, 2 * m, s);
+    default: return x3 ? launch_tc<256, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<256, false>(L, ws, n, active, m, y, 2 * m, s);
   }
 }
 
