@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3", "bf16"])
+    ap.add_argument("--precision", default="fp16x3", choices=["fp32", "bf16x3", "bf16", "fp16x3"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--validate", action="store_true", help="also compare against the FP64 oracle (minutes)")

@@ -135,7 +135,9 @@ int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, floa
  * (0 = automatic).  Process-wide. */
 enum {
   BEM_TUNE_ASSEMBLY_CHUNK = 1,      /* trial tiles (16 triangles) per work item */
-  BEM_TUNE_ASSEMBLY_CTAS_PER_SM = 2 /* persistent CTAs per SM (<= occupancy limit) */
+  BEM_TUNE_ASSEMBLY_CTAS_PER_SM = 2, /* persistent CTAs per SM (<= occupancy limit) */
+  BEM_TUNE_TC_PROMOTE = 3            /* tensor-core matvec: K blocks (64 reals) accumulated in tensor
+                                        memory before the partial sum leaves it (0: automatic) */
 };
 int bem_set_tuning(int key, int value);
 int bem_get_tuning(int key);
@@ -214,7 +216,9 @@ int bem_vertex_gradient(const void* geom, float k, const void* lambda, const voi
 enum {
   BEM_PREC_FP32 = 0,   /* complex64 CUDA-core matvec */
   BEM_PREC_BF16X3 = 1, /* tensor-core bf16 hi/lo split (3 products), FP32 accumulate */
-  BEM_PREC_BF16 = 2    /* tensor-core bf16 (1 product), FP32 accumulate */
+  BEM_PREC_BF16 = 2,   /* tensor-core bf16 (1 product), FP32 accumulate */
+  BEM_PREC_FP16X3 = 3  /* tensor-core fp16 hi/lo split with power-of-two row / column scales
+                          (3 products): FP32-level accuracy at the bytes of BF16X3 */
 };
 
 typedef struct bem_solver_params {
@@ -239,7 +243,8 @@ typedef struct bem_solver_info {
  * planes once (bem_tc_operator_prepare), after which bem_tc_matmul computes
  * Y = A X for m <= 128 right-hand sides with FP32 accumulation in tensor
  * memory.  precision: BEM_PREC_BF16X3 (A and X split hi/lo, three products)
- * or BEM_PREC_BF16 (A in bf16, X split, two products).  No counterpart in the
+ * BEM_PREC_BF16 (A in bf16, X split, two products) or BEM_PREC_FP16X3 (fp16
+ * hi/lo splits with power-of-two scales, three products).  No counterpart in the
  * reference (it multiplies with cuBLAS through torch). */
 size_t bem_tc_operator_bytes(int n, int m, int precision);
 int bem_tc_operator_prepare(const void* A, int n, int precision, void* workspace, size_t workspace_bytes,

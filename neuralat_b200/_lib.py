@@ -27,7 +27,7 @@ BEM_ERR_UNSUPPORTED = 9
 # layers and orders
 SINGLE_LAYER, DOUBLE_LAYER, ADJOINT_DOUBLE_LAYER, HYPERSINGULAR, BM_LHS, BM_RHS = range(6)
 ORDER_EXACT, ORDER_APPROX, ORDER_APPROX_1 = range(3)
-PREC_FP32, PREC_BF16X3, PREC_BF16 = range(3)
+PREC_FP32, PREC_BF16X3, PREC_BF16, PREC_FP16X3 = range(4)
 
 # every symbol include/bem_b200.h declares
 EXPORTED = (
@@ -50,7 +50,7 @@ class BEMError(RuntimeError):
         super().__init__(f"{what}: {msg} (status {self.status})" if what else f"{msg} (status {self.status})")
 
 
-TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM = 1, 2
+TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE = 1, 2, 3
 
 
 class BatchProblem(ctypes.Structure):

@@ -88,7 +88,7 @@ class _ListenerPressure(torch.autograd.Function):
 
 
 def listener_pressure(vertices: torch.Tensor, neumann: torch.Tensor, triangles: torch.Tensor, points: torch.Tensor,
-                      k: float, *, precision: str = "bf16x3", rtol: float = 1e-7, store_matrices: bool = True):
+                      k: float, *, precision: str = "fp16x3", rtol: float = 1e-7, store_matrices: bool = True):
     """Listener pressures (P,) complex64, differentiable w.r.t. ``vertices``
     (float32 (N,3)) and ``neumann`` (complex64 (N,))."""
     return _ListenerPressure.apply(vertices, neumann, triangles, points, float(k), precision, rtol, store_matrices)

@@ -61,7 +61,7 @@ def assemble_batch(solvers, ks, mass_coeff=0.5, k_coeff=-1.0, stream=None):
     return outs
 
 
-def problem_bytes(nv: int, m: int, restart: int = 120) -> int:
+def problem_bytes(nv: int, m: int, restart: int = 200) -> int:
     """Device bytes one problem holds while it is solved (V, LHS, tensor-core
     planes, Krylov basis and vectors)."""
     return 3 * 8 * nv * nv + 8 * m * (restart + 1) * nv + 64 * m * nv
@@ -70,8 +70,8 @@ def problem_bytes(nv: int, m: int, restart: int = 120) -> int:
 class BatchRunner:
     """Run a list of meshes x wavenumbers x RHS through the GPU in waves."""
 
-    def __init__(self, memory_budget_bytes: int | None = None, workers: int = 4, precision: str = "bf16x3",
-                 rtol: float = 1e-6, restart: int = 120):
+    def __init__(self, memory_budget_bytes: int | None = None, workers: int = 4, precision: str = "fp16x3",
+                 rtol: float = 1e-6, restart: int = 200):
         if memory_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget_bytes = int(0.6 * free)

@@ -11,9 +11,11 @@ see:
   refinement (same stopping test as the reference's BiCGSTAB:
   ``||b - A x||^2 < tol ||b||^2``); ``solver="bicgstab"`` runs the
   reference's BiCGSTAB iteration instead;
-* new keyword-only options: ``precision`` ("fp32", "bf16x3", "bf16") of the
-  Krylov matvec, ``solver``, ``restart``, ``rtol``; right-hand sides may be
-  (N,) or (N, m);
+* new keyword-only options: ``precision`` of the Krylov matvec ("fp32":
+  CUDA cores; "fp16x3": tensor cores with fp16 hi/lo splits and scales,
+  FP32-level accuracy; "bf16x3" / "bf16": tensor cores with bf16 splits,
+  ~3e-5 / ~1e-3, refined in FP64), ``solver``, ``restart``, ``rtol``;
+  right-hand sides may be (N,) or (N, m);
 * ``boundary2potential``/``single_potential``/``double_potential`` evaluate
   listeners without building the P x N potential matrices;
 * mesh errors raise ``BEMError`` (the reference has no checks).
@@ -40,7 +42,7 @@ _LAYERS = {
     "bm_lhs": L.BM_LHS,
     "bm_rhs": L.BM_RHS,
 }
-_PRECISIONS = {"fp32": L.PREC_FP32, "bf16x3": L.PREC_BF16X3, "bf16": L.PREC_BF16}
+_PRECISIONS = {"fp32": L.PREC_FP32, "bf16x3": L.PREC_BF16X3, "bf16": L.PREC_BF16, "fp16x3": L.PREC_FP16X3}
 
 
 def _vp(t) -> ctypes.c_void_p:
@@ -110,7 +112,7 @@ class SolveInfo(dict):
     pass
 
 
-def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_iters=1000, restart=120,
+def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_iters=1000, restart=200,
           precision="fp32", max_refine=None, inner_rtol=None, info: dict | None = None, raise_on_failure=False):
     """Device GMRES (+ FP64 refinement) for complex64 A and b of shape (n,) or (n, m)."""
     check_tensor(A, torch.complex64)
@@ -124,7 +126,7 @@ def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_
     p.precision = prec
     p.restart = int(min(restart, 255, max(1, max_iters)))  # Krylov dimension per cycle
     p.max_iters = int(max_iters)
-    p.max_refine = int(max_refine if max_refine is not None else (2 if prec == L.PREC_FP32 else 6))
+    p.max_refine = int(max_refine if max_refine is not None else (2 if prec in (L.PREC_FP32, L.PREC_FP16X3) else 6))
     p.rtol = float(rtol)
     p.atol = float(atol)
     p.inner_rtol = float(inner_rtol if inner_rtol is not None else (1e-3 if prec == L.PREC_BF16X3 else 3e-2))
@@ -146,7 +148,7 @@ def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_
 
 
 def solve_linear_equation(A_func, b, x=None, nsteps=500, tol=1e-10, atol=1e-16, *, solver="gmres",
-                          precision="fp32", restart=120, info: dict | None = None):
+                          precision="fp32", restart=200, info: dict | None = None):
     """Solve A x = b (solver.py:61-66).
 
     ``A_func`` is a complex64 (n, n) tensor or a callable x -> A x.  Stops when
@@ -215,7 +217,7 @@ class BEM_Solver:
         return out
 
     # ---- boundary integral equations -------------------------------------
-    def CBIE(self, k, neumann, *, precision="fp32", solver="gmres", rtol=1e-5, restart=120, max_iters=1000,
+    def CBIE(self, k, neumann, *, precision="fp32", solver="gmres", rtol=1e-5, restart=200, max_iters=1000,
              info: dict | None = None):
         """Exterior Neumann CBIE (solver.py:97-104): (0.5 I - K) u = -V g."""
         V, lhs = self.assemble_vk(k)
@@ -291,7 +293,7 @@ class BEM_Solver:
         return self._b2p(k, neumann, dirichlet, points)
 
     # ---- the whole path ------------------------------------------------------
-    def solve_and_evaluate(self, k, neumann, points, *, precision="bf16x3", rtol=1e-6, restart=120, max_iters=1000,
+    def solve_and_evaluate(self, k, neumann, points, *, precision="fp16x3", rtol=1e-6, restart=200, max_iters=1000,
                            info: dict | None = None):
         """Assemble (fused V, 0.5 I - K), solve the CBIE for every column of
         ``neumann`` and evaluate the listener pressures.  Returns (u, p)."""

@@ -35,6 +35,8 @@ namespace bemb {
 
 int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
 
+extern int g_tc_promote;  // tensor-core matvec accumulator segment (tc_matvec.cu)
+
 namespace {
 extern int g_tune_chunk;
 extern int g_tune_ctas_per_sm;
@@ -714,6 +716,7 @@ int set_tuning(int key, int value) {
   switch (key) {
     case BEM_TUNE_ASSEMBLY_CHUNK: g_tune_chunk = value; return BEM_OK;
     case BEM_TUNE_ASSEMBLY_CTAS_PER_SM: g_tune_ctas_per_sm = value; return BEM_OK;
+    case BEM_TUNE_TC_PROMOTE: g_tc_promote = value; return BEM_OK;
   }
   return BEM_ERR_INVALID_ARGUMENT;
 }
@@ -722,6 +725,7 @@ int get_tuning(int key) {
   switch (key) {
     case BEM_TUNE_ASSEMBLY_CHUNK: return g_tune_chunk;
     case BEM_TUNE_ASSEMBLY_CTAS_PER_SM: return g_tune_ctas_per_sm;
+    case BEM_TUNE_TC_PROMOTE: return g_tc_promote;
   }
   return -1;
 }

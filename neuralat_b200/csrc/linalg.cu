@@ -24,6 +24,7 @@
 
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "async_copy.cuh"
 #include "bem_common.cuh"
@@ -38,7 +39,10 @@ int tc_matvec(const void* ws, int n, int precision, const float2* X, int m, floa
               cudaStream_t s);
 int tc_error(const void* ws, int* err_host, cudaStream_t s);
 size_t tc_workspace_bytes(int n, int m, int precision);
-int tc_b_planes(void* ws, int n, int m, int precision, __nv_bfloat16** bh, __nv_bfloat16** bl, int* ldb, int* nb);
+int tc_b_planes(void* ws, int n, int m, int precision, __nv_bfloat16** bh, __nv_bfloat16** bl, int* ldb, int* nb,
+                float** cinv);
+int encode_map_2d_f32(CUtensorMap* map, const void* ptr, unsigned long long cols, unsigned long long rows,
+                      unsigned long long ld_bytes, unsigned box_cols, unsigned box_rows);
 int tc_gemm(const void* ws, int n, int precision, int m, float2* Y, const int* active, cudaStream_t s);
 
 namespace {
@@ -181,6 +185,310 @@ int launch_cmatmul(const float2* A, int n, const typename C2<T>::type* X, int ld
 }
 
 // ---------------------------------------------------------------------------
+// FP32 complex matvec Y += A X (HBM-streaming, CUDA cores, 4 FMA per complex
+// product), for the FP32 precision mode and the right-hand side -V g.
+//
+// Split over 1024-column chunks of A (blockIdx.x), row ranges (blockIdx.y)
+// and groups of MR <= 8 right-hand sides (blockIdx.z).  The CTA stages its X
+// chunk transposed in shared memory ([rhs][column]: lanes reading
+// consecutive columns hit consecutive banks); each warp owns 4 rows at a
+// time and meets every A value with MR right-hand sides.  Lane partial sums
+// are combined with a warp reduce-scatter and added to Y with one vector
+// atomic per entry, so Y must hold zero (or the sum to add to) beforehand.
+//  * cgemv_tma_kernel (n even, rows 16-byte aligned): a producer warp streams
+//    32-row x 128-column tiles of A (2-D tensor map over the matrix as FP32
+//    pairs, no multicast; rows / columns past n arrive zero-filled) through a
+//    4-stage shared-memory ring, so memory-level parallelism does not depend
+//    on registers; 8 compute warps read A and X from shared memory.
+//  * cgemv_kernel (any n): lanes stream A rows from global memory.
+// ---------------------------------------------------------------------------
+constexpr int kGvThreads = 256;
+constexpr int kGvRows = 4;       // rows per warp
+constexpr int kGvChunk = 1024;   // columns per CTA
+
+// Warp reduce-scatter of NC complex values held as 2*NC floats (NC a power
+// of two, 1..32): lane L returns the warp total of complex value
+// L >> (5 - log2 NC).
+template <int NC>
+__device__ __forceinline__ float2 warp_rs_complex(float (&v)[2 * NC], int lane) {
+#pragma unroll
+  for (int half = NC / 2, off = 16; half >= 1; half >>= 1, off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int j = 0; j < half; j++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const float send = upper ? v[2 * j + h] : v[2 * (j + half) + h];
+        const float keep = upper ? v[2 * (j + half) + h] : v[2 * j + h];
+        v[2 * j + h] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+      }
+    }
+  }
+  float re = v[0], im = v[1];
+#pragma unroll
+  for (int off = 16 / NC; off >= 1; off >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, off);
+    im += __shfl_xor_sync(0xffffffffu, im, off);
+  }
+  return make_float2(re, im);
+}
+
+// acc[2(r MR + s)] += A row r (columns c, c+1) * X (columns c, c+1, rhs s)
+template <int MR>
+__device__ __forceinline__ void cgemv_fma2(float (&acc)[2 * kGvRows * MR], const float4 (&a)[kGvRows],
+                                           const float2* xs, int c) {
+#pragma unroll
+  for (int sl = 0; sl < MR; sl++) {
+    const float4 x = *reinterpret_cast<const float4*>(&xs[sl * kGvChunk + c]);
+#pragma unroll
+    for (int r = 0; r < kGvRows; r++) {
+      float& re = acc[2 * (r * MR + sl)];
+      float& im = acc[2 * (r * MR + sl) + 1];
+      re = fmaf(a[r].x, x.x, re);
+      re = fmaf(-a[r].y, x.y, re);
+      re = fmaf(a[r].z, x.z, re);
+      re = fmaf(-a[r].w, x.w, re);
+      im = fmaf(a[r].x, x.y, im);
+      im = fmaf(a[r].y, x.x, im);
+      im = fmaf(a[r].z, x.w, im);
+      im = fmaf(a[r].w, x.z, im);
+    }
+  }
+}
+
+// X chunk [c0, c0 + cn) x [s0, s0 + MR) -> xs[rhs][column], zero-padded.
+template <int MR>
+__device__ __forceinline__ void cgemv_stage_x(const float2* __restrict__ X, int m, int c0, int cn, int s0,
+                                              float2* xs, int nthreads) {
+  for (int e = threadIdx.x; e < MR * kGvChunk; e += nthreads) {
+    const int c = e / MR, sl = e - c * MR;
+    float2 v = make_float2(0.f, 0.f);
+    if (c < cn && s0 + sl < m) v = X[(size_t)(c0 + c) * m + s0 + sl];
+    xs[sl * kGvChunk + c] = v;
+  }
+}
+
+// Reduce a warp's 4 x MR partial sums and add them to Y (rows row0..row0+3).
+template <int MR>
+__device__ __forceinline__ void cgemv_flush(float (&acc)[2 * kGvRows * MR], int lane, int row0, int r_end, int s0,
+                                            int m, float2* __restrict__ Y) {
+  constexpr int NC = kGvRows * MR;
+  const float2 t = warp_rs_complex<NC>(acc, lane);
+  constexpr int kShift = NC >= 32 ? 0 : (NC == 16 ? 1 : (NC == 8 ? 2 : (NC == 4 ? 3 : 4)));
+  if ((lane & ((1 << kShift) - 1)) == 0) {
+    const int idx = lane >> kShift;
+    const int r = idx / MR, sl = idx - r * MR;
+    if (row0 + r < r_end && s0 + sl < m) atomicAdd(&Y[(size_t)(row0 + r) * m + s0 + sl], t);
+  }
+}
+
+template <int MR>
+__global__ void __launch_bounds__(kGvThreads, 2)
+    cgemv_kernel(const float2* __restrict__ A, int n, const float2* __restrict__ X, int m, float2* __restrict__ Y,
+                 int rows_per_cta, const int* __restrict__ active) {
+  extern __shared__ __align__(16) float2 xs[];  // [MR][kGvChunk]
+  if (active) {  // GMRES: nothing to do once every column has converged
+    int any = 0;
+    for (int c = 0; c < m; c++) any |= active[c];
+    if (!any) return;
+  }
+  const int c0 = blockIdx.x * kGvChunk;
+  const int cn = min(kGvChunk, n - c0);
+  const int s0 = blockIdx.z * MR;
+  cgemv_stage_x<MR>(X, m, c0, cn, s0, xs, kGvThreads);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r_begin = blockIdx.y * rows_per_cta;
+  const int r_end = min(n, r_begin + rows_per_cta);
+  for (int rb = r_begin + warp * kGvRows; rb < r_end; rb += kGvRows * (kGvThreads / 32)) {
+    float acc[2 * kGvRows * MR];
+#pragma unroll
+    for (int q = 0; q < 2 * kGvRows * MR; q++) acc[q] = 0.f;
+    const float2* arow[kGvRows];
+#pragma unroll
+    for (int r = 0; r < kGvRows; r++) arow[r] = A + (size_t)min(rb + r, n - 1) * n + c0;
+#pragma unroll 4
+    for (int c = lane; c < cn; c += 32) {
+      float2 a[kGvRows];
+#pragma unroll
+      for (int r = 0; r < kGvRows; r++) a[r] = __ldcs(arow[r] + c);
+#pragma unroll
+      for (int sl = 0; sl < MR; sl++) {
+        const float2 x = xs[sl * kGvChunk + c];
+#pragma unroll
+        for (int r = 0; r < kGvRows; r++) {
+          float& re = acc[2 * (r * MR + sl)];
+          float& im = acc[2 * (r * MR + sl) + 1];
+          re = fmaf(a[r].x, x.x, re);
+          re = fmaf(-a[r].y, x.y, re);
+          im = fmaf(a[r].x, x.y, im);
+          im = fmaf(a[r].y, x.x, im);
+        }
+      }
+    }
+    cgemv_flush<MR>(acc, lane, rb, r_end, s0, m, Y);
+  }
+}
+
+constexpr int kGtComputeWarps = 8;
+constexpr int kGtThreads = 32 * (kGtComputeWarps + 1);
+constexpr int kGtBlockRows = kGvRows * kGtComputeWarps;  // 32
+constexpr int kGtTileCols = 128;                          // complex columns per stage
+constexpr int kGtStages = 4;
+constexpr size_t kGtStageBytes = sizeof(float2) * kGtBlockRows * kGtTileCols;  // 32 KB
+
+template <int MR>
+__host__ __device__ constexpr size_t gt_smem_bytes() {
+  return kGtStageBytes * kGtStages + sizeof(float2) * MR * kGvChunk + 2 * kGtStages * sizeof(uint64_t);
+}
+
+template <int MR>
+__global__ void __launch_bounds__(kGtThreads, 1)
+    cgemv_tma_kernel(const __grid_constant__ CUtensorMap amap, int n, const float2* __restrict__ X, int m,
+                     float2* __restrict__ Y, int rows_per_cta, const int* __restrict__ active, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char gt_raw[];
+  float2* tiles = reinterpret_cast<float2*>(gt_raw);                           // [stage][32][128]
+  float2* xs = reinterpret_cast<float2*>(gt_raw + kGtStageBytes * kGtStages);  // [MR][kGvChunk]
+  uint64_t* full = reinterpret_cast<uint64_t*>(gt_raw + kGtStageBytes * kGtStages + sizeof(float2) * MR * kGvChunk);
+  uint64_t* empty = full + kGtStages;
+  if (active) {  // GMRES: nothing to do once every column has converged
+    int any = 0;
+    for (int c = 0; c < m; c++) any |= active[c];
+    if (!any) return;
+  }
+  const int c0 = blockIdx.x * kGvChunk;
+  const int cn = min(kGvChunk, n - c0);
+  const int ntiles = (cn + kGtTileCols - 1) / kGtTileCols;
+  const int s0 = blockIdx.z * MR;
+  const int r_begin = blockIdx.y * rows_per_cta;
+  const int r_end = min(n, r_begin + rows_per_cta);
+  const int nblocks = r_end > r_begin ? (r_end - r_begin + kGtBlockRows - 1) / kGtBlockRows : 0;
+  const int total = nblocks * ntiles;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kGtStages; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kGtComputeWarps);
+    }
+    mbar_init_fence();
+  }
+  cgemv_stage_x<MR>(X, m, c0, cn, s0, xs, kGtThreads);
+  __syncthreads();
+
+  if (warp == kGtComputeWarps) {  // producer
+    if (lane == 0) {
+      const uint64_t pol = l2_evict_first_policy();
+      for (int g = 0; g < total; g++) {
+        const int st = g % kGtStages;
+        if (g >= kGtStages && !mbar_wait(&empty[st], ((uint32_t)(g / kGtStages) - 1u) & 1u, err)) break;
+        const int b = g / ntiles, t = g - b * ntiles;
+        mbar_expect_tx(&full[st], (uint32_t)kGtStageBytes);
+        tma_load_2d_hint(tiles + (size_t)st * kGtBlockRows * kGtTileCols, &amap, 2 * (c0 + t * kGtTileCols),
+                         r_begin + b * kGtBlockRows, &full[st], pol);
+      }
+    }
+    return;
+  }
+
+  for (int b = 0; b < nblocks; b++) {
+    float acc[2 * kGvRows * MR];
+#pragma unroll
+    for (int q = 0; q < 2 * kGvRows * MR; q++) acc[q] = 0.f;
+    for (int t = 0; t < ntiles; t++) {
+      const int g = b * ntiles + t;
+      const int st = g % kGtStages;
+      mbar_wait(&full[st], (uint32_t)(g / kGtStages) & 1u, err);
+      const float2* tile = tiles + (size_t)st * kGtBlockRows * kGtTileCols + (size_t)warp * kGvRows * kGtTileCols;
+#pragma unroll
+      for (int j = 0; j < kGtTileCols / 64; j++) {
+        const int col = 2 * lane + 64 * j;
+        float4 a[kGvRows];
+#pragma unroll
+        for (int r = 0; r < kGvRows; r++) a[r] = *reinterpret_cast<const float4*>(tile + r * kGtTileCols + col);
+        cgemv_fma2<MR>(acc, a, xs, t * kGtTileCols + col);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+    }
+    cgemv_flush<MR>(acc, lane, r_begin + b * kGtBlockRows + warp * kGvRows, r_end, s0, m, Y);
+  }
+}
+
+inline int device_sms() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+template <int MR>
+int launch_cgemv_mr(const float2* A, int n, const float2* X, int m, float2* Y, const int* active, cudaStream_t s) {
+  static std::atomic<bool> attr{false};
+  const int smem = (int)(sizeof(float2) * MR * kGvChunk);
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(cgemv_kernel<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr.store(true, std::memory_order_release);
+  }
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cgemv_kernel<MR>, kGvThreads, smem));
+  const int kc = (n + kGvChunk - 1) / kGvChunk;
+  const int groups = (m + MR - 1) / MR;
+  long long rg = (long long)device_sms() * (occ > 0 ? occ : 1) / ((long long)kc * groups);
+  if (rg < 1) rg = 1;
+  const int step = kGvRows * (kGvThreads / 32);
+  const int rows = (int)(((n + rg - 1) / rg + step - 1) / step * step);
+  rg = (n + rows - 1) / rows;
+  (cgemv_kernel<MR><<<dim3((unsigned)kc, (unsigned)rg, (unsigned)groups), kGvThreads, smem, s>>>(A, n, X, m, Y, rows,
+                                                                                               active),
+   count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+template <int MR>
+int launch_cgemv_tma(const float2* A, int n, const float2* X, int m, float2* Y, const int* active, int* err,
+                     cudaStream_t s) {
+  static std::atomic<bool> attr{false};
+  const int smem = (int)gt_smem_bytes<MR>();
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(cgemv_tma_kernel<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr.store(true, std::memory_order_release);
+  }
+  CUtensorMap map;
+  int rc = encode_map_2d_f32(&map, A, 2ull * n, (unsigned long long)n, 8ull * n, 2 * kGtTileCols, kGtBlockRows);
+  if (rc) return rc;
+  const int kc = (n + kGvChunk - 1) / kGvChunk;
+  const int groups = (m + MR - 1) / MR;
+  long long rg = (long long)device_sms() / ((long long)kc * groups);
+  if (rg < 1) rg = 1;
+  const int rows = (int)(((n + rg - 1) / rg + kGtBlockRows - 1) / kGtBlockRows * kGtBlockRows);
+  rg = (n + rows - 1) / rows;
+  (cgemv_tma_kernel<MR><<<dim3((unsigned)kc, (unsigned)rg, (unsigned)groups), kGtThreads, smem, s>>>(
+       map, n, X, m, Y, rows, active, err),
+   count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+// Y += A X for an n x n complex64 A and m right-hand sides (row-major
+// (n, m)).  err: device int raised if a bounded wait of the TMA variant
+// expired; NULL selects the register variant.
+int launch_cgemv(const float2* A, int n, const float2* X, int m, float2* Y, const int* active, cudaStream_t s,
+                 int* err = nullptr) {
+  if (n <= 0 || m <= 0) return BEM_OK;
+  if ((n & 1) == 0 && err && ((uintptr_t)A & 15) == 0) {
+    if (m == 1) return launch_cgemv_tma<1>(A, n, X, m, Y, active, err, s);
+    if (m == 2) return launch_cgemv_tma<2>(A, n, X, m, Y, active, err, s);
+    if (m <= 4) return launch_cgemv_tma<4>(A, n, X, m, Y, active, err, s);
+    return launch_cgemv_tma<8>(A, n, X, m, Y, active, err, s);
+  }
+  if (m == 1) return launch_cgemv_mr<1>(A, n, X, m, Y, active, s);
+  if (m == 2) return launch_cgemv_mr<2>(A, n, X, m, Y, active, s);
+  if (m <= 4) return launch_cgemv_mr<4>(A, n, X, m, Y, active, s);
+  return launch_cgemv_mr<8>(A, n, X, m, Y, active, s);
+}
+
+// ---------------------------------------------------------------------------
 // GMRES state and kernels
 // ---------------------------------------------------------------------------
 struct GmState {
@@ -199,6 +507,8 @@ struct GmPtrs {
   float2* Vb;      // [m][R+1][ldv]  orthonormal Krylov basis, complex64 storage
   __nv_bfloat16* bh;  // tensor-core B planes (hi, lo) of the matvec operand, or NULL (FP32 matvec on X)
   __nv_bfloat16* bl;
+  float* cinv;     // fp16 planes: inverse per-column scale read by the GEMM epilogue
+  int f16;         // B planes hold fp16 scaled by kF16VecScale (normalised vectors)
   double2* H;      // [m][R][R+1]  column k, rows 0..k+1
   double* cs;      // [m][R]
   double2* sn;     // [m][R]
@@ -279,9 +589,11 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&v)[NV], int lane)
 }
 
 // Matvec operand for unknowns j, j+1 of column s: complex64 X (FP32 matvec)
-// or the bf16 hi/lo B planes of the tensor-core GEMM (rows 2s: (re, -im),
-// 2s+1: (im, re) per unknown, as tc_pack_b_kernel writes them).  x1 is zero
-// when j+1 is the padding entry.
+// or the hi/lo B planes of the tensor-core GEMM (rows 2s: (re, -im),
+// 2s+1: (im, re) per unknown, as the tensor-core pack kernels write them):
+// bf16, or fp16 scaled by kF16VecScale (the vectors are normalised, so
+// |component| <= 1).  x1 is zero when j+1 is the padding entry.
+constexpr float kF16VecScale = 16384.f;
 __device__ __forceinline__ void store_operand(const GmPtrs& P, int j, int s, float2 x0, float2 x1) {
   if (!P.bh) {
     P.X[(size_t)j * P.m + s] = x0;
@@ -289,6 +601,22 @@ __device__ __forceinline__ void store_operand(const GmPtrs& P, int j, int s, flo
     return;
   }
   const float e[2][4] = {{x0.x, -x0.y, x1.x, -x1.y}, {x0.y, x0.x, x1.y, x1.x}};
+  if (P.f16) {
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      __align__(8) __half hi[4], lo[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float v = e[r][q] * kF16VecScale;
+        hi[q] = __float2half_rn(v);
+        lo[q] = __float2half_rn(v - __half2float(hi[q]));
+      }
+      const size_t o = (size_t)(2 * s + r) * P.ldb + 2 * j;
+      *reinterpret_cast<uint2*>(P.bh + o) = *reinterpret_cast<const uint2*>(hi);
+      *reinterpret_cast<uint2*>(P.bl + o) = *reinterpret_cast<const uint2*>(lo);
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < 2; r++) {
     __align__(8) __nv_bfloat16 hi[4], lo[4];
@@ -752,6 +1080,7 @@ constexpr int kPairThreads = 256;
 __global__ void __launch_bounds__(kPairThreads) gm_start_norm_kernel(GmPtrs P) {
   const int i = blockIdx.x * 2 * kPairThreads + 2 * threadIdx.x;
   const int s = blockIdx.y;
+  if (P.f16 && blockIdx.x == 0 && threadIdx.x == 0) P.cinv[s] = 1.f / kF16VecScale;
   if (i >= P.n) return;
   const double b = P.beta[s];
   const double inv = b > 0.0 ? 1.0 / b : 0.0;
@@ -878,7 +1207,8 @@ Layout layout(int n, int m, int R, int precision) {
 
 bool params_ok(const bem_solver_params* p) {
   return p && p->restart >= 1 && p->restart < kMaxRestart && p->max_iters >= 1 && p->max_refine >= 1 && p->rtol >= 0.0 &&
-         (p->precision == BEM_PREC_FP32 || p->precision == BEM_PREC_BF16X3 || p->precision == BEM_PREC_BF16);
+         (p->precision == BEM_PREC_FP32 || p->precision == BEM_PREC_BF16X3 || p->precision == BEM_PREC_BF16 ||
+          p->precision == BEM_PREC_FP16X3);
 }
 
 // Per-step column activity in host-mapped pinned memory (kSnapRing slots of
@@ -997,7 +1327,8 @@ int arnoldi_shape(int n, ArnShape* out) {
 }  // namespace
 
 int cmatmul(const float2* A, int n, const float2* X, int m, float2* Y, cudaStream_t s) {
-  return launch_cmatmul<float, 0>(A, n, X, m, m, Y, m, nullptr, 0, nullptr, nullptr, s);
+  BEM_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)n * m, s));
+  return launch_cgemv(A, n, X, m, Y, nullptr, s);
 }
 
 }  // namespace bemb
@@ -1047,6 +1378,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   P.bh = nullptr;
   P.bl = nullptr;
   P.ldb = 0;
+  P.cinv = nullptr;
+  P.f16 = 0;
   P.beta = (double*)(w + L.beta);
   P.tol = (double*)(w + L.tol);
   P.resid = (double*)(w + L.resid);
@@ -1064,7 +1397,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int rc = tc_operator_prepare((const float2*)A, n, prec, tcws, s);
     if (rc) return rc;
     int nb = 0;
-    if ((rc = tc_b_planes(tcws, n, m, prec, &P.bh, &P.bl, &P.ldb, &nb))) return rc;
+    if ((rc = tc_b_planes(tcws, n, m, prec, &P.bh, &P.bl, &P.ldb, &nb, &P.cinv))) return rc;
+    P.f16 = prec == BEM_PREC_FP16X3;
     // rows 2m..nb-1 of the B planes stay zero; the step kernels write rows < 2m
     BEM_CUDA_TRY(cudaMemsetAsync(P.bh, 0, sizeof(__nv_bfloat16) * (size_t)nb * P.ldb, s));
     BEM_CUDA_TRY(cudaMemsetAsync(P.bl, 0, sizeof(__nv_bfloat16) * (size_t)nb * P.ldb, s));
@@ -1072,8 +1406,10 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     BEM_CUDA_TRY(cudaMemsetAsync(P.X, 0, sizeof(float2) * (size_t)n * m, s));
   }
   auto inner_matvec_on = [&](cudaStream_t st) -> int {
-    if (prec == BEM_PREC_FP32)
-      return launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, nullptr, st);
+    if (prec == BEM_PREC_FP32) {
+      BEM_CUDA_TRY(cudaMemsetAsync(P.Y, 0, sizeof(float2) * (size_t)n * m, st));
+      return launch_cgemv((const float2*)A, n, P.X, m, P.Y, nullptr, st, &P.st->err);
+    }
     return tc_matvec(tcws, n, prec, P.X, m, P.Y, nullptr, st);
   };
   auto inner_matvec = [&]() -> int { return inner_matvec_on(s); };
@@ -1082,7 +1418,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   const dim3 pair_grid((n + 2 * kPairThreads - 1) / (2 * kPairThreads), m);
   // re-orthogonalise (CGS2) when a cycle has to reach the full tolerance;
   // the mixed-precision inner cycles only reduce the residual by inner_rtol
-  const int reorth = (prec == BEM_PREC_FP32 || params->inner_rtol < 1e-4) ? 1 : 0;
+  const bool full_cycle = prec == BEM_PREC_FP32 || prec == BEM_PREC_FP16X3;  // FP32-level matvec
+  const int reorth = (full_cycle || params->inner_rtol < 1e-4) ? 1 : 0;
   ArnShape shape;
   {
     int rc0 = arnoldi_shape(n, &shape);
@@ -1093,7 +1430,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   // gm_arnoldi_kernel clears again after reading it
   auto arnoldi_step = [&](cudaStream_t st) -> int {
     int r2 = prec == BEM_PREC_FP32
-                 ? launch_cmatmul<float, 0>((const float2*)A, n, P.X, m, m, P.Y, m, nullptr, 0, nullptr, P.active, st)
+                 ? launch_cgemv((const float2*)A, n, P.X, m, P.Y, P.active, st, &P.st->err)
                  : tc_gemm(tcws, n, prec, m, P.Y, P.active, st);
     if (r2) return r2;
     cudaLaunchConfig_t cfg = {};
@@ -1170,7 +1507,9 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     refinements = outer + 1;
 
     // inner restarted GMRES on A_lp d = r
-    const double inner_rtol = prec == BEM_PREC_FP32 ? 0.0 : params->inner_rtol;
+    // FP32-level matvecs: one cycle to the target unless it is below their
+    // accuracy (~4e-7 relative); then refinement takes over
+    const double inner_rtol = full_cycle ? 3e-7 : params->inner_rtol;
     bool first_cycle = true;
     while (total_iters < params->max_iters) {
       BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));

@@ -9,8 +9,22 @@
 // so D (n x 2m, fp32) is Y in complex64 layout.  Precision modes:
 //   BF16X3: A = Ah + Al, x = xh + xl (bf16 hi/lo splits), D = Ah xh + Ah xl + Al xh
 //   BF16:   A = Ah only (half the HBM bytes), D = Ah xh + Ah xl
+//   FP16X3: as BF16X3 with fp16 hi/lo planes.  fp16 keeps 11 significant
+//           bits, so the two-term split is accurate to 2^-24 (FP32 level,
+//           against 2^-16 for bf16) at the same 4 bytes per real.  Its range
+//           is narrow, so every row of A is scaled by a power of two that puts
+//           the row maximum below 2^14 (kept as rinv), every right-hand side
+//           likewise (cinv; normalised Krylov vectors use the fixed 2^14), and
+//           the epilogue multiplies D back by rinv[row] * cinv[s].
 // with FP32 accumulation in tensor memory; the solver's FP64 refinement
 // against the FP32 matrix recovers full accuracy.
+//
+// Accumulation: the tensor core's in-place FP32 accumulation over a long K
+// range loses precision (measured: ~3e-5 relative on the BEM matrix whatever
+// the operand split), so accumulator segments are short (`promote` K blocks,
+// two by default for N <= 64): after each segment the epilogue adds the
+// tensor-memory sum to per-row registers with round-to-nearest FP32 adds and
+// writes Y once per row block (fp16x3 then matches an FP32 matvec, ~5e-7).
 //
 // Kernel: one CTA per SM, stream-K over (128-row block, 64-wide K block)
 // units so every SM streams the same number of A bytes; warp 0 issues TMA
@@ -24,6 +38,7 @@
 #include <atomic>
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <cstring>
 
@@ -31,6 +46,8 @@
 #include "bem_common.cuh"
 
 namespace bemb {
+
+int g_tc_promote = 0;  // accumulator segment length in K blocks (0: automatic); a tuning knob
 
 namespace {
 
@@ -48,33 +65,10 @@ struct TcArgs {
   const int* active;  // if set: nothing to do unless some active[c] != 0, c < nact
   int nact;
   int* err;       // set to 1 when a wait expired
+  const float* rinv;  // FP16X3: per-row and per-right-hand-side inverse scales
+  const float* cinv;
+  long long promote;  // K blocks per accumulator segment
 };
-
-// 2-D tiled TMA load (no multicast) completing on `bar`.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// Same, with an L2 eviction-priority policy (used to stream the matrix
-// evict-first so that the small, re-read Krylov basis stays in L2).
-__device__ __forceinline__ void tma_load_2d_hint(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar,
-                                                 uint64_t policy) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, "
-      "%3}], [%4], %5;" ::"r"(smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
-      : "memory");
-}
-
-__device__ __forceinline__ uint64_t l2_evict_first_policy() {
-  uint64_t pol;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
 
 // Shared-memory matrix descriptor: K-major tile with 128-byte swizzle, rows
 // of 128 bytes, 8-row core groups 1024 bytes apart (SBO), sm100 version 1.
@@ -87,9 +81,11 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return d;
 }
 
-// Instruction descriptor, kind::f16: bf16 x bf16 -> f32, both K-major.
-__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor, kind::f16 -> f32 accumulate, both operands K-major
+// and of the same type: bf16 x bf16 (formats 1) or f16 x f16 (formats 0).
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N, bool f16) {
+  return (1u << 4) | (f16 ? 0u : ((1u << 7) | (1u << 10))) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -128,12 +124,28 @@ struct TcSmem {
   static constexpr int kBBytes = NB * kBK * 2;
   static constexpr int kStageBytes = (X3 ? 2 : 1) * kABytes + 2 * kBBytes;
   static constexpr int kStages = (kSmemBudget / kStageBytes) > 8 ? 8 : (kSmemBudget / kStageBytes);
-  static constexpr int kTmemCols =
-      (2 * NB <= 32) ? 32 : (2 * NB <= 64 ? 64 : (2 * NB <= 128 ? 128 : (2 * NB <= 256 ? 256 : 512)));
+  // tensor-memory accumulators in flight: with one-K-block segments the MMA
+  // issuer runs up to kAccBufs segments ahead of the epilogue
+  static constexpr int kAccBufs = NB <= 64 ? 4 : 2;
+  static constexpr int kTmemCols = (kAccBufs * NB <= 32)    ? 32
+                                   : (kAccBufs * NB <= 64)  ? 64
+                                   : (kAccBufs * NB <= 128) ? 128
+                                   : (kAccBufs * NB <= 256) ? 256
+                                                            : 512;
   static constexpr int kBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
 };
 
-template <int NB, bool X3>
+// End of the accumulator segment that starts at unit u: the row block's end,
+// the CTA's end, or `promote` K blocks, whichever comes first (the MMA issuer
+// and the epilogue walk the same segments).
+__device__ __forceinline__ long long segment_end(long long u, long long u1, const TcArgs& p) {
+  const long long rb_end = (u / p.n_kb + 1) * p.n_kb;
+  long long e = rb_end < u1 ? rb_end : u1;
+  if (u + p.promote < e) e = u + p.promote;
+  return e;
+}
+
+template <int NB, bool X3, bool F16>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                    const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, TcArgs p) {
@@ -149,8 +161,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   uint64_t* full = bars;
   uint64_t* empty = bars + S::kStages;
   uint64_t* accf = bars + 2 * S::kStages;
-  uint64_t* acce = accf + 2;
-  uint32_t* tmem_slot = (uint32_t*)(acce + 2);
+  uint64_t* acce = accf + S::kAccBufs;
+  uint32_t* tmem_slot = (uint32_t*)(acce + S::kAccBufs);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // this CTA's contiguous range of (row block, K block) units
@@ -162,7 +174,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < S::kAccBufs; b++) {
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 4 * 32);
     }
@@ -200,7 +212,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
-    constexpr uint32_t idesc = instr_desc(kBM, NB);
+    constexpr uint32_t idesc = instr_desc(kBM, NB, F16);
     int stage = 0;
     uint32_t phase = 0;
     int buf = 0;
@@ -208,8 +220,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     bool ok = true;
     long long u = u0;
     while (u < u1 && ok) {
-      const int rb = (int)(u / p.n_kb);
-      const long long seg_end = (long long)(rb + 1) * p.n_kb < u1 ? (long long)(rb + 1) * p.n_kb : u1;
+      const long long seg_end = segment_end(u, u1, p);
       if (!mbar_wait(&acce[buf], acc_phase ^ 1u, p.err)) break;
       tc_fence_after();
       const uint32_t dt = tmem_base + (uint32_t)(buf * NB);
@@ -240,40 +251,75 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
       }
       umma_commit(&accf[buf]);  // accumulator complete (also on a failed wait: unwinds the epilogue)
-      if (++buf == 2) {
+      if (++buf == S::kAccBufs) {
         buf = 0;
         acc_phase ^= 1u;
       }
     }
   } else if (warp >= 2) {
     // ---------------- epilogue: TMEM -> registers -> atomics into Y ----------------
+    // Each lane owns one row.  With NB <= 64 the segment sums are added in
+    // registers (round-to-nearest FP32) and Y receives one atomic per entry
+    // when the row block (or this CTA's range) ends; wider tiles add every
+    // segment to Y directly.
+    constexpr bool kRegAcc = NB <= 64;
     const int quarter = warp & 3;  // TMEM lanes this warp may access
     int buf = 0;
     uint32_t acc_phase = 0;
     long long u = u0;
+    float racc[kRegAcc ? NB : 1];
+#pragma unroll
+    for (int i = 0; i < (kRegAcc ? NB : 1); i++) racc[i] = 0.f;
     while (u < u1) {
       const int rb = (int)(u / p.n_kb);
-      const long long seg_end = (long long)(rb + 1) * p.n_kb < u1 ? (long long)(rb + 1) * p.n_kb : u1;
+      const long long seg_end = segment_end(u, u1, p);
       u = seg_end;
+      const bool row_done = u == u1 || u % p.n_kb == 0;
       if (!mbar_wait(&accf[buf], acc_phase, p.err)) break;
       tc_fence_after();
       const int row = rb * kBM + quarter * 32 + lane;
       float* yr = p.Y + (size_t)row * p.m2;
-#pragma unroll 1
-      for (int c = 0; c < NB; c += 16) {
-        float t[16];
-        tmem_ld16(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NB + c), t);
-        if (row < p.n) {
+      const float ri = (F16 && row < p.n) ? p.rinv[row] : 1.f;
+      if (kRegAcc) {
 #pragma unroll
-          for (int i = 0; i < 16; i += 2)
-            if (c + i < p.m2) atomicAdd((float2*)(yr + c + i), make_float2(t[i], t[i + 1]));
+        for (int c = 0; c < (kRegAcc ? NB : 16); c += 16) {
+          float t[16];
+          tmem_ld16(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NB + c), t);
+#pragma unroll
+          for (int i = 0; i < 16; i++) racc[c + i] += t[i];
+        }
+      } else {
+#pragma unroll 1
+        for (int c = 0; c < NB; c += 16) {
+          float t[16];
+          tmem_ld16(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NB + c), t);
+          if (row < p.n) {
+#pragma unroll
+            for (int i = 0; i < 16; i += 2)
+              if (c + i < p.m2) {
+                const float sc = F16 ? ri * p.cinv[(c + i) >> 1] : 1.f;
+                atomicAdd((float2*)(yr + c + i), make_float2(t[i] * sc, t[i + 1] * sc));
+              }
+          }
         }
       }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
-      if (++buf == 2) {
+      if (++buf == S::kAccBufs) {
         buf = 0;
         acc_phase ^= 1u;
+      }
+      if (kRegAcc && row_done) {
+        if (row < p.n) {
+#pragma unroll
+          for (int i = 0; i < (kRegAcc ? NB : 1); i += 2)
+            if (i < p.m2) {
+              const float sc = F16 ? ri * p.cinv[i >> 1] : 1.f;
+              atomicAdd((float2*)(yr + i), make_float2(racc[i] * sc, racc[i + 1] * sc));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < (kRegAcc ? NB : 1); i++) racc[i] = 0.f;
       }
     }
   }
@@ -328,6 +374,87 @@ __global__ void tc_pack_b_kernel(const float2* __restrict__ X, int n, int m, int
   }
 }
 
+// Power of two q with |v| * q < 2^14 for |v| <= mx (1 for mx == 0).
+__device__ __forceinline__ float f16_scale(float mx) {
+  if (!(mx > 0.f)) return 1.f;
+  int e;
+  frexpf(mx, &e);  // mx < 2^e
+  return ldexpf(1.f, 14 - e);
+}
+
+// A -> fp16 hi/lo planes, row r scaled by a power of two (rinv[r] = 1/scale).
+// One block per row at a time: a max reduction, then the split.
+__global__ void __launch_bounds__(256) tc_split_a_f16_kernel(const float* __restrict__ A, int n, int ld,
+                                                            __half* __restrict__ Ah, __half* __restrict__ Al,
+                                                            float* __restrict__ rinv) {
+  __shared__ float red[8];
+  for (int r = blockIdx.x; r < n; r += gridDim.x) {
+    const float* row = A + (size_t)r * 2 * n;
+    float mx = 0.f;
+    for (int c = threadIdx.x; c < 2 * n; c += 256) mx = fmaxf(mx, fabsf(row[c]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    float rmx = 0.f;
+#pragma unroll
+    for (int w = 0; w < 8; w++) rmx = fmaxf(rmx, red[w]);
+    const float q = f16_scale(rmx);
+    if (threadIdx.x == 0) rinv[r] = 1.f / q;
+    for (int c = threadIdx.x; c < ld; c += 256) {
+      const float a = c < 2 * n ? row[c] * q : 0.f;
+      const __half h = __float2half_rn(a);
+      Ah[(size_t)r * ld + c] = h;
+      Al[(size_t)r * ld + c] = __float2half_rn(a - __half2float(h));
+    }
+    __syncthreads();  // red is reused by the next row
+  }
+}
+
+// Column maxima of X (n x m complex64) for the fp16 scales: grid (blocks, m).
+__global__ void tc_colmax_kernel(const float2* __restrict__ X, int n, int m, unsigned* __restrict__ cmax) {
+  const int s = blockIdx.y;
+  float mx = 0.f;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const float2 x = X[(size_t)j * m + s];
+    mx = fmaxf(mx, fmaxf(fabsf(x.x), fabsf(x.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&cmax[s], __float_as_uint(mx));  // non-negative floats order as uints
+}
+
+// X -> fp16 B planes with the per-column scales (rows 2s, 2s+1 as for bf16).
+__global__ void tc_pack_b_f16_kernel(const float2* __restrict__ X, int n, int m, int ld, int nb,
+                                     const unsigned* __restrict__ cmax, __half* __restrict__ Bh,
+                                     __half* __restrict__ Bl, float* __restrict__ cinv) {
+  const long long total = (long long)nb * n;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(idx / n), j = (int)(idx - (long long)row * n);
+    const int s = row >> 1;
+    float e0 = 0.f, e1 = 0.f;
+    if (s < m) {
+      const float q = f16_scale(__uint_as_float(cmax[s]));
+      if (j == 0 && (row & 1) == 0) cinv[s] = 1.f / q;
+      const float2 x = X[(size_t)j * m + s];
+      if ((row & 1) == 0) {
+        e0 = x.x * q;
+        e1 = -x.y * q;
+      } else {
+        e0 = x.y * q;
+        e1 = x.x * q;
+      }
+    }
+    const __half h0 = __float2half_rn(e0), h1 = __float2half_rn(e1);
+    const size_t o = (size_t)row * ld + 2 * j;
+    Bh[o] = h0;
+    Bh[o + 1] = h1;
+    Bl[o] = __float2half_rn(e0 - __half2float(h0));
+    Bl[o + 1] = __float2half_rn(e1 - __half2float(h1));
+  }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -363,11 +490,32 @@ int make_map(CUtensorMap* map, const void* ptr, int kext, int rows, int ld, int 
 
 inline size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 
-// Workspace: [header: error flag, zero flag][A hi][A lo (bf16x3)][B hi][B lo].
-// The A offsets do not depend on m.
+}  // namespace
+
+// 2-D FP32 tensor map (no swizzle, zero fill outside the tensor) over a
+// row-major matrix of `rows` rows of `cols` floats, `ld_bytes` apart.
+int encode_map_2d_f32(CUtensorMap* map, const void* ptr, unsigned long long cols, unsigned long long rows,
+                      unsigned long long ld_bytes, unsigned box_cols, unsigned box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return BEM_ERR_CUDA;
+  if (((uintptr_t)ptr & 15) || (ld_bytes & 15)) return BEM_ERR_INVALID_ARGUMENT;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? BEM_OK : BEM_ERR_CUDA;
+}
+
+namespace {
+
+// Workspace: [header: error flag][column maxima (m)][cinv (m)][rinv (n)]
+// [A hi][A lo (bf16x3, fp16x3)][B hi][B lo].  The A offsets do not depend on m.
 struct TcLayout {
   int ld, nb;
-  size_t hdr, ah, alo, bh, bl, total;
+  size_t hdr, cmax, cinv, rinv, ah, alo, bh, bl, total;
 };
 
 TcLayout tc_layout(int n, int m, int precision) {
@@ -378,10 +526,16 @@ TcLayout tc_layout(int n, int m, int precision) {
   size_t o = 0;
   L.hdr = o;
   o = al256(o + 256);
+  L.cmax = o;
+  o = al256(o + 128 * sizeof(unsigned));
+  L.cinv = o;
+  o = al256(o + 128 * sizeof(float));
+  L.rinv = o;
+  o = al256(o + sizeof(float) * (size_t)n);
   L.ah = o;
   o = al256(o + (size_t)n * L.ld * 2);
   L.alo = o;
-  if (precision == BEM_PREC_BF16X3) o = al256(o + (size_t)n * L.ld * 2);
+  if (precision == BEM_PREC_BF16X3 || precision == BEM_PREC_FP16X3) o = al256(o + (size_t)n * L.ld * 2);
   L.bh = o;
   o = al256(o + (size_t)L.nb * L.ld * 2);
   L.bl = o;
@@ -390,12 +544,13 @@ TcLayout tc_layout(int n, int m, int precision) {
   return L;
 }
 
-template <int NB, bool X3>
+template <int NB, bool X3, bool F16>
 int launch_tc(const TcLayout& L, char* ws, int n, const int* active, int nact, float* Y, int m2, cudaStream_t s) {
   using S = TcSmem<NB, X3>;
   static std::atomic<bool> attr{false};
   if (!attr.load(std::memory_order_acquire)) {
-    BEM_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NB, X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
+    BEM_CUDA_TRY(
+        cudaFuncSetAttribute(tc_gemm_kernel<NB, X3, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
     attr.store(true, std::memory_order_release);
   }
   CUtensorMap mah, mal, mbh, mbl;
@@ -414,11 +569,16 @@ int launch_tc(const TcLayout& L, char* ws, int n, const int* active, int nact, f
   a.err = (int*)(ws + L.hdr);
   a.active = active;
   a.nact = nact;
+  a.rinv = F16 ? (const float*)(ws + L.rinv) : nullptr;
+  a.cinv = F16 ? (const float*)(ws + L.cinv) : nullptr;
+  // two K blocks per segment: fp16x3 error 6e-7 on the BEM matrix (one block:
+  // 4e-7 but 18% slower; 16 blocks: 4e-6; a whole row block: 3e-5)
+  a.promote = g_tc_promote > 0 ? g_tc_promote : (NB <= 64 ? 2 : (1ll << 40));
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = (long long)sms < a.units ? sms : (int)a.units;
-  (tc_gemm_kernel<NB, X3><<<grid, kTcThreads, S::kBytes, s>>>(mah, mal, mbh, mbl, a), count_launch());
+  (tc_gemm_kernel<NB, X3, F16><<<grid, kTcThreads, S::kBytes, s>>>(mah, mal, mbh, mbl, a), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
@@ -426,7 +586,9 @@ int launch_tc(const TcLayout& L, char* ws, int n, const int* active, int nact, f
 }  // namespace
 
 size_t tc_workspace_bytes(int n, int m, int precision) {
-  if ((precision != BEM_PREC_BF16X3 && precision != BEM_PREC_BF16) || n <= 0 || m <= 0 || m > 128) return 0;
+  if ((precision != BEM_PREC_BF16X3 && precision != BEM_PREC_BF16 && precision != BEM_PREC_FP16X3) || n <= 0 ||
+      m <= 0 || m > 128)
+    return 0;
   return tc_layout(n, m, precision).total;
 }
 
@@ -434,9 +596,15 @@ int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStr
   const TcLayout L = tc_layout(n, 1, precision);
   char* w = (char*)ws;
   BEM_CUDA_TRY(cudaMemsetAsync(w + L.hdr, 0, 256, s));
-  (tc_split_a_kernel<<<1184, 256, 0, s>>>((const float*)A, n, L.ld, (__nv_bfloat16*)(w + L.ah),
-                                          precision == BEM_PREC_BF16X3 ? (__nv_bfloat16*)(w + L.alo) : nullptr),
-   count_launch());
+  if (precision == BEM_PREC_FP16X3) {
+    (tc_split_a_f16_kernel<<<n < 1184 ? n : 1184, 256, 0, s>>>((const float*)A, n, L.ld, (__half*)(w + L.ah),
+                                                                (__half*)(w + L.alo), (float*)(w + L.rinv)),
+     count_launch());
+  } else {
+    (tc_split_a_kernel<<<1184, 256, 0, s>>>((const float*)A, n, L.ld, (__nv_bfloat16*)(w + L.ah),
+                                            precision == BEM_PREC_BF16X3 ? (__nv_bfloat16*)(w + L.alo) : nullptr),
+     count_launch());
+  }
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
@@ -450,18 +618,28 @@ int tc_matvec(const void* ws_, int n, int precision, const float2* X, int m, flo
   if (m <= 0 || m > 128) return BEM_ERR_UNSUPPORTED;
   char* ws = (char*)ws_;
   const TcLayout L = tc_layout(n, m, precision);
-  (tc_pack_b_kernel<<<1184, 256, 0, s>>>(X, n, m, L.ld, L.nb, (__nv_bfloat16*)(ws + L.bh),
-                                         (__nv_bfloat16*)(ws + L.bl)),
-   count_launch());
+  if (precision == BEM_PREC_FP16X3) {
+    BEM_CUDA_TRY(cudaMemsetAsync(ws + L.cmax, 0, sizeof(unsigned) * m, s));
+    (tc_colmax_kernel<<<dim3(n < 8192 ? (n + 255) / 256 : 32, m), 256, 0, s>>>(X, n, m, (unsigned*)(ws + L.cmax)),
+     count_launch());
+    (tc_pack_b_f16_kernel<<<1184, 256, 0, s>>>(X, n, m, L.ld, L.nb, (const unsigned*)(ws + L.cmax),
+                                               (__half*)(ws + L.bh), (__half*)(ws + L.bl), (float*)(ws + L.cinv)),
+     count_launch());
+  } else {
+    (tc_pack_b_kernel<<<1184, 256, 0, s>>>(X, n, m, L.ld, L.nb, (__nv_bfloat16*)(ws + L.bh),
+                                           (__nv_bfloat16*)(ws + L.bl)),
+     count_launch());
+  }
   BEM_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)n * m, s));
   return tc_gemm(ws_, n, precision, m, Y, active, s);
 }
 
 // B operand planes, for producers that write them directly: element (j, s)
 // of X occupies columns 2j, 2j+1 of rows 2s, 2s+1 (row stride ldb), as
-// written by tc_pack_b_kernel.  Rows 2m..nb-1 must be zero.
+// written by tc_pack_b_kernel (bf16) or tc_pack_b_f16_kernel (fp16, scaled:
+// the producer also sets cinv[s]).  Rows 2m..nb-1 must be zero.
 int tc_b_planes(void* ws_, int n, int m, int precision, __nv_bfloat16** bh, __nv_bfloat16** bl, int* ldb,
-                int* nb) {
+                int* nb, float** cinv) {
   if (m <= 0 || m > 128) return BEM_ERR_UNSUPPORTED;
   char* ws = (char*)ws_;
   const TcLayout L = tc_layout(n, m, precision);
@@ -469,6 +647,7 @@ int tc_b_planes(void* ws_, int n, int m, int precision, __nv_bfloat16** bh, __nv
   *bl = (__nv_bfloat16*)(ws + L.bl);
   *ldb = L.ld;
   *nb = L.nb;
+  *cinv = (float*)(ws + L.cinv);
   return BEM_OK;
 }
 
@@ -477,15 +656,21 @@ int tc_gemm(const void* ws_, int n, int precision, int m, float2* Y, const int* 
   if (m <= 0 || m > 128) return BEM_ERR_UNSUPPORTED;
   char* ws = (char*)ws_;
   const TcLayout L = tc_layout(n, m, precision);
-  const bool x3 = precision == BEM_PREC_BF16X3;
   float* y = (float*)Y;
+#define BEM_TC_CASE(NBV)                                                                                  \
+  case NBV:                                                                                               \
+    if (precision == BEM_PREC_FP16X3) return launch_tc<NBV, true, true>(L, ws, n, active, m, y, 2 * m, s); \
+    if (precision == BEM_PREC_BF16X3) return launch_tc<NBV, true, false>(L, ws, n, active, m, y, 2 * m, s); \
+    return launch_tc<NBV, false, false>(L, ws, n, active, m, y, 2 * m, s);
   switch (L.nb) {
-    case 16: return x3 ? launch_tc<16, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<16, false>(L, ws, n, active, m, y, 2 * m, s);
-    case 32: return x3 ? launch_tc<32, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<32, false>(L, ws, n, active, m, y, 2 * m, s);
-    case 64: return x3 ? launch_tc<64, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<64, false>(L, ws, n, active, m, y, 2 * m, s);
-    case 128: return x3 ? launch_tc<128, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<128, false>(L, ws, n, active, m, y, 2 * m, s);
-    default: return x3 ? launch_tc<256, true>(L, ws, n, active, m, y, 2 * m, s) : launch_tc<256, false>(L, ws, n, active, m, y, 2 * m, s);
+    BEM_TC_CASE(16)
+    BEM_TC_CASE(32)
+    BEM_TC_CASE(64)
+    BEM_TC_CASE(128)
+    BEM_TC_CASE(256)
   }
+#undef BEM_TC_CASE
+  return BEM_ERR_UNSUPPORTED;
 }
 
 // Error flag of the tensor-core kernels that used this workspace (syncs).
@@ -504,7 +689,8 @@ extern "C" size_t bem_tc_operator_bytes(int n, int m, int precision) { return tc
 extern "C" int bem_tc_operator_prepare(const void* A, int n, int precision, void* ws, size_t ws_bytes,
                                        bem_stream_t stream) {
   if (!A || !ws || n <= 0) return BEM_ERR_INVALID_ARGUMENT;
-  if (precision != BEM_PREC_BF16X3 && precision != BEM_PREC_BF16) return BEM_ERR_INVALID_ARGUMENT;
+  if (precision != BEM_PREC_BF16X3 && precision != BEM_PREC_BF16 && precision != BEM_PREC_FP16X3)
+    return BEM_ERR_INVALID_ARGUMENT;
   if (ws_bytes < tc_workspace_bytes(n, 1, precision)) return BEM_ERR_WORKSPACE;
   return tc_operator_prepare((const float2*)A, n, precision, ws, (cudaStream_t)stream);
 }
