@@ -252,6 +252,246 @@ __global__ void __launch_bounds__(kRegThreads, 2)
 }
 
 // ---------------------------------------------------------------------------
+// Symmetric evaluation of the regular pairs (V and K together).  G(|x - y|)
+// is symmetric, so each unordered non-touching pair {i, j} is evaluated once
+// and scattered both ways:
+//   V_ji = V_ij^T,
+//   K_ij uses the trial plane of j (dn_j(p) = n_j . (c_j - x_p)),
+//   K_ji uses the plane of i at the trial points (dn_i(q) = n_i . (c_i - y_q)),
+// both from the same r, sincos and kernel values.  A work item is a test group
+// (2 tiles, 32 triangles: one per lane) against a chunk of trial tiles; only
+// trial tiles at or after the group's first tile are used, and on the group's
+// own tiles only pairs j > i.  One warp per trial triangle (16 warps); the
+// test points are staged structure-of-arrays in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kSymThreads = 32 * kTile;  // 512: warp w takes trial triangle w
+
+struct SymSmem {
+  float2 slotV[kTestCorners][kSlotStride];
+  float2 slotK[kTestCorners][kSlotStride];
+  float2 slotM[kTestCorners][kSlotStride];  // K_ji^T, indexed like slotK
+  float xs[18][kTestTris];                  // test quadrature points, [coordinate][lane]
+  TriRec trial[kTile];
+  TileRec tileJ;
+  TileRec tileI[2];
+};
+
+// aV, aK as pair_block; aM[3a+b] = sum_pq C_ap C_bq dn_i(q) Gk(r_pq) = K_ji[b][a].
+__device__ __forceinline__ void pair_block_sym(const float (*xs)[kTestTris], int lane, const float (&yq)[18],
+                                               const float (&dq)[6], float njx, float njy, float njz, float cjx,
+                                               float cjy, float cjz, float k, float2 (&aV)[9], float2 (&aK)[9],
+                                               float2 (&aM)[9]) {
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    aV[e] = make_float2(0.f, 0.f);
+    aK[e] = make_float2(0.f, 0.f);
+    aM[e] = make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int p = 0; p < 6; p++) {
+    const float px = xs[3 * p][lane], py = xs[3 * p + 1][lane], pz = xs[3 * p + 2][lane];
+    const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);
+    float2 tV[3], tK[3], uK[3];
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      tV[b] = make_float2(0.f, 0.f);
+      tK[b] = make_float2(0.f, 0.f);
+      uK[b] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const float dx = yq[3 * q] - px, dy = yq[3 * q + 1] - py, dz = yq[3 * q + 2] - pz;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float rinv = fminf(rsqrtf(r2), 1.0f / kEps);
+      const float r = fmaxf(r2 * rinv, kEps);
+      float s, c;
+      __sincosf(k * r, &s, &c);
+      const float gvr = c * rinv, gvi = s * rinv;
+      const float rinv2 = rinv * rinv;
+      const float gkr = fmaf(k, s, gvr) * rinv2;   // (c + kr s) / r^3
+      const float gki = fmaf(-k, c, gvi) * rinv2;  // (s - kr c) / r^3
+      const float mkr = dq[q] * gkr, mki = dq[q] * gki;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        const float w = (float)(tri6_w(q) * tri6_phi(q, b));
+        tV[b].x = fmaf(w, gvr, tV[b].x);
+        tV[b].y = fmaf(w, gvi, tV[b].y);
+        tK[b].x = fmaf(w, gkr, tK[b].x);
+        tK[b].y = fmaf(w, gki, tK[b].y);
+        uK[b].x = fmaf(w, mkr, uK[b].x);
+        uK[b].y = fmaf(w, mki, uK[b].y);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float wa = (float)(tri6_w(p) * tri6_phi(p, a));
+      const float wk = wa * dn;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        aV[3 * a + b].x = fmaf(wa, tV[b].x, aV[3 * a + b].x);
+        aV[3 * a + b].y = fmaf(wa, tV[b].y, aV[3 * a + b].y);
+        aK[3 * a + b].x = fmaf(wk, tK[b].x, aK[3 * a + b].x);
+        aK[3 * a + b].y = fmaf(wk, tK[b].y, aK[3 * a + b].y);
+        aM[3 * a + b].x = fmaf(wa, uK[b].x, aM[3 * a + b].x);
+        aM[3 * a + b].y = fmaf(wa, uK[b].y, aM[3 * a + b].y);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g, float k, float2* __restrict__ V,
+                                                 float2* __restrict__ K, float v_scale, float k_scale, int grp,
+                                                 int jt_begin, int jt_end) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nt = g.nt, nv = g.nv;
+  const int tile0 = 2 * grp;
+  const bool has_t1 = tile0 + 1 < g.ntiles;
+  const int ti = grp * kTestTris + lane;
+  const bool valid_i = ti < nt;
+  const TriRec& ri = g.rec[valid_i ? ti : nt - 1];
+  const float area_i = ri.area;
+  const float nix = ri.n[0], niy = ri.n[1], niz = ri.n[2], cix = ri.c[0], ciy = ri.c[1], ciz = ri.c[2];
+  const int iv0 = ri.v[0], iv1 = ri.v[1], iv2 = ri.v[2];
+
+  __syncthreads();  // the previous item is done with tileI and xs
+  copy_words(&sm.tileI[0], &g.tiles[tile0], sizeof(TileRec), tid, kSymThreads);
+  if (has_t1) copy_words(&sm.tileI[1], &g.tiles[tile0 + 1], sizeof(TileRec), tid, kSymThreads);
+  for (int e = tid; e < 18 * kTestTris; e += kSymThreads) {
+    const int c = e / kTestTris, l = e - c * kTestTris;
+    const int t = min(grp * kTestTris + l, nt - 1);
+    sm.xs[c][l] = g.rec[t].qp[c];
+  }
+
+  for (int jt = jt_begin; jt < jt_end; jt++) {
+    __syncthreads();  // gather of the previous trial tile is done with the slots
+    copy_words(&sm.tileJ, &g.tiles[jt], sizeof(TileRec), tid, kSymThreads);
+    const int ntriJ = min(kTile, nt - jt * kTile);
+    copy_words(sm.trial, &g.rec[jt * kTile], ntriJ * (int)sizeof(TriRec), tid, kSymThreads);
+    __syncthreads();
+
+    // ---- compute: warp w takes trial triangle w ----
+    const int tt = warp;
+    const int tj = jt * kTile + tt;
+    float aa = 0.f;
+    if (tt < ntriJ) {
+      const TriRec& rj = sm.trial[tt];
+      const int j0 = rj.v[0], j1 = rj.v[1], j2 = rj.v[2];
+      const bool touching = (iv0 == j0) | (iv0 == j1) | (iv0 == j2) | (iv1 == j0) | (iv1 == j1) | (iv1 == j2) |
+                            (iv2 == j0) | (iv2 == j1) | (iv2 == j2);
+      // on the group's own tiles each unordered pair once (j > i)
+      const bool once = jt >= tile0 + 2 || tj > ti;
+      aa = (valid_i && !touching && once) ? area_i * rj.area : 0.f;
+    }
+    if (tt < ntriJ && __any_sync(0xffffffffu, aa != 0.f)) {
+      const TriRec& rj = sm.trial[tt];
+      float yq[18];
+#pragma unroll
+      for (int e = 0; e < 18; e++) yq[e] = rj.qp[e];
+      float dq[6];
+#pragma unroll
+      for (int q = 0; q < 6; q++)
+        dq[q] = nix * (cix - yq[3 * q]) + niy * (ciy - yq[3 * q + 1]) + niz * (ciz - yq[3 * q + 2]);
+      float2 aV[9], aK[9], aM[9];
+      pair_block_sym(sm.xs, lane, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aV, aK, aM);
+      const float sv = aa * v_scale, sk = aa * k_scale;
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          sm.slotV[3 * lane + a][3 * tt + b] = make_float2(aV[3 * a + b].x * sv, aV[3 * a + b].y * sv);
+          sm.slotK[3 * lane + a][3 * tt + b] = make_float2(aK[3 * a + b].x * sk, aK[3 * a + b].y * sk);
+          sm.slotM[3 * lane + a][3 * tt + b] = make_float2(aM[3 * a + b].x * sk, aM[3 * a + b].y * sk);
+        }
+    } else if (tt < ntriJ) {
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          sm.slotV[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotK[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotM[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+
+    // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
+    const int nI0 = sm.tileI[0].nlv;
+    const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
+    const int nJ = sm.tileJ.nlv;
+    const int total = (nI0 + nI1) * nJ;
+    for (int e = tid; e < total; e += kSymThreads) {
+      const int ai = e / nJ;
+      const int b = e - ai * nJ;
+      const int s = ai >= nI0;
+      const int a = ai - s * nI0;
+      const TileRec& TI = sm.tileI[s];
+      float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f), acc_m = make_float2(0.f, 0.f);
+      const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+      const int cb0 = sm.tileJ.lv_ptr[b], cb1 = sm.tileJ.lv_ptr[b + 1];
+      for (int ca = ca0; ca < ca1; ca++) {
+        const int row = s * kTileCorners + TI.lv_corner[ca];
+        for (int cb = cb0; cb < cb1; cb++) {
+          const int col = sm.tileJ.lv_corner[cb];
+          acc_v.x += sm.slotV[row][col].x;
+          acc_v.y += sm.slotV[row][col].y;
+          acc_k.x += sm.slotK[row][col].x;
+          acc_k.y += sm.slotK[row][col].y;
+          acc_m.x += sm.slotM[row][col].x;
+          acc_m.y += sm.slotM[row][col].y;
+        }
+      }
+      const int A = TI.vid[a], B = sm.tileJ.vid[b];
+      if (acc_v.x != 0.f || acc_v.y != 0.f || acc_k.x != 0.f || acc_k.y != 0.f || acc_m.x != 0.f ||
+          acc_m.y != 0.f) {
+        atomicAdd(&V[(size_t)A * nv + B], acc_v);
+        atomicAdd(&V[(size_t)B * nv + A], acc_v);
+        atomicAdd(&K[(size_t)A * nv + B], acc_k);
+        atomicAdd(&K[(size_t)B * nv + A], acc_m);
+      }
+    }
+  }
+}
+
+// The used (group, trial tile) units in order: group g owns the ntiles - 2g
+// trial tiles from its first tile on, so the units before group g number
+// S(g) = g (ntiles - g + 1).  Items are equal runs of `chunk` consecutive
+// units (a run crossing a group boundary is split), dealt round-robin to a
+// persistent grid: every CTA gets the same amount of work.
+__device__ __forceinline__ long long sym_units_before(long long g, long long ntiles) { return g * (ntiles - g + 1); }
+
+__device__ __forceinline__ int sym_group_of(long long pos, int ntiles, int ngroups) {
+  const double b = (double)ntiles + 1.0;
+  const double disc = b * b - 4.0 * (double)pos;
+  long long g = (long long)((b - sqrt(disc > 0.0 ? disc : 0.0)) * 0.5);
+  if (g < 0) g = 0;
+  if (g > ngroups - 1) g = ngroups - 1;
+  while (g + 1 < ngroups && sym_units_before(g + 1, ntiles) <= pos) g++;
+  while (g > 0 && sym_units_before(g, ntiles) > pos) g--;
+  return (int)g;
+}
+
+__global__ void __launch_bounds__(kSymThreads, 1)
+    regular_sym_kernel(GeomView g, float k, float2* __restrict__ V, float2* __restrict__ K, float v_scale,
+                       float k_scale, long long chunk, long long n_units, int n_items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SymSmem& sm = *reinterpret_cast<SymSmem*>(smem_raw);
+  const int ngroups = (g.nt + kTestTris - 1) / kTestTris;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    long long pos = (long long)item * chunk;
+    const long long end = pos + chunk < n_units ? pos + chunk : n_units;
+    while (pos < end) {  // uniform over the block
+      const int grp = sym_group_of(pos, g.ntiles, ngroups);
+      const long long base = sym_units_before(grp, g.ntiles);
+      const long long gend = base + (g.ntiles - 2 * grp);
+      const long long stop = end < gend ? end : gend;
+      const int jt0 = 2 * grp + (int)(pos - base);
+      regular_sym_item(sm, g, k, V, K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos));
+      pos = stop;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Singular (touching) pairs: Sauter-Schwab quadrature on the reference
 // triangle (0,0),(1,0),(1,1) (integrand.h:54-185), after re-ordering so the
 // shared vertices come first (integrand.h:351-387).  One warp per pair; the
@@ -657,6 +897,31 @@ int launch_singular(const GeomView& g, float k, float2* V, float2* K, float v_sc
 }  // namespace
 
 // V and/or (mass_coeff M + k_coeff K), both overwritten.
+int launch_regular_sym(const GeomView& g, float k, float2* V, float2* K, float v_scale, float k_scale,
+                       cudaStream_t s) {
+  const int smem = (int)sizeof(SymSmem);
+  static std::atomic<bool> attr_set{false};
+  if (!attr_set.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(regular_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_set.store(true, std::memory_order_release);
+  }
+  const int n_groups = (g.nt + kTestTris - 1) / kTestTris;
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_sym_kernel, kSymThreads, smem));
+  const int grid = sm_count() * (occ > 0 ? occ : 1);
+  const long long n_units = (long long)n_groups * g.ntiles - (long long)n_groups * (n_groups - 1);
+  // 8 equal items per CTA (a tuned chunk overrides)
+  long long chunk = (n_units + 8LL * grid - 1) / (8LL * grid);
+  if (chunk < 1) chunk = 1;
+  if (g_tune_chunk > 0) chunk = g_tune_chunk;
+  const long long n_items = (n_units + chunk - 1) / chunk;
+  (regular_sym_kernel<<<grid < n_items ? grid : (int)n_items, kSymThreads, smem, s>>>(g, k, V, K, v_scale, k_scale,
+                                                                                       chunk, n_units, (int)n_items),
+   count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
 int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_coeff, float k_coeff, cudaStream_t s) {
   const size_t bytes = sizeof(float2) * (size_t)g.nv * g.nv;
   if (V) BEM_CUDA_TRY(cudaMemsetAsync(V, 0, bytes, s));
@@ -665,7 +930,7 @@ int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_
   const float k_scale = -kInv4Pi * k_coeff;  // K = -(...)/(4 pi)
   int rc;
   if (V && Kout) {
-    if ((rc = launch_regular<true, true>(g, k, V, Kout, v_scale, k_scale, s))) return rc;
+    if ((rc = launch_regular_sym(g, k, V, Kout, v_scale, k_scale, s))) return rc;
     return launch_singular<true, true>(g, k, V, Kout, v_scale, k_scale, mass_coeff, s);
   } else if (V) {
     if ((rc = launch_regular<true, false>(g, k, V, nullptr, v_scale, 0.f, s))) return rc;
