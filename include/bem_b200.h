@@ -136,8 +136,11 @@ int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, floa
 enum {
   BEM_TUNE_ASSEMBLY_CHUNK = 1,      /* trial tiles (16 triangles) per work item */
   BEM_TUNE_ASSEMBLY_CTAS_PER_SM = 2, /* persistent CTAs per SM (<= occupancy limit) */
-  BEM_TUNE_TC_PROMOTE = 3            /* tensor-core matvec: K blocks (64 reals) accumulated in tensor
+  BEM_TUNE_TC_PROMOTE = 3,           /* tensor-core matvec: K blocks (64 reals) accumulated in tensor
                                         memory before the partial sum leaves it (0: automatic) */
+  BEM_TUNE_GMRES_REORTH = 4,         /* Arnoldi Gram-Schmidt passes: 0 automatic (one), 1 one, 2 two */
+  BEM_TUNE_ARNOLDI_CLUSTER = 5       /* largest thread-block cluster (power of two <= 16) per Krylov
+                                        column in the Arnoldi kernel (0: automatic) */
 };
 int bem_set_tuning(int key, int value);
 int bem_get_tuning(int key);

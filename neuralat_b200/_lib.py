@@ -50,7 +50,7 @@ class BEMError(RuntimeError):
         super().__init__(f"{what}: {msg} (status {self.status})" if what else f"{msg} (status {self.status})")
 
 
-TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE = 1, 2, 3
+TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE, TUNE_GMRES_REORTH, TUNE_ARNOLDI_CLUSTER = 1, 2, 3, 4, 5
 
 
 class BatchProblem(ctypes.Structure):

@@ -35,7 +35,9 @@ namespace bemb {
 
 int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
 
-extern int g_tc_promote;  // tensor-core matvec accumulator segment (tc_matvec.cu)
+extern int g_tc_promote;    // tensor-core matvec accumulator segment (tc_matvec.cu)
+extern int g_gmres_reorth;  // Gram-Schmidt passes of the Arnoldi step (linalg.cu)
+extern int g_arn_max_cluster;  // largest Arnoldi cluster size (linalg.cu)
 
 namespace {
 extern int g_tune_chunk;
@@ -982,6 +984,14 @@ int set_tuning(int key, int value) {
     case BEM_TUNE_ASSEMBLY_CHUNK: g_tune_chunk = value; return BEM_OK;
     case BEM_TUNE_ASSEMBLY_CTAS_PER_SM: g_tune_ctas_per_sm = value; return BEM_OK;
     case BEM_TUNE_TC_PROMOTE: g_tc_promote = value; return BEM_OK;
+    case BEM_TUNE_GMRES_REORTH:
+      if (value > 2) return BEM_ERR_INVALID_ARGUMENT;
+      g_gmres_reorth = value;
+      return BEM_OK;
+    case BEM_TUNE_ARNOLDI_CLUSTER:
+      if (value > 16 || (value & (value - 1))) return BEM_ERR_INVALID_ARGUMENT;
+      g_arn_max_cluster = value;
+      return BEM_OK;
   }
   return BEM_ERR_INVALID_ARGUMENT;
 }
@@ -991,6 +1001,8 @@ int get_tuning(int key) {
     case BEM_TUNE_ASSEMBLY_CHUNK: return g_tune_chunk;
     case BEM_TUNE_ASSEMBLY_CTAS_PER_SM: return g_tune_ctas_per_sm;
     case BEM_TUNE_TC_PROMOTE: return g_tc_promote;
+    case BEM_TUNE_GMRES_REORTH: return g_gmres_reorth;
+    case BEM_TUNE_ARNOLDI_CLUSTER: return g_arn_max_cluster;
   }
   return -1;
 }

@@ -10,8 +10,9 @@
 //    by the 4 rows, lanes read A rows coalesced.  Accumulation in float or
 //    double (the latter is the FP64 refinement residual).
 //  * restarted GMRES, one Krylov space per right-hand side sharing every
-//    operator application: Arnoldi in FP64 with classical Gram-Schmidt and
-//    re-orthogonalisation (CGS2), complex Givens rotations in FP64, all state
+//    operator application: Arnoldi with classical Gram-Schmidt in FP64 (one
+//    pass by default, re-orthogonalisation on request), complex Givens
+//    rotations in FP64, all state
 //    on the device; the host only watches a convergence flag through events,
 //    without stalling the GPU.  Outer FP64 iterative refinement
 //    r = b - A x against the FP32 matrix.
@@ -32,6 +33,9 @@
 namespace bemb {
 
 namespace cg = cooperative_groups;
+
+int g_gmres_reorth = 0;     // Gram-Schmidt passes: 0 automatic, 1 one pass (CGS), 2 two passes (CGS2); a tuning knob
+int g_arn_max_cluster = 0;  // largest Arnoldi cluster size tried (0: 16); a tuning knob
 
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
@@ -541,8 +545,9 @@ struct GmPtrs {
 // the whole step:
 //   w = Y (Y cleared for the next accumulating matvec)
 //   h1 = V^H w                 classical Gram-Schmidt, FP64 sums
-//   w' = w - V h1;  h2 = V^H w'  (re-orthogonalisation, CGS2)
-//   w'' = w' - V h2;  h_{k+1,k} = |w''|
+//   w' = w - V h1            (one pass by default; with re-orthogonalisation
+//   h2 = V^H w', w'' = w' - V h2   also this second pass, CGS2)
+//   h_{k+1,k} = |w''|
 //   v_{k+1} = w'' / h_{k+1,k} -> basis (complex64) and the next matvec operand
 //   Givens rotation of the new Hessenberg column (CTA 0 of the cluster)
 // Partial sums of each CTA are combined across the cluster through
@@ -1271,10 +1276,12 @@ int host_ring(int m, HostRing** r) {
   return BEM_OK;
 }
 
-// Launch shape of gm_arnoldi_kernel for n unknowns: the smallest
-// power-of-two cluster (<= 16 CTAs) whose CTAs hold at most 768 unknowns
-// each, widened while the w slice would not fit in shared memory; checked
-// against the device with cudaOccupancyMaxActiveClusters.
+// Launch shape of gm_arnoldi_kernel for n unknowns and m columns.  One
+// cluster (<= 16 CTAs, a power of two) per column; each CTA holds `units`
+// unknowns (at most 768 with the widest cluster).  A cluster must fit in one
+// GPC, so not every cluster size lets all m clusters be resident at once: the
+// shape minimises waves x (units + a fixed-cost allowance), with the number of
+// co-resident clusters from cudaOccupancyMaxActiveClusters.
 struct ArnShape {
   int cluster = 1;
   int units = 0;
@@ -1282,7 +1289,7 @@ struct ArnShape {
   size_t smem = 0;
 };
 
-int arnoldi_shape(int n, ArnShape* out) {
+int arnoldi_shape(int n, int m, ArnShape* out) {
   static std::atomic<bool> attr{false};
   int dev = 0, smem_optin = 0;
   BEM_CUDA_TRY(cudaGetDevice(&dev));
@@ -1292,8 +1299,10 @@ int arnoldi_shape(int n, ArnShape* out) {
     BEM_CUDA_TRY(cudaFuncSetAttribute(gm_arnoldi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
     attr.store(true, std::memory_order_release);
   }
+  const int max_cl = g_arn_max_cluster > 0 && g_arn_max_cluster < kArnMaxCluster ? g_arn_max_cluster : kArnMaxCluster;
   int cl = 1;
-  while (cl < kArnMaxCluster && (long long)cl * 2 * kArnThreads < n) cl *= 2;
+  while (cl < max_cl && (long long)cl * 2 * kArnThreads < n) cl *= 2;
+  long long best_cost = -1;
   for (; cl >= 1; cl /= 2) {
     const int units = (((n + cl - 1) / cl) + 1) & ~1;
     int chunk = kChunkMax;
@@ -1312,16 +1321,21 @@ int arnoldi_shape(int n, ArnShape* out) {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, gm_arnoldi_kernel, &cfg) == cudaSuccess && nclusters > 0) {
+    if (cudaOccupancyMaxActiveClusters(&nclusters, gm_arnoldi_kernel, &cfg) != cudaSuccess || nclusters <= 0) {
+      cudaGetLastError();
+      continue;
+    }
+    const long long waves = (m + nclusters - 1) / nclusters;
+    const long long cost = waves * ((long long)units + 512);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
       out->cluster = cl;
       out->units = units;
       out->chunk = chunk;
       out->smem = smem;
-      return BEM_OK;
     }
-    cudaGetLastError();
   }
-  return BEM_ERR_UNSUPPORTED;
+  return best_cost < 0 ? BEM_ERR_UNSUPPORTED : BEM_OK;
 }
 
 }  // namespace
@@ -1416,13 +1430,14 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
 
   const dim3 gv((n + 255) / 256, m);
   const dim3 pair_grid((n + 2 * kPairThreads - 1) / (2 * kPairThreads), m);
-  // re-orthogonalise (CGS2) when a cycle has to reach the full tolerance;
-  // the mixed-precision inner cycles only reduce the residual by inner_rtol
   const bool full_cycle = prec == BEM_PREC_FP32 || prec == BEM_PREC_FP16X3;  // FP32-level matvec
-  const int reorth = (full_cycle || params->inner_rtol < 1e-4) ? 1 : 0;
+  // one classical Gram-Schmidt pass by default: with FP64 dot products and the
+  // FP64-refined outer loop it converged exactly like CGS2 here (same
+  // iterations and residuals at 4 and 10 kHz) for half the basis traffic
+  const int reorth = g_gmres_reorth == 2 ? 1 : 0;
   ArnShape shape;
   {
-    int rc0 = arnoldi_shape(n, &shape);
+    int rc0 = arnoldi_shape(n, m, &shape);
     if (rc0) return rc0;
   }
   // one Arnoldi step: the matvec reads the operand that gm_arnoldi_kernel (or
