@@ -184,6 +184,34 @@ def cpu_baseline(v, t, k, g, pts, budget_s=20.0):
     }
 
 
+# Multi-rank plumbing ("replicas only": every rank solves its own problem, no
+# collective on the data path).
+def rank_barrier(dist, cuda: bool = True) -> None:
+    if dist is not None:
+        dist.barrier()
+    if cuda:
+        import torch
+
+        torch.cuda.synchronize()
+
+
+def max_over_ranks_of(x: float, dist, device) -> float:
+    """The slowest rank's time (device timings are compared as the max over ranks)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_seconds_per_problem(ms_per_step: float, world: int) -> float:
+    """World replicas each finish one problem per step (max-over-ranks step
+    time), so the whole job solves `world` problems per step."""
+    return (ms_per_step / 1e3) / world
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -264,16 +292,10 @@ def run_ours(args):
         return u, p
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        rank_barrier(dist, cuda=True)
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        tt = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return max_over_ranks_of(x, dist, dev)
 
     # ---- warm-up --------------------------------------------------------------
     info = {}
@@ -297,7 +319,7 @@ def run_ours(args):
         l1 = lib.bem_kernel_launches()
     total_ms = max_over_ranks(t_start.elapsed_time(t_end))
     ms_per_step = total_ms / args.steps
-    value = (ms_per_step / 1e3) / world  # whole-job s/problem: world replicas in parallel
+    value = whole_job_seconds_per_problem(ms_per_step, world)
     stages = {n: float(np.mean([r[i].elapsed_time(r[i + 1]) for r in rec])) for i, n in enumerate(stage_names)}
     asm_ms = stages["assemble"]
 
@@ -357,11 +379,16 @@ def run_ours(args):
     clocks = clk.summary()
     peak = fp32_peak_tflops(clocks.get("sm_max_mhz"))
     achieved = F_VK * n_eval / (asm_ms / 1e3) / 1e12
+    # DRAM traffic of regular_sym_kernel: 167.4 MB per launch measured by ncu at
+    # icosphere s4 (N = 2562: the atomic read-modify-write of the two output
+    # matrices), scaled by the units processed, (10242 / 2562)^2, to this mesh
+    traffic = 167.4e6 * (v.shape[0] / 2562.0) ** 2
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None,
-                "kernel": "bem_boundary_matrices_vk (regular_vk_kernel + singular + memset), 63 flop x "
-                          f"{n_eval:.4e} regular quadrature-point pairs per launch; peak = nominal FP32 "
-                          "(SMs x 128 FMA x 2 x max SM clock), no measured FP32 peak available"}
+                "traffic": traffic,
+                "kernel": "bem_boundary_matrices_vk (regular_sym_kernel + singular + memset, timed as one stage), "
+                          f"63 flop x {n_eval:.4e} ordered regular quadrature-point pairs per launch (the kernel "
+                          "evaluates each unordered pair once); peak = nominal FP32 (SMs x 128 FMA x 2 x max SM "
+                          "clock; no measured FP32 peak available); traffic scaled from an s4 ncu capture"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
