@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--kernel-case", choices=["assemble", "solve", "eval"], default=None,
                     help="profiling case: one stage on an icosphere of --subdiv, after one warm-up launch")
     ap.add_argument("--subdiv", type=int, default=4)
+    ap.add_argument("--large-case", action="store_true",
+                    help="large multi-RHS configuration: icosphere s6 (N=40962) with 5%% radial noise, 64 RHS, "
+                         "8 kHz, 4096 listeners (stage times, solver info, FP64 residual)")
     ap.add_argument("--batch-case", action="store_true",
                     help="batching workload: meshes x wavenumbers through the batch runner vs one at a time")
     ap.add_argument("--batch-meshes", type=int, default=16)
@@ -518,9 +521,62 @@ def run_batch_case(args):
     print(json.dumps(line), flush=True)
 
 
+def run_large_case(args):
+    """One problem of the large multi-RHS configuration through the public API
+    (BEM_Solver -> fused assembly -> -V g -> GMRES -> listeners), timed per
+    stage with CUDA events after one warm-up problem."""
+    import torch
+
+    from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
+    from neuralat_b200.bem import meshes as M
+
+    w = M.large_multi_rhs(m=64)
+    v = torch.from_numpy(w["vertices"].astype(np.float32)).cuda()
+    t = torch.from_numpy(w["triangles"].astype(np.int32)).cuda()
+    g = torch.from_numpy(w["neumann"].astype(np.complex64)).cuda()
+    pts = torch.from_numpy(w["points"].astype(np.float32)).cuda()
+    k = float(w["k"])
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        return e
+
+    def problem(info):
+        e = [ev()]
+        s = BEM_Solver(v, t)
+        e.append(ev())
+        V, A = s.assemble_vk(k)
+        e.append(ev())
+        rhs = -cmatmul(V, g)
+        del V
+        e.append(ev())
+        u = gmres(A, rhs, rtol=1e-6, precision=args.precision, info=info)
+        e.append(ev())
+        p = s.boundary2potential(k, g, u, pts)
+        e.append(ev())
+        torch.cuda.synchronize()
+        return e, p
+
+    problem({})
+    info = {}
+    e, p = problem(info)
+    names = ["geometry", "assemble", "rhs", "solve", "eval"]
+    stages = {n: e[i].elapsed_time(e[i + 1]) for i, n in enumerate(names)}
+    line = {"case": "large_multi_rhs", "N": int(v.shape[0]), "T": int(t.shape[0]), "rhs": int(g.shape[1]),
+            "listeners": int(pts.shape[0]), "k": k, "precision": args.precision,
+            "s_per_problem": e[0].elapsed_time(e[-1]) / 1e3, "stages_ms": stages,
+            "solver": {kk: info.get(kk) for kk in ("iterations", "refinements", "matvecs", "rel_residual", "status")},
+            "pressure_finite": bool(torch.isfinite(torch.view_as_real(p)).all()),
+            "peak_device_gb": torch.cuda.max_memory_allocated() / 1e9}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.batch_case:
+    if args.large_case:
+        run_large_case(args)
+    elif args.batch_case:
         run_batch_case(args)
     elif args.kernel_case:
         run_kernel_case(args)

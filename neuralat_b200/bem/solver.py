@@ -129,7 +129,7 @@ def gmres(A: torch.Tensor, b: torch.Tensor, x=None, *, rtol=1e-5, atol=0.0, max_
     p.max_refine = int(max_refine if max_refine is not None else (2 if prec in (L.PREC_FP32, L.PREC_FP16X3) else 6))
     p.rtol = float(rtol)
     p.atol = float(atol)
-    p.inner_rtol = float(inner_rtol if inner_rtol is not None else (1e-3 if prec == L.PREC_BF16X3 else 3e-2))
+    p.inner_rtol = float(inner_rtol if inner_rtol is not None else (3e-2 if prec == L.PREC_BF16 else 1e-3))
     lib = L.lib()
     ws_bytes = int(lib.bem_gmres_workspace_bytes(n, m, ctypes.byref(p)))
     if ws_bytes == 0:

@@ -989,7 +989,7 @@ int set_tuning(int key, int value) {
       g_gmres_reorth = value;
       return BEM_OK;
     case BEM_TUNE_ARNOLDI_CLUSTER:
-      if (value > 16 || (value & (value - 1))) return BEM_ERR_INVALID_ARGUMENT;
+      if (value > 16) return BEM_ERR_INVALID_ARGUMENT;
       g_arn_max_cluster = value;
       return BEM_OK;
   }

@@ -575,19 +575,19 @@ __device__ __forceinline__ const float2* vrow(const GmPtrs& P, int s, int l) {
 
 // Warp reduce-scatter of NV doubles (NV a power of two, 2..32): afterwards
 // the returned value of lane L is the warp total of value L >> (5 - log2 NV).
-template <int NV>
-__device__ __forceinline__ double warp_reduce_scatter(double (&v)[NV], int lane) {
+template <int NV, typename T>
+__device__ __forceinline__ T warp_reduce_scatter(T (&v)[NV], int lane) {
 #pragma unroll
   for (int half = NV / 2, off = 16; half >= 1; half >>= 1, off >>= 1) {
     const bool upper = (lane & off) != 0;
 #pragma unroll
     for (int j = 0; j < half; j++) {
-      const double send = upper ? v[j] : v[j + half];
-      const double keep = upper ? v[j + half] : v[j];
+      const T send = upper ? v[j] : v[j + half];
+      const T keep = upper ? v[j + half] : v[j];
       v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
     }
   }
-  double t = v[0];
+  T t = v[0];
 #pragma unroll
   for (int off = 16 / NV; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
   return t;
@@ -640,6 +640,7 @@ struct ArnSmem {
   uint64_t full[kRingStages];     // bulk-copy completion of each ring stage
   uint64_t empty[kRingStages];    // consumer warps done with the stage
   double red[kArnWarps][2 * kChunkMax];
+  double dred[2][kArnConsumerWarps][2 * kChunkMax];  // dot-pass partials per consumer warp, double-buffered
   double part1[2 * kMaxRestart];  // this CTA's partial h1 (re, im), read by the whole cluster
   double part2[2 * kMaxRestart];  // partial h2
   double part3[2];                // partial |w''|^2
@@ -682,8 +683,11 @@ struct ArnStream {
     const uint32_t row_bytes = (uint32_t)ucta * 8u;
     mbar_expect_tx(&S->full[st], row_bytes * (uint32_t)nl);
     float2* dst = stage_rows(g);
+    // the basis is re-read every step: keep it in L2 while the matvec streams
+    // the matrix evict-first
+    const uint64_t pol = l2_evict_last_policy();
     for (int li = 0; li < nl; li++)
-      bulk_load(dst + (size_t)li * units, vrow(*P, s, l0 + li) + i0, row_bytes, &S->full[st]);
+      bulk_load_hint(dst + (size_t)li * units, vrow(*P, s, l0 + li) + i0, row_bytes, &S->full[st], pol);
   }
   // consumer warps: wait for the chunk's rows
   __device__ const float2* acquire(int pass, int c) const {
@@ -698,33 +702,49 @@ struct ArnStream {
   }
 };
 
-// Dots pass (consumer warps): warp w reduces row l0 + w of each chunk,
-// part[2l + c] = sum over this CTA's unknowns of conj(V[l]) w.
-__device__ __forceinline__ void arn_dots(const ArnStream& T, int pass, const double2* __restrict__ wsl, int npairs,
-                                         double* part) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Dots pass (consumer threads own pairs, as in the update pass):
+// part[2l + c] = sum over this CTA's unknowns of conj(V[l]) w.  Each thread
+// forms its pairs' products for every row of the chunk in FP32 (w rounded
+// to FP32 like the stored basis), a warp reduce-scatter sums the lanes, and
+// the consumer warps' partials are added in FP64 behind one named barrier
+// (consumers only; the partial arrays are double-buffered by chunk parity).
+__device__ __forceinline__ void consumer_barrier() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kArnConsumers) : "memory");
+}
+
+__device__ __forceinline__ void arn_dots(const ArnStream& T, ArnSmem& S, int pass, const double2* __restrict__ wsl,
+                                         int npairs, double* part) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int c = 0; c < T.nch; c++) {
     const float2* rows = T.acquire(pass, c);
     const int l0 = c * T.chunk, nl = min(T.chunk, T.k + 1 - l0);
-    if (warp < nl) {
-      double re = 0.0, im = 0.0;
-      for (int p = lane; p < npairs; p += 32) {
-        const float4 a = staged_pair(rows, warp, T.units, p, T.i0 + 2 * p + 1 >= T.P->n);
-        const double2 w0 = wsl[2 * p], w1 = wsl[2 * p + 1];
-        re += (double)a.x * w0.x + (double)a.y * w0.y + (double)a.z * w1.x + (double)a.w * w1.y;
-        im += (double)a.x * w0.y - (double)a.y * w0.x + (double)a.z * w1.y - (double)a.w * w1.x;
-      }
+    float v[2 * kChunkMax];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_xor_sync(0xffffffffu, re, o);
-        im += __shfl_xor_sync(0xffffffffu, im, o);
-      }
-      if (lane == 0) {
-        part[2 * (l0 + warp)] = re;
-        part[2 * (l0 + warp) + 1] = im;
+    for (int q = 0; q < 2 * kChunkMax; q++) v[q] = 0.f;
+    for (int p = tid; p < npairs; p += kArnConsumers) {
+      const bool pad = T.i0 + 2 * p + 1 >= T.P->n;
+      const double2 w0d = wsl[2 * p], w1d = wsl[2 * p + 1];
+      const float4 w = make_float4((float)w0d.x, (float)w0d.y, (float)w1d.x, (float)w1d.y);
+#pragma unroll
+      for (int li = 0; li < kChunkMax; li++) {
+        if (li < nl) {
+          const float4 a = staged_pair(rows, li, T.units, p, pad);
+          v[2 * li] = fmaf(a.x, w.x, fmaf(a.y, w.y, fmaf(a.z, w.z, fmaf(a.w, w.w, v[2 * li]))));
+          v[2 * li + 1] = fmaf(a.x, w.y, fmaf(-a.y, w.x, fmaf(a.z, w.w, fmaf(-a.w, w.z, v[2 * li + 1]))));
+        }
       }
     }
+    const float t = warp_reduce_scatter<2 * kChunkMax>(v, lane);
+    double (*red)[2 * kChunkMax] = S.dred[c & 1];
+    if ((lane & 1) == 0) red[warp][lane >> 1] = (double)t;
+    consumer_barrier();  // all partials written; every consumer is done with the stage
     T.release(pass, c);
+    if (tid < 2 * nl) {
+      double sum = 0.0;
+#pragma unroll
+      for (int w = 0; w < kArnConsumerWarps; w++) sum += red[w][tid];
+      part[2 * l0 + tid] = sum;
+    }
   }
 }
 
@@ -936,7 +956,7 @@ __global__ void __launch_bounds__(kArnThreads, 1) gm_arnoldi_kernel(GmPtrs P, in
       first = min(kRingStages, T.nch);
       __syncwarp();
     } else if (dots) {
-      arn_dots(T, pass, wsl, npairs, part);
+      arn_dots(T, S, pass, wsl, npairs, part);
     } else {
       arn_update(T, pass, coef, wsl, npairs);
     }
@@ -1277,10 +1297,11 @@ int host_ring(int m, HostRing** r) {
 }
 
 // Launch shape of gm_arnoldi_kernel for n unknowns and m columns.  One
-// cluster (<= 16 CTAs, a power of two) per column; each CTA holds `units`
-// unknowns (at most 768 with the widest cluster).  A cluster must fit in one
-// GPC, so not every cluster size lets all m clusters be resident at once: the
-// shape minimises waves x (units + a fixed-cost allowance), with the number of
+// cluster (<= 16 CTAs, any size) per column; each CTA holds `units` unknowns.
+// The step streams the basis once per pass through every CTA, so more CTAs
+// per column means fewer bytes per SM, but a cluster must fit in one GPC and
+// not every size lets all m clusters be resident at once: the shape
+// minimises waves x (units + a fixed-cost allowance), with the number of
 // co-resident clusters from cudaOccupancyMaxActiveClusters.
 struct ArnShape {
   int cluster = 1;
@@ -1301,9 +1322,9 @@ int arnoldi_shape(int n, int m, ArnShape* out) {
   }
   const int max_cl = g_arn_max_cluster > 0 && g_arn_max_cluster < kArnMaxCluster ? g_arn_max_cluster : kArnMaxCluster;
   int cl = 1;
-  while (cl < max_cl && (long long)cl * 2 * kArnThreads < n) cl *= 2;
+  while (cl < max_cl && (long long)cl * 2 * kArnThreads < n) cl++;
   long long best_cost = -1;
-  for (; cl >= 1; cl /= 2) {
+  for (; cl >= 1; cl--) {
     const int units = (((n + cl - 1) / cl) + 1) & ~1;
     int chunk = kChunkMax;
     while (chunk > 1 && arn_smem_bytes(units, chunk) > (size_t)smem_optin) chunk--;
@@ -1430,7 +1451,9 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
 
   const dim3 gv((n + 255) / 256, m);
   const dim3 pair_grid((n + 2 * kPairThreads - 1) / (2 * kPairThreads), m);
-  const bool full_cycle = prec == BEM_PREC_FP32 || prec == BEM_PREC_FP16X3;  // FP32-level matvec
+  // FP32-level matvec: CUDA-core FP32, or fp16x3 up to 64 right-hand sides
+  // (wider tensor-core tiles accumulate whole rows in tensor memory, ~3e-5)
+  const bool full_cycle = prec == BEM_PREC_FP32 || (prec == BEM_PREC_FP16X3 && m <= 64);
   // one classical Gram-Schmidt pass by default: with FP64 dot products and the
   // FP64-refined outer loop it converged exactly like CGS2 here (same
   // iterations and residuals at 4 and 10 kHz) for half the basis traffic

@@ -22,9 +22,10 @@
 // Accumulation: the tensor core's in-place FP32 accumulation over a long K
 // range loses precision (measured: ~3e-5 relative on the BEM matrix whatever
 // the operand split), so accumulator segments are short (`promote` K blocks,
-// two by default for N <= 64): after each segment the epilogue adds the
-// tensor-memory sum to per-row registers with round-to-nearest FP32 adds and
-// writes Y once per row block (fp16x3 then matches an FP32 matvec, ~5e-7).
+// two by default for N <= 128, i.e. up to 64 right-hand sides): after each
+// segment the epilogue adds the tensor-memory sum to per-row registers with
+// round-to-nearest FP32 adds and writes Y once per row block (fp16x3 then
+// matches an FP32 matvec, ~5e-7).
 //
 // Kernel: one CTA per SM, stream-K over (128-row block, 64-wide K block)
 // units so every SM streams the same number of A bytes; warp 0 issues TMA
@@ -126,7 +127,7 @@ struct TcSmem {
   static constexpr int kStages = (kSmemBudget / kStageBytes) > 8 ? 8 : (kSmemBudget / kStageBytes);
   // tensor-memory accumulators in flight: with one-K-block segments the MMA
   // issuer runs up to kAccBufs segments ahead of the epilogue
-  static constexpr int kAccBufs = NB <= 64 ? 4 : 2;
+  static constexpr int kAccBufs = NB <= 128 ? 4 : 2;
   static constexpr int kTmemCols = (kAccBufs * NB <= 32)    ? 32
                                    : (kAccBufs * NB <= 64)  ? 64
                                    : (kAccBufs * NB <= 128) ? 128
@@ -258,11 +259,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   } else if (warp >= 2) {
     // ---------------- epilogue: TMEM -> registers -> atomics into Y ----------------
-    // Each lane owns one row.  With NB <= 64 the segment sums are added in
+    // Each lane owns one row.  With NB <= 128 the segment sums are added in
     // registers (round-to-nearest FP32) and Y receives one atomic per entry
     // when the row block (or this CTA's range) ends; wider tiles add every
     // segment to Y directly.
-    constexpr bool kRegAcc = NB <= 64;
+    constexpr bool kRegAcc = NB <= 128;
     const int quarter = warp & 3;  // TMEM lanes this warp may access
     int buf = 0;
     uint32_t acc_phase = 0;
@@ -573,7 +574,7 @@ int launch_tc(const TcLayout& L, char* ws, int n, const int* active, int nact, f
   a.cinv = F16 ? (const float*)(ws + L.cinv) : nullptr;
   // two K blocks per segment: fp16x3 error 6e-7 on the BEM matrix (one block:
   // 4e-7 but 18% slower; 16 blocks: 4e-6; a whole row block: 3e-5)
-  a.promote = g_tc_promote > 0 ? g_tc_promote : (NB <= 64 ? 2 : (1ll << 40));
+  a.promote = g_tc_promote > 0 ? g_tc_promote : (NB <= 128 ? 2 : (1ll << 40));
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

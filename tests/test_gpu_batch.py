@@ -85,16 +85,16 @@ def test_batch_runner_matches_per_problem(solvers):
     gs = [M.smoothed_gaussian_field(v.shape[0], t, 3, seed=i) for i, (v, t) in enumerate(ms)]
     pts = M.sphere_points(64, 1.0, seed=3)
     # a tiny budget forces several waves
-    runner = BatchRunner(memory_budget_bytes=3 * 8 * 642 * 642 * 2, workers=3, precision="fp32", rtol=1e-6)
+    runner = BatchRunner(memory_budget_bytes=3 * 8 * 642 * 642 * 2, workers=3, precision="fp32", rtol=1e-7)
     res = runner.run(ms, ks, gs, pts, return_dirichlet=True)
     assert sorted(res.index) == sorted((mi, ki) for mi in range(3) for ki in range(len(ks[mi])))
     ptt = torch.as_tensor(pts, dtype=torch.float32, device="cuda")
     for (mi, ki), p, u, info in zip(res.index, res.pressure, res.dirichlet, res.info):
         s = BEM_Solver(*ms[mi])
         g = torch.as_tensor(gs[mi], dtype=torch.complex64, device="cuda")
-        u1 = s.CBIE(ks[mi][ki], g, rtol=1e-6)
+        u1 = s.CBIE(ks[mi][ki], g, rtol=1e-7)  # both solves tight: the solutions may differ by cond x rtol
         p1 = s.boundary2potential(ks[mi][ki], g, u1, ptt)
-        assert info["rel_residual"] <= 1e-5
+        assert info["rel_residual"] <= 1e-7
         assert relfro(u.cpu(), u1.cpu()) <= 1e-4
         assert relfro(p.cpu(), p1.cpu()) <= 1e-4
 

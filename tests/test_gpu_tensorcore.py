@@ -58,7 +58,8 @@ def test_fp16x3_scales_rows_and_columns_of_any_magnitude():
     assert np.max(np.abs(Y - ref) / scale) <= 3e-6
 
 
-def test_fp16x3_matvec_of_a_bem_matrix_matches_fp32():
+@pytest.mark.parametrize("m", [8, 64])
+def test_fp16x3_matvec_of_a_bem_matrix_matches_fp32(m):
     """On a Galerkin CBIE matrix (dominant mass diagonal, oscillatory far
     field) the fp16x3 operator with short accumulator segments is as accurate
     as an FP32 matvec (relative error <= 2e-6; a long in-place tensor-memory
@@ -68,7 +69,7 @@ def test_fp16x3_matvec_of_a_bem_matrix_matches_fp32():
     s = BEM_Solver(v, t)
     _, A = s.assemble_vk(M.wavenumber(4000.0))
     rng = np.random.default_rng(4)
-    X = torch.from_numpy((rng.standard_normal((A.shape[0], 8)) + 1j * rng.standard_normal((A.shape[0], 8)))
+    X = torch.from_numpy((rng.standard_normal((A.shape[0], m)) + 1j * rng.standard_normal((A.shape[0], m)))
                          .astype(np.complex64)).cuda()
     Y = tc_matmul(A, X, L.PREC_FP16X3).to(torch.complex128)
     ref = A.to(torch.complex128) @ X.to(torch.complex128)
