@@ -131,6 +131,11 @@ size_t bem_batch_workspace_bytes(int nproblems);
 int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, float mass_coeff, float k_coeff,
                           void* workspace, size_t workspace_bytes, bem_stream_t stream);
 
+/* BEM_OK, or BEM_ERR_CUDA if a bounded wait of an assembly kernel (the
+ * bulk copies of trial tiles) expired since the last call; clears the flag
+ * and synchronises `stream`.  No counterpart in the reference. */
+int bem_assembly_status(bem_stream_t stream);
+
 /* Launch-shape knobs of the assembly kernels, set by the autotuner
  * (0 = automatic).  Process-wide. */
 enum {

@@ -39,7 +39,7 @@ EXPORTED = (
     "bem_tc_operator_bytes", "bem_tc_operator_prepare", "bem_tc_matmul", "bem_tc_status",
     "bem_boundary2potential_noalloc_max", "bem_boundary2potential_noalloc",
     "bem_cmatmul_adjoint", "bem_conj_transpose", "bem_boundary2potential_adjoint", "bem_vertex_gradient",
-    "bem_batch_workspace_bytes", "bem_batch_matrices_vk", "bem_set_tuning", "bem_get_tuning",
+    "bem_batch_workspace_bytes", "bem_batch_matrices_vk", "bem_set_tuning", "bem_assembly_status", "bem_get_tuning",
 )
 
 
@@ -130,6 +130,7 @@ def lib():
         "bem_batch_workspace_bytes": ([i], sz),
         "bem_batch_matrices_vk": ([P(BatchProblem), i, f, f, vp, sz, vp], i),
         "bem_set_tuning": ([i, i], i),
+        "bem_assembly_status": ([vp], i),
         "bem_get_tuning": ([i], i),
     }
     for name, (argt, rest) in sigs.items():

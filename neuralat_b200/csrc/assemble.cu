@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "async_copy.cuh"
 #include "bem_common.cuh"
 
 namespace bemb {
@@ -273,10 +274,23 @@ struct SymSmem {
   float2 slotK[kTestCorners][kSlotStride];
   float2 slotM[kTestCorners][kSlotStride];  // K_ji^T, indexed like slotK
   float xs[18][kTestTris];                  // test quadrature points, [coordinate][lane]
-  TriRec trial[kTile];
-  TileRec tileJ;
+  TriRec trial[2][kTile];                   // trial tile records, double-buffered
+  TileRec tileJ[2];
   TileRec tileI[2];
+  uint64_t tile_full[2];                    // bulk-copy completion of each trial buffer
 };
+
+// A bounded wait of the assembly kernels expired (read by bem_assembly_status).
+__device__ int g_asm_err;
+
+// Thread 0: bulk-copy trial tile jt (records and vertex table) into buffer b.
+__device__ __forceinline__ void sym_fetch_tile(SymSmem& sm, const GeomView& g, int jt, int b) {
+  const int ntri = min(kTile, g.nt - jt * kTile);
+  const uint32_t rec_bytes = (uint32_t)(ntri * sizeof(TriRec));
+  mbar_expect_tx(&sm.tile_full[b], rec_bytes + (uint32_t)sizeof(TileRec));
+  bulk_load(sm.trial[b], &g.rec[jt * kTile], rec_bytes, &sm.tile_full[b]);
+  bulk_load(&sm.tileJ[b], &g.tiles[jt], (uint32_t)sizeof(TileRec), &sm.tile_full[b]);
+}
 
 // aV, aK as pair_block; aM[3a+b] = sum_pq C_ap C_bq dn_i(q) Gk(r_pq) = K_ji[b][a].
 __device__ __forceinline__ void pair_block_sym(const float (*xs)[kTestTris], int lane, const float (&yq)[18],
@@ -341,9 +355,11 @@ __device__ __forceinline__ void pair_block_sym(const float (*xs)[kTestTris], int
   }
 }
 
+// `uses` counts the trial tiles this CTA has processed (buffer = uses & 1,
+// mbarrier parity = (uses >> 1) & 1).
 __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g, float k, float2* __restrict__ V,
                                                  float2* __restrict__ K, float v_scale, float k_scale, int grp,
-                                                 int jt_begin, int jt_end) {
+                                                 int jt_begin, int jt_end, unsigned& uses) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nt = g.nt, nv = g.nv;
   const int tile0 = 2 * grp;
@@ -355,7 +371,8 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
   const float nix = ri.n[0], niy = ri.n[1], niz = ri.n[2], cix = ri.c[0], ciy = ri.c[1], ciz = ri.c[2];
   const int iv0 = ri.v[0], iv1 = ri.v[1], iv2 = ri.v[2];
 
-  __syncthreads();  // the previous item is done with tileI and xs
+  __syncthreads();  // the previous item is done with tileI, xs and both trial buffers
+  if (tid == 0) sym_fetch_tile(sm, g, jt_begin, uses & 1);
   copy_words(&sm.tileI[0], &g.tiles[tile0], sizeof(TileRec), tid, kSymThreads);
   if (has_t1) copy_words(&sm.tileI[1], &g.tiles[tile0 + 1], sizeof(TileRec), tid, kSymThreads);
   for (int e = tid; e < 18 * kTestTris; e += kSymThreads) {
@@ -364,19 +381,24 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     sm.xs[c][l] = g.rec[t].qp[c];
   }
 
-  for (int jt = jt_begin; jt < jt_end; jt++) {
-    __syncthreads();  // gather of the previous trial tile is done with the slots
-    copy_words(&sm.tileJ, &g.tiles[jt], sizeof(TileRec), tid, kSymThreads);
+  for (int jt = jt_begin; jt < jt_end; jt++, uses++) {
+    const int bf = uses & 1;
+    __syncthreads();  // the previous tile's gather is done with the slots and with buffer bf ^ 1
+    if (tid == 0 && jt + 1 < jt_end) sym_fetch_tile(sm, g, jt + 1, bf ^ 1);
+    if (!mbar_wait(&sm.tile_full[bf], (uses >> 1) & 1u, &g_asm_err)) {
+      // expired (flag raised): let the copy land before the buffer is reused
+      mbar_wait_drain(&sm.tile_full[bf], (uses >> 1) & 1u);
+    }
+    const TriRec* trial = sm.trial[bf];
+    const TileRec& tileJ = sm.tileJ[bf];
     const int ntriJ = min(kTile, nt - jt * kTile);
-    copy_words(sm.trial, &g.rec[jt * kTile], ntriJ * (int)sizeof(TriRec), tid, kSymThreads);
-    __syncthreads();
 
     // ---- compute: warp w takes trial triangle w ----
     const int tt = warp;
     const int tj = jt * kTile + tt;
     float aa = 0.f;
     if (tt < ntriJ) {
-      const TriRec& rj = sm.trial[tt];
+      const TriRec& rj = trial[tt];
       const int j0 = rj.v[0], j1 = rj.v[1], j2 = rj.v[2];
       const bool touching = (iv0 == j0) | (iv0 == j1) | (iv0 == j2) | (iv1 == j0) | (iv1 == j1) | (iv1 == j2) |
                             (iv2 == j0) | (iv2 == j1) | (iv2 == j2);
@@ -385,7 +407,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
       aa = (valid_i && !touching && once) ? area_i * rj.area : 0.f;
     }
     if (tt < ntriJ && __any_sync(0xffffffffu, aa != 0.f)) {
-      const TriRec& rj = sm.trial[tt];
+      const TriRec& rj = trial[tt];
       float yq[18];
 #pragma unroll
       for (int e = 0; e < 18; e++) yq[e] = rj.qp[e];
@@ -419,7 +441,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
     const int nI0 = sm.tileI[0].nlv;
     const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
-    const int nJ = sm.tileJ.nlv;
+    const int nJ = tileJ.nlv;
     const int total = (nI0 + nI1) * nJ;
     for (int e = tid; e < total; e += kSymThreads) {
       const int ai = e / nJ;
@@ -429,11 +451,11 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
       const TileRec& TI = sm.tileI[s];
       float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f), acc_m = make_float2(0.f, 0.f);
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
-      const int cb0 = sm.tileJ.lv_ptr[b], cb1 = sm.tileJ.lv_ptr[b + 1];
+      const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
       for (int ca = ca0; ca < ca1; ca++) {
         const int row = s * kTileCorners + TI.lv_corner[ca];
         for (int cb = cb0; cb < cb1; cb++) {
-          const int col = sm.tileJ.lv_corner[cb];
+          const int col = tileJ.lv_corner[cb];
           acc_v.x += sm.slotV[row][col].x;
           acc_v.y += sm.slotV[row][col].y;
           acc_k.x += sm.slotK[row][col].x;
@@ -442,7 +464,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
           acc_m.y += sm.slotM[row][col].y;
         }
       }
-      const int A = TI.vid[a], B = sm.tileJ.vid[b];
+      const int A = TI.vid[a], B = tileJ.vid[b];
       if (acc_v.x != 0.f || acc_v.y != 0.f || acc_k.x != 0.f || acc_k.y != 0.f || acc_m.x != 0.f ||
           acc_m.y != 0.f) {
         atomicAdd(&V[(size_t)A * nv + B], acc_v);
@@ -478,6 +500,12 @@ __global__ void __launch_bounds__(kSymThreads, 1)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SymSmem& sm = *reinterpret_cast<SymSmem*>(smem_raw);
   const int ngroups = (g.nt + kTestTris - 1) / kTestTris;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.tile_full[0], 1);
+    mbar_init(&sm.tile_full[1], 1);
+    mbar_init_fence();
+  }
+  unsigned uses = 0;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     long long pos = (long long)item * chunk;
     const long long end = pos + chunk < n_units ? pos + chunk : n_units;
@@ -487,7 +515,7 @@ __global__ void __launch_bounds__(kSymThreads, 1)
       const long long gend = base + (g.ntiles - 2 * grp);
       const long long stop = end < gend ? end : gend;
       const int jt0 = 2 * grp + (int)(pos - base);
-      regular_sym_item(sm, g, k, V, K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos));
+      regular_sym_item(sm, g, k, V, K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos), uses);
       pos = stop;
     }
   }
@@ -977,6 +1005,16 @@ thread_local PinnedStage t_stage;
 
 inline size_t al256b(size_t x) { return (x + 255) / 256 * 256; }
 }  // namespace
+
+// Reads and clears the flag that an assembly kernel's bounded wait expired
+// (synchronises the stream).
+int assembly_status(int* err_host, cudaStream_t s) {
+  int zero = 0;
+  BEM_CUDA_TRY(cudaMemcpyFromSymbolAsync(err_host, g_asm_err, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaMemcpyToSymbolAsync(g_asm_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  return BEM_OK;
+}
 
 int set_tuning(int key, int value) {
   if (value < 0) return BEM_ERR_INVALID_ARGUMENT;

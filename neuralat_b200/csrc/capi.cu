@@ -7,6 +7,7 @@
 #include "bem_common.cuh"
 
 namespace bemb {
+int assembly_status(int* err_host, cudaStream_t s);
 int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
 int assemble_vk(const GeomView& g, float k, float2* V, float2* Kout, float mass_coeff, float k_coeff, cudaStream_t s);
 int assemble_mass(const GeomView& g, float2* M, float coeff, bool zero, cudaStream_t s);
@@ -101,4 +102,11 @@ extern "C" int bem_batch_matrices_vk(const bem_batch_problem* problems, int npro
   }
   return assemble_vk_batch(views.data(), ks.data(), Vs.data(), Ks.data(), nproblems, mass_coeff, k_coeff, workspace,
                            workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" int bem_assembly_status(bem_stream_t stream) {
+  int err = 0;
+  const int rc = assembly_status(&err, (cudaStream_t)stream);
+  if (rc) return rc;
+  return err ? BEM_ERR_CUDA : BEM_OK;
 }

@@ -11,6 +11,7 @@ import torch
 from neuralat_b200 import _lib as L
 from neuralat_b200.bem import BEM_Solver, cmatmul, gmres, map_triangle2vertex, solve_linear_equation
 from neuralat_b200.bem import meshes as M
+from neuralat_b200.bem.solver import _stream
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -65,6 +66,7 @@ def test_s3_vk_vs_oracle(solvers):
     k = M.wavenumber(1000.0)
     s = solvers["s3"]
     V, lhs = s.assemble_vk(k)
+    assert L.lib().bem_assembly_status(_stream()) == L.BEM_OK  # no bounded wait expired
     Mo = O.identity_matrix(*_mesh("s3"))
     assert relfro(V.cpu().numpy(), oracle_matrix("single", "s3", k)) <= MAT_TOL
     assert relfro(lhs.cpu().numpy(), 0.5 * Mo - oracle_matrix("double", "s3", k)) <= MAT_TOL
