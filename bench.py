@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--large-case", action="store_true",
                     help="large multi-RHS configuration: icosphere s6 (N=40962) with 5%% radial noise, 64 RHS, "
                          "8 kHz, 4096 listeners (stage times, solver info, FP64 residual)")
+    ap.add_argument("--grad-case", action="store_true",
+                    help="differentiation configuration: icosphere s4, 2 kHz, one RHS, 128 listeners, "
+                         "L = sum |p|^2, forward + hand-written adjoint backward (dL/dvertices, dL/dneumann)")
     ap.add_argument("--batch-case", action="store_true",
                     help="batching workload: meshes x wavenumbers through the batch runner vs one at a time")
     ap.add_argument("--batch-meshes", type=int, default=16)
@@ -488,35 +491,51 @@ def run_batch_case(args):
     pts_d = torch.from_numpy(pts.astype(np.float32)).cuda()
 
     def one_at_a_time():
-        out = []
+        infos = []
         for (v, t), kk, g in zip(meshes, ks, gs):
             s = BEM_Solver(v, t)
             gd = torch.from_numpy(g).cuda()
             for k in kk:
-                _, p = s.solve_and_evaluate(k, gd, pts_d, precision=args.precision, rtol=1e-6)
-                out.append(p)
+                infos.append({})
+                s.solve_and_evaluate(k, gd, pts_d, precision=args.precision, rtol=1e-6, info=infos[-1])
         torch.cuda.synchronize()
-        return out
+        return infos
 
     tuned = autotune.tune_assembly([BEM_Solver(v, t) for v, t in meshes[:8]], [k[0] for k in ks[:8]], repeats=2)
     runner = BatchRunner(workers=4, precision=args.precision, rtol=1e-6)
-    runner.run(meshes[:2], [k[:1] for k in ks[:2]], gs[:2], pts)  # warm-up
+    # warm-up: a few problems of every mesh size, so each worker thread has its stream and buffers
+    warm, seen = [], {}
+    for i, (v, _) in enumerate(meshes):
+        if seen.get(v.shape[0], 0) < 4:
+            seen[v.shape[0]] = seen.get(v.shape[0], 0) + 1
+            warm.append(i)
+    runner.run([meshes[i] for i in warm], [ks[i][:1] for i in warm], [gs[i] for i in warm], pts)
     one_at_a_time()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    one_at_a_time()
+    seq_infos = one_at_a_time()
     t_seq = time.perf_counter() - t0
     t0 = time.perf_counter()
     res = runner.run(meshes, ks, gs, pts)
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
+    runner.close()
+    by_conc = {}
+    for w in res.waves:
+        c = by_conc.setdefault(str(w["concurrency"]), {"problems": 0, "seconds": 0.0})
+        c["problems"] += w["problems"]
+        c["seconds"] += w["seconds"]
     line = {
         "case": "batching", "problems": nprob, "meshes": len(meshes),
         "vertices": sorted({int(m[0].shape[0]) for m in meshes}), "rhs": 16, "listeners": int(pts.shape[0]),
         "precision": args.precision, "tuning": {k: tuned[k] for k in ("chunk", "ctas_per_sm")},
         "one_at_a_time_problems_per_s": nprob / t_seq, "batched_problems_per_s": nprob / t_batch,
         "speedup": t_seq / t_batch,
-        "max_rel_residual": max(i.get("rel_residual", 0.0) for i in res.info),
+        "max_rel_residual_converged": max((i.get("rel_residual", 0.0) for i in res.info if i.get("status") == 0),
+                                          default=None),
+        "not_converged": sum(1 for i in res.info if i.get("status") != 0),
+        "one_at_a_time_not_converged": sum(1 for i in seq_infos if i.get("status") != 0),
+        "waves_by_concurrency": by_conc,
     }
     print(json.dumps(line), flush=True)
 
@@ -572,9 +591,54 @@ def run_large_case(args):
     print(json.dumps(line), flush=True)
 
 
+def run_grad_case(args):
+    """Forward and backward time of the differentiable listener pressures
+    (neuralat_b200.bem.listener_pressure) on the differentiation workload."""
+    import torch
+
+    from neuralat_b200.bem import listener_pressure
+    from neuralat_b200.bem import meshes as M
+
+    w = M.differentiation()
+    v0 = torch.from_numpy(w["vertices"].astype(np.float32)).cuda()
+    t = torch.from_numpy(w["triangles"].astype(np.int32)).cuda()
+    g0 = torch.from_numpy(w["neumann"].astype(np.complex64)).cuda()
+    pts = torch.from_numpy(w["points"].astype(np.float32)).cuda()
+    k = float(w["k"])
+
+    def once():
+        v = v0.clone().requires_grad_(True)
+        g = g0.clone().requires_grad_(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        p = listener_pressure(v, g, t, pts, k)
+        loss = (p.real ** 2 + p.imag ** 2).sum()
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2), v.grad, g.grad
+
+    for _ in range(max(args.warmup, 1)):
+        once()
+    runs = [once() for _ in range(max(args.steps, 1))]
+    fwd = float(np.median([r[0] for r in runs]))
+    bwd = float(np.median([r[1] for r in runs]))
+    vg, gg = runs[-1][2], runs[-1][3]
+    line = {"case": "differentiation", "N": int(v0.shape[0]), "T": int(t.shape[0]), "listeners": int(pts.shape[0]),
+            "k": k, "forward_ms": fwd, "backward_ms": bwd, "steps": len(runs),
+            "grad_finite": bool(torch.isfinite(vg).all() and torch.isfinite(torch.view_as_real(gg)).all()),
+            "grad_vertices_norm": float(vg.norm()), "grad_neumann_norm": float(gg.abs().norm())}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.large_case:
+    if args.grad_case:
+        run_grad_case(args)
+    elif args.large_case:
         run_large_case(args)
     elif args.batch_case:
         run_batch_case(args)

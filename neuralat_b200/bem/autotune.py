@@ -1,8 +1,8 @@
 """Autotuner for the assembly launch shape.
 
 Times the batched fused assembly (``bem_batch_matrices_vk``) of a sample of
-problems for every candidate (trial tiles per work item, persistent CTAs per
-SM), keeps the fastest, and installs it with ``bem_set_tuning``.  Results are
+problems for every candidate (used (test group, trial tile) units per work
+item, persistent CTAs per SM), keeps the fastest, and installs it with ``bem_set_tuning``.  Results are
 cached per GPU model and problem-size signature in a JSON file
 (``$NEURALAT_B200_CACHE`` or ``~/.cache/neuralat_b200/autotune.json``), so a
 later process reuses them without re-timing.
@@ -17,8 +17,8 @@ import torch
 from .. import _lib as L
 from .batch import assemble_batch
 
-CHUNKS = (1, 2, 4, 8, 16, 32)
-CTAS = (1, 2)
+CHUNKS = (2, 4, 8, 16, 32, 64)
+CTAS = (1,)  # the symmetric regular-pair kernel holds one CTA per SM
 
 
 def _cache_path() -> str:
@@ -30,7 +30,7 @@ def _signature(solvers) -> str:
     sizes = sorted(s.geometry.nt for s in solvers)
     gpu = torch.cuda.get_device_name()
     bucket = [1 << max(0, (n - 1).bit_length()) for n in sizes]
-    return f"{gpu}|asm|{len(sizes)}|{bucket[0]}-{bucket[-1]}"
+    return f"{gpu}|asm-sym|{len(sizes)}|{bucket[0]}-{bucket[-1]}"
 
 
 def _load():

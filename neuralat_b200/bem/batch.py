@@ -13,13 +13,18 @@ batch runner changes how the work reaches the GPU:
   without launch-per-problem overhead) plus one launch per touching-pair
   type (``bem_batch_matrices_vk``);
 * the solves of a wave run concurrently, one CUDA stream per worker thread,
-  each Arnoldi step replayed from a captured CUDA graph;
+  each Arnoldi step replayed from a captured CUDA graph; the concurrency
+  follows the problem size (a 10k-unknown solve already keeps every SM busy,
+  so problems of 4096 unknowns or more run two at a time, smaller ones on
+  every worker);
 * launch shapes come from the autotuner (``neuralat_b200.bem.autotune``).
 """
 from __future__ import annotations
 
 import concurrent.futures as cf
 import ctypes
+import threading
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -35,6 +40,7 @@ class BatchResult:
     pressure: list = field(default_factory=list)   # per problem: (P, m) complex64
     info: list = field(default_factory=list)       # per problem: solver info dict
     index: list = field(default_factory=list)      # per problem: (mesh index, k index)
+    waves: list = field(default_factory=list)      # per wave: size, problems, concurrency, seconds
 
 
 def assemble_batch(solvers, ks, mass_coeff=0.5, k_coeff=-1.0, stream=None):
@@ -78,17 +84,43 @@ class BatchRunner:
         self.budget = memory_budget_bytes
         self.workers = max(1, workers)
         self.precision, self.rtol, self.restart = precision, rtol, restart
-        self._streams = [torch.cuda.Stream() for _ in range(self.workers)]
+        self._local = threading.local()
+        # persistent workers: each keeps its stream and the solver's per-thread
+        # host buffers for the runner's lifetime
+        self._pool = cf.ThreadPoolExecutor(max_workers=self.workers)
 
-    def _solve_one(self, widx, A, rhs, solver, k, g, pts, want_u):
-        st = self._streams[widx % self.workers]
-        st.wait_stream(torch.cuda.current_stream())
+    def close(self) -> None:
+        self._pool.shutdown(wait=True)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def concurrency(self, nv: int) -> int:
+        """Concurrent solves for problems of nv unknowns."""
+        return min(2, self.workers) if nv >= 4096 else self.workers
+
+    def _stream(self):
+        st = getattr(self._local, "stream", None)
+        if st is None:
+            st = self._local.stream = torch.cuda.Stream()
+        return st
+
+    def _solve_lane(self, tasks, pts, want_u, ready):
+        """Solve tasks [(A, rhs, solver, k, g)] one after another on this worker's stream."""
+        st = self._stream()
+        st.wait_event(ready)
+        out = []
         with torch.cuda.stream(st):
-            info = {}
-            u = gmres(A, rhs, rtol=self.rtol, restart=self.restart, precision=self.precision, info=info)
-            p = solver.boundary2potential(k, g, u, pts)
+            for A, rhs, solver, k, g in tasks:
+                info = {}
+                u = gmres(A, rhs, rtol=self.rtol, restart=self.restart, precision=self.precision, info=info)
+                p = solver.boundary2potential(k, g, u, pts)
+                out.append(((u if want_u else None), p, info))
             st.synchronize()
-        return (u if want_u else None), p, info
+        return out
 
     def run(self, meshes, ks_per_mesh, neumann_per_mesh, points, return_dirichlet=False) -> BatchResult:
         """meshes: list of (vertices, triangles) numpy arrays; ks_per_mesh: list
@@ -101,36 +133,46 @@ class BatchRunner:
         # largest first: big problems start early and small ones fill the tail
         jobs.sort(key=lambda j: -solvers[j[0]].geometry.nv)
         res = BatchResult()
-        wave, used = [], 0
+        # waves: one size class (same concurrency) and within the memory budget
+        wave, used, conc = [], 0, None
         waves = []
         for j in jobs:
-            b = problem_bytes(solvers[j[0]].geometry.nv, gs[j[0]].shape[1], self.restart)
-            if wave and used + b > self.budget:
-                waves.append(wave)
+            nv = solvers[j[0]].geometry.nv
+            b = problem_bytes(nv, gs[j[0]].shape[1], self.restart)
+            c = self.concurrency(nv)
+            if wave and (used + b > self.budget or c != conc):
+                waves.append((wave, conc))
                 wave, used = [], 0
             wave.append(j)
             used += b
+            conc = c
         if wave:
-            waves.append(wave)
-        pool = cf.ThreadPoolExecutor(max_workers=self.workers)
-        try:
-            for wave in waves:
-                ss = [solvers[mi] for mi, _ in wave]
-                ks = [float(ks_per_mesh[mi][ki]) for mi, ki in wave]
-                mats = assemble_batch(ss, ks)
-                rhss = []
-                for (mi, _), (V, A) in zip(wave, mats):
-                    rhss.append(-cmatmul(V, gs[mi]))
-                mats = [A for _, A in mats]  # V is no longer needed
-                futs = [pool.submit(self._solve_one, w, A, rhs, solvers[mi], k, gs[mi], pts, return_dirichlet)
-                        for w, ((mi, ki), A, rhs, k) in enumerate(zip(wave, mats, rhss, ks))]
-                for (mi, ki), f in zip(wave, futs):
-                    u, p, info = f.result()
-                    res.dirichlet.append(u)
-                    res.pressure.append(p)
-                    res.info.append(info)
-                    res.index.append((mi, ki))
-                del mats, rhss
-        finally:
-            pool.shutdown(wait=True)
+            waves.append((wave, conc))
+        for wave, conc in waves:
+            t0 = time.perf_counter()
+            ss = [solvers[mi] for mi, _ in wave]
+            ks = [float(ks_per_mesh[mi][ki]) for mi, ki in wave]
+            mats = assemble_batch(ss, ks)
+            rhss = []
+            for (mi, _), (V, A) in zip(wave, mats):
+                rhss.append(-cmatmul(V, gs[mi]))
+            mats = [A for _, A in mats]  # V is no longer needed
+            ready = torch.cuda.Event()
+            ready.record()
+            tasks = [(A, rhs, solvers[mi], k, gs[mi]) for (mi, _), A, rhs, k in zip(wave, mats, rhss, ks)]
+            lanes = [list(range(w, len(wave), conc)) for w in range(conc)]  # round-robin over workers
+            futs = [self._pool.submit(self._solve_lane, [tasks[i] for i in lane], pts, return_dirichlet, ready)
+                    for lane in lanes if lane]
+            out = [None] * len(wave)
+            for lane, f in zip([ln for ln in lanes if ln], futs):
+                for i, r in zip(lane, f.result()):
+                    out[i] = r
+            for (mi, ki), (u, p, info) in zip(wave, out):
+                res.dirichlet.append(u)
+                res.pressure.append(p)
+                res.info.append(info)
+                res.index.append((mi, ki))
+            res.waves.append({"vertices": int(ss[0].geometry.nv), "problems": len(wave), "concurrency": conc,
+                              "seconds": time.perf_counter() - t0})
+            del mats, rhss, tasks
         return res

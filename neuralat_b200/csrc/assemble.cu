@@ -781,14 +781,16 @@ __global__ void __launch_bounds__(128)
 
 // ---------------------------------------------------------------------------
 // Batched assembly: many problems (meshes of uneven size, wavenumbers) in one
-// persistent launch.  Regular work items of all problems form one queue that
-// CTAs drain with an atomic counter (dynamic load balance); touching pairs of
-// all problems are concatenated per type.
+// persistent launch.  Regular work items of all problems (runs of used
+// (test group, trial tile) units, each unordered pair once) form one queue
+// that CTAs drain with an atomic counter (dynamic load balance); touching
+// pairs of all problems are concatenated per type.
 // ---------------------------------------------------------------------------
 struct BatchProblem {
   GeomView g;
   float k;
-  int chunk, n_chunks;
+  int chunk, n_chunks;      // units per item, items
+  long long n_units;        // used (test group, trial tile) units
   float2* V;
   float2* K;
   long long item_begin;   // prefix sum of regular items
@@ -813,25 +815,42 @@ __device__ __forceinline__ int find_problem(const BatchProblem* probs, int np, l
   return lo;
 }
 
-__global__ void __launch_bounds__(kRegThreads, 2)
-    regular_vk_batch_kernel(BatchHeader* __restrict__ hdr, const BatchProblem* __restrict__ probs, float v_scale,
-                            float k_scale) {
+// Each unordered regular pair of every problem once (the symmetric item of
+// regular_sym_kernel); items are runs of `chunk` units of one problem.
+__global__ void __launch_bounds__(kSymThreads, 1)
+    regular_sym_batch_kernel(BatchHeader* __restrict__ hdr, const BatchProblem* __restrict__ probs, float v_scale,
+                             float k_scale) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  RegSmem<true, true>& sm = *reinterpret_cast<RegSmem<true, true>*>(smem_raw);
+  SymSmem& sm = *reinterpret_cast<SymSmem*>(smem_raw);
   __shared__ long long s_item;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.tile_full[0], 1);
+    mbar_init(&sm.tile_full[1], 1);
+    mbar_init_fence();
+  }
   const int np = hdr->nproblems;
   const long long total = hdr->total_items;
+  unsigned uses = 0;
   for (;;) {
     __syncthreads();  // everyone has read s_item of the previous round
     if (threadIdx.x == 0) s_item = (long long)atomicAdd(&hdr->next_item, 1ull);
     __syncthreads();
     const long long item = s_item;
     if (item >= total) break;
-    const int pi = find_problem(probs, np, item, -1);
-    const BatchProblem& P = probs[pi];
-    const int local = (int)(item - P.item_begin);
-    const int grp = local / P.n_chunks;
-    regular_item<true, true>(sm, P.g, P.k, P.V, P.K, v_scale, k_scale, grp, local - grp * P.n_chunks, P.chunk);
+    const BatchProblem& P = probs[find_problem(probs, np, item, -1)];
+    const GeomView& g = P.g;
+    const int ngroups = (g.nt + kTestTris - 1) / kTestTris;
+    long long pos = (item - P.item_begin) * P.chunk;
+    const long long end = pos + P.chunk < P.n_units ? pos + P.chunk : P.n_units;
+    while (pos < end) {  // uniform over the block
+      const int grp = sym_group_of(pos, g.ntiles, ngroups);
+      const long long base = sym_units_before(grp, g.ntiles);
+      const long long gend = base + (g.ntiles - 2 * grp);
+      const long long stop = end < gend ? end : gend;
+      const int jt0 = 2 * grp + (int)(pos - base);
+      regular_sym_item(sm, g, P.k, P.V, P.K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos), uses);
+      pos = stop;
+    }
   }
 }
 
@@ -1053,10 +1072,10 @@ int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs,
                       float mass_coeff, float k_coeff, void* ws, size_t ws_bytes, cudaStream_t s) {
   if (np <= 0) return BEM_ERR_INVALID_ARGUMENT;
   if (!ws || ws_bytes < batch_workspace_bytes(np)) return BEM_ERR_WORKSPACE;
-  const int smem = (int)sizeof(RegSmem<true, true>);
+  const int smem = (int)sizeof(SymSmem);
   static std::atomic<bool> attr{false};
   if (!attr.load(std::memory_order_acquire)) {
-    BEM_CUDA_TRY(cudaFuncSetAttribute(regular_vk_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    BEM_CUDA_TRY(cudaFuncSetAttribute(regular_sym_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr.store(true, std::memory_order_release);
   }
   // host descriptors
@@ -1083,13 +1102,15 @@ int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs,
     BatchProblem& P = hp[p];
     P.g = g;
     P.k = ks[p];
-    int chunk = g_tune_chunk > 0 ? g_tune_chunk : (g.ntiles / 4 < 1 ? 1 : (g.ntiles / 4 > 32 ? 32 : g.ntiles / 4));
+    const long long ngroups = (g.nt + kTestTris - 1) / kTestTris;
+    P.n_units = ngroups * g.ntiles - ngroups * (ngroups - 1);
+    int chunk = g_tune_chunk > 0 ? g_tune_chunk : (g.ntiles / 8 < 1 ? 1 : (g.ntiles / 8 > 64 ? 64 : g.ntiles / 8));
     P.chunk = chunk;
-    P.n_chunks = (g.ntiles + chunk - 1) / chunk;
+    P.n_chunks = (int)((P.n_units + chunk - 1) / chunk);
     P.V = Vs[p];
     P.K = Ks[p];
     P.item_begin = items;
-    items += (long long)((g.nt + kTestTris - 1) / kTestTris) * P.n_chunks;
+    items += P.n_chunks;
     P.pair_begin[0] = pairs[0];
     P.pair_begin[1] = pairs[1];
     P.pair_begin[2] = pairs[2];
@@ -1105,12 +1126,12 @@ int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs,
   BEM_CUDA_TRY(cudaEventRecord(t_stage.ev, s));
   const float v_scale = kInv4Pi, k_scale = -kInv4Pi * k_coeff;
   int occ = 0;
-  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_vk_batch_kernel, kRegThreads, smem));
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_sym_batch_kernel, kSymThreads, smem));
   if (g_tune_ctas_per_sm > 0 && g_tune_ctas_per_sm < occ) occ = g_tune_ctas_per_sm;
   const long long grid = (long long)sm_count() * (occ > 0 ? occ : 1);
   if (items > 0)
-    (regular_vk_batch_kernel<<<(unsigned)(grid < items ? grid : items), kRegThreads, smem, s>>>(dh, dp, v_scale,
-                                                                                                k_scale),
+    (regular_sym_batch_kernel<<<(unsigned)(grid < items ? grid : items), kSymThreads, smem, s>>>(dh, dp, v_scale,
+                                                                                                 k_scale),
      count_launch());
   const int wpb = 4;
   if (pairs[0])

@@ -85,9 +85,11 @@ def test_batch_runner_matches_per_problem(solvers):
     gs = [M.smoothed_gaussian_field(v.shape[0], t, 3, seed=i) for i, (v, t) in enumerate(ms)]
     pts = M.sphere_points(64, 1.0, seed=3)
     # a tiny budget forces several waves
-    runner = BatchRunner(memory_budget_bytes=3 * 8 * 642 * 642 * 2, workers=3, precision="fp32", rtol=1e-7)
-    res = runner.run(ms, ks, gs, pts, return_dirichlet=True)
+    with BatchRunner(memory_budget_bytes=3 * 8 * 642 * 642 * 2, workers=3, precision="fp32", rtol=1e-7) as runner:
+        res = runner.run(ms, ks, gs, pts, return_dirichlet=True)
+        assert all(w["concurrency"] == runner.concurrency(w["vertices"]) for w in res.waves)
     assert sorted(res.index) == sorted((mi, ki) for mi in range(3) for ki in range(len(ks[mi])))
+    assert sum(w["problems"] for w in res.waves) == len(res.index)
     ptt = torch.as_tensor(pts, dtype=torch.float32, device="cuda")
     for (mi, ki), p, u, info in zip(res.index, res.pressure, res.dirichlet, res.info):
         s = BEM_Solver(*ms[mi])
