@@ -40,6 +40,7 @@ EXPORTED = (
     "bem_boundary2potential_noalloc_max", "bem_boundary2potential_noalloc",
     "bem_cmatmul_adjoint", "bem_conj_transpose", "bem_boundary2potential_adjoint", "bem_vertex_gradient",
     "bem_batch_workspace_bytes", "bem_batch_matrices_vk", "bem_set_tuning", "bem_assembly_status", "bem_get_tuning",
+    "bem_boundary_matrices_bm", "bem_batch_matrices_bm",
 )
 
 
@@ -56,6 +57,11 @@ TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE, TUNE_GMRES_REOR
 class BatchProblem(ctypes.Structure):
     _fields_ = [("geom", ctypes.c_void_p), ("k", ctypes.c_float), ("v_out", ctypes.c_void_p),
                 ("k_out", ctypes.c_void_p)]
+
+
+class BmProblem(ctypes.Structure):
+    _fields_ = [("geom", ctypes.c_void_p), ("k", ctypes.c_float), ("lhs_out", ctypes.c_void_p),
+                ("rhs_out", ctypes.c_void_p)]
 
 
 class SolverParams(ctypes.Structure):
@@ -132,6 +138,8 @@ def lib():
         "bem_set_tuning": ([i, i], i),
         "bem_assembly_status": ([vp], i),
         "bem_get_tuning": ([i], i),
+        "bem_boundary_matrices_bm": ([vp, f, vp, vp, vp], i),
+        "bem_batch_matrices_bm": ([P(BmProblem), i, vp, sz, vp], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)

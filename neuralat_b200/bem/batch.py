@@ -67,23 +67,57 @@ def assemble_batch(solvers, ks, mass_coeff=0.5, k_coeff=-1.0, stream=None):
     return outs
 
 
+def assemble_batch_bm(solvers, ks, stream=None):
+    """Fused Burton-Miller (lhs, rhs) matrices of ``neumann2dirichlet`` for
+    each (solver, k) in one launch family."""
+    assert len(solvers) == len(ks) and len(ks) > 0
+    lib = L.lib()
+    dev = solvers[0].device
+    n = len(ks)
+    probs = (L.BmProblem * n)()
+    outs = []
+    for i, (s, k) in enumerate(zip(solvers, ks)):
+        lhs, rhs = s._new_matrix(), s._new_matrix()
+        outs.append((lhs, rhs))
+        probs[i].geom = s.geometry.ptr.value
+        probs[i].k = float(k)
+        probs[i].lhs_out = lhs.data_ptr()
+        probs[i].rhs_out = rhs.data_ptr()
+    nbytes = int(lib.bem_batch_workspace_bytes(n))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else _stream(dev)
+        L.check(lib.bem_batch_matrices_bm(probs, n, _vp(ws), nbytes, st), "bem_batch_matrices_bm")
+    return outs
+
+
 def problem_bytes(nv: int, m: int, restart: int = 200) -> int:
     """Device bytes one problem holds while it is solved (V, LHS, tensor-core
     planes, Krylov basis and vectors)."""
     return 3 * 8 * nv * nv + 8 * m * (restart + 1) * nv + 64 * m * nv
 
 
+FORMULATIONS = ("cbie", "burton_miller")
+
+
 class BatchRunner:
-    """Run a list of meshes x wavenumbers x RHS through the GPU in waves."""
+    """Run a list of meshes x wavenumbers x RHS through the GPU in waves.
+
+    formulation "cbie": (1/2 I - K) u = -V g (``BEM_Solver.CBIE``);
+    "burton_miller": the <2,3> Burton-Miller system of
+    ``BEM_Solver.neumann2dirichlet`` (free of interior resonances)."""
 
     def __init__(self, memory_budget_bytes: int | None = None, workers: int = 4, precision: str = "fp16x3",
-                 rtol: float = 1e-6, restart: int = 200):
+                 rtol: float = 1e-6, restart: int = 200, formulation: str = "cbie", max_iters: int = 1000):
+        if formulation not in FORMULATIONS:
+            raise ValueError(f"formulation must be one of {FORMULATIONS}")
         if memory_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget_bytes = int(0.6 * free)
         self.budget = memory_budget_bytes
         self.workers = max(1, workers)
         self.precision, self.rtol, self.restart = precision, rtol, restart
+        self.formulation, self.max_iters = formulation, max_iters
         self._local = threading.local()
         # persistent workers: each keeps its stream and the solver's per-thread
         # host buffers for the runner's lifetime
@@ -116,19 +150,42 @@ class BatchRunner:
         with torch.cuda.stream(st):
             for A, rhs, solver, k, g in tasks:
                 info = {}
-                u = gmres(A, rhs, rtol=self.rtol, restart=self.restart, precision=self.precision, info=info)
+                u = gmres(A, rhs, rtol=self.rtol, restart=self.restart, max_iters=self.max_iters,
+                          precision=self.precision, info=info)
                 p = solver.boundary2potential(k, g, u, pts)
                 out.append(((u if want_u else None), p, info))
             st.synchronize()
         return out
 
     def run(self, meshes, ks_per_mesh, neumann_per_mesh, points, return_dirichlet=False) -> BatchResult:
-        """meshes: list of (vertices, triangles) numpy arrays; ks_per_mesh: list
-        of wavenumber lists; neumann_per_mesh: list of (N, m) arrays; points (P, 3)."""
+        """meshes: list of (vertices, triangles) numpy arrays or ``BEM_Solver``s;
+        ks_per_mesh: list of wavenumber lists; neumann_per_mesh: per mesh an
+        (N,) or (N, m) array shared by its wavenumbers, or a list with one
+        such array per wavenumber (a vibration mode per wavenumber); points
+        (P, 3).  Results are (N, m) / (P, m) per problem, m = 1 for (N,)."""
         dev = torch.device("cuda", torch.cuda.current_device())
-        pts = torch.as_tensor(np.asarray(points, np.float32), device=dev).contiguous()
-        solvers = [BEM_Solver(np.asarray(v, np.float32), np.asarray(t, np.int32)) for v, t in meshes]
-        gs = [torch.as_tensor(np.asarray(g, np.complex64), device=dev).contiguous() for g in neumann_per_mesh]
+        pts = (points.to(device=dev, dtype=torch.float32) if torch.is_tensor(points)
+               else torch.as_tensor(np.asarray(points, np.float32), device=dev)).contiguous()
+        solvers = [m if isinstance(m, BEM_Solver) else BEM_Solver(np.asarray(m[0], np.float32),
+                                                                   np.asarray(m[1], np.int32)) for m in meshes]
+
+        def dev_c64(g):
+            g = g if torch.is_tensor(g) else torch.from_numpy(np.asarray(g, np.complex64))
+            g = g.to(device=dev, dtype=torch.complex64)
+            return (g.reshape(-1, 1) if g.dim() == 1 else g).contiguous()
+
+        gs = []
+        for mi, g in enumerate(neumann_per_mesh):
+            if isinstance(g, (list, tuple)):
+                if len(g) != len(ks_per_mesh[mi]):
+                    raise ValueError(f"mesh {mi}: {len(g)} Neumann arrays for {len(ks_per_mesh[mi])} wavenumbers")
+                gs.append([dev_c64(x) for x in g])
+            else:
+                gs.append(dev_c64(g))
+
+        def neumann(mi, ki):
+            return gs[mi][ki] if isinstance(gs[mi], list) else gs[mi]
+
         jobs = [(mi, ki) for mi in range(len(meshes)) for ki in range(len(ks_per_mesh[mi]))]
         # largest first: big problems start early and small ones fill the tail
         jobs.sort(key=lambda j: -solvers[j[0]].geometry.nv)
@@ -138,7 +195,7 @@ class BatchRunner:
         waves = []
         for j in jobs:
             nv = solvers[j[0]].geometry.nv
-            b = problem_bytes(nv, gs[j[0]].shape[1], self.restart)
+            b = problem_bytes(nv, neumann(*j).shape[1], self.restart)
             c = self.concurrency(nv)
             if wave and (used + b > self.budget or c != conc):
                 waves.append((wave, conc))
@@ -152,14 +209,19 @@ class BatchRunner:
             t0 = time.perf_counter()
             ss = [solvers[mi] for mi, _ in wave]
             ks = [float(ks_per_mesh[mi][ki]) for mi, ki in wave]
-            mats = assemble_batch(ss, ks)
-            rhss = []
-            for (mi, _), (V, A) in zip(wave, mats):
-                rhss.append(-cmatmul(V, gs[mi]))
-            mats = [A for _, A in mats]  # V is no longer needed
+            # keep only the left-hand sides once the right-hand sides are formed
+            if self.formulation == "cbie":
+                pairs = assemble_batch(ss, ks)  # (V, 1/2 I - K)
+                rhss = [-cmatmul(V, neumann(*j)) for j, (V, _) in zip(wave, pairs)]
+                mats = [A for _, A in pairs]
+            else:
+                pairs = assemble_batch_bm(ss, ks)  # (lhs, rhs operator)
+                rhss = [cmatmul(R, neumann(*j)) for j, (_, R) in zip(wave, pairs)]
+                mats = [A for A, _ in pairs]
+            del pairs
             ready = torch.cuda.Event()
             ready.record()
-            tasks = [(A, rhs, solvers[mi], k, gs[mi]) for (mi, _), A, rhs, k in zip(wave, mats, rhss, ks)]
+            tasks = [(A, rhs, solvers[mi], k, neumann(mi, ki)) for (mi, ki), A, rhs, k in zip(wave, mats, rhss, ks)]
             lanes = [list(range(w, len(wave), conc)) for w in range(conc)]  # round-robin over workers
             futs = [self._pool.submit(self._solve_lane, [tasks[i] for i in lane], pts, return_dirichlet, ready)
                     for lane in lanes if lane]

@@ -209,6 +209,15 @@ class BEM_Solver:
                                                      _stream(self.device)), "bem_boundary_matrices_vk")
         return V, A
 
+    def assemble_bm(self, wavenumber):
+        """Fused Burton-Miller matrices of ``neumann2dirichlet`` at the <2,3>
+        rules: (bm_lhs + 1/2 I, bm_rhs - (i/(2k)) I), one pass."""
+        lhs, rhs = self._new_matrix(), self._new_matrix()
+        with torch.cuda.device(self.device):
+            L.check(L.lib().bem_boundary_matrices_bm(self.geometry.ptr, float(wavenumber), _vp(lhs), _vp(rhs),
+                                                     _stream(self.device)), "bem_boundary_matrices_bm")
+        return lhs, rhs
+
     def identity_matrix(self):
         out = self._new_matrix()
         with torch.cuda.device(self.device):
@@ -240,12 +249,13 @@ class BEM_Solver:
         return solve_linear_equation(lhs, rhs, **kw)
 
     def neumann2dirichlet(self, k, neumann, **kw):
-        """Burton-Miller with the <2,3> rules (solver.py:118-126)."""
-        identity = self.identity_matrix()
-        beta = 1j / k
-        lhs = (self.assemble_boundary_matrix(k, "bm_lhs", approx=True) + 0.5 * identity).contiguous()
-        rhs_m = (self.assemble_boundary_matrix(k, "bm_rhs", approx=True) - beta * 0.5 * identity).contiguous()
-        return solve_linear_equation(lhs, cmatmul(rhs_m, neumann.to(torch.complex64)), **kw)
+        """Burton-Miller with the <2,3> rules (solver.py:118-126): the fused
+        assembly of (bm_lhs + 1/2 I, bm_rhs - (i/(2k)) I), then
+        ``solve_linear_equation`` (same options)."""
+        lhs, rhs_m = self.assemble_bm(k)
+        rhs = cmatmul(rhs_m, neumann.to(torch.complex64))
+        del rhs_m
+        return solve_linear_equation(lhs, rhs, **kw)
 
     # ---- listeners ----------------------------------------------------------
     def potential_matrix(self, k, points, layer_type="single"):

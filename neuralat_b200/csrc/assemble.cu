@@ -481,19 +481,6 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
 // S(g) = g (ntiles - g + 1).  Items are equal runs of `chunk` consecutive
 // units (a run crossing a group boundary is split), dealt round-robin to a
 // persistent grid: every CTA gets the same amount of work.
-__device__ __forceinline__ long long sym_units_before(long long g, long long ntiles) { return g * (ntiles - g + 1); }
-
-__device__ __forceinline__ int sym_group_of(long long pos, int ntiles, int ngroups) {
-  const double b = (double)ntiles + 1.0;
-  const double disc = b * b - 4.0 * (double)pos;
-  long long g = (long long)((b - sqrt(disc > 0.0 ? disc : 0.0)) * 0.5);
-  if (g < 0) g = 0;
-  if (g > ngroups - 1) g = ngroups - 1;
-  while (g + 1 < ngroups && sym_units_before(g + 1, ntiles) <= pos) g++;
-  while (g > 0 && sym_units_before(g, ntiles) > pos) g--;
-  return (int)g;
-}
-
 __global__ void __launch_bounds__(kSymThreads, 1)
     regular_sym_kernel(GeomView g, float k, float2* __restrict__ V, float2* __restrict__ K, float v_scale,
                        float k_scale, long long chunk, long long n_units, int n_items) {

@@ -51,6 +51,17 @@ struct __align__(16) TriRec {
 };
 static_assert(sizeof(TriRec) == 128, "TriRec must be 128 bytes");
 
+// Burton-Miller companion record, sorted order: the points of the 3-point
+// degree-2 triangle rule (phi = 2/3 at the point's own vertex, 1/6 at the
+// others; weights 1/3) used by the <2,3> Burton-Miller bindings, and the
+// surface curls n x grad(phi_b) of the three P1 functions (rows b).
+struct __align__(16) BmRec {
+  float qp[9];
+  float curl[9];
+  float pad[2];
+};
+static_assert(sizeof(BmRec) == 80, "BmRec must be 80 bytes");
+
 constexpr int kTile = 16;               // triangles per geometry tile
 constexpr int kTileCorners = 3 * kTile;  // 48
 
@@ -85,9 +96,10 @@ struct GeomHeader {
   uint64_t off_vert_pairs;  // int2[n_vert]
   uint64_t off_normals;    // float[nt*3]
   uint64_t off_curls;      // float[nt*9]   rows: n x grad(phi_b)
+  uint64_t off_bmrec;      // BmRec[nt] in sorted order
   uint64_t bytes;
 };
-constexpr uint32_t kGeomMagic = 0x42454D32u;  // "BEM2"
+constexpr uint32_t kGeomMagic = 0x42454D33u;  // "BEM3"
 
 // Device-side view of a built geometry.
 struct GeomView {
@@ -102,7 +114,24 @@ struct GeomView {
   const int2* vert_pairs;
   const float* normals;
   const float* curls;
+  const BmRec* bm;         // sorted order
 };
+
+// Symmetric regular-pair work units: test group g (32 triangles = tiles 2g,
+// 2g+1) is paired with the ntiles - 2g trial tiles from its first tile on,
+// so the units before group g number S(g) = g (ntiles - g + 1).
+__device__ __forceinline__ long long sym_units_before(long long g, long long ntiles) { return g * (ntiles - g + 1); }
+
+__device__ __forceinline__ int sym_group_of(long long pos, int ntiles, int ngroups) {
+  const double b = (double)ntiles + 1.0;
+  const double disc = b * b - 4.0 * (double)pos;
+  long long g = (long long)((b - sqrt(disc > 0.0 ? disc : 0.0)) * 0.5);
+  if (g < 0) g = 0;
+  if (g > ngroups - 1) g = ngroups - 1;
+  while (g + 1 < ngroups && sym_units_before(g + 1, ntiles) <= pos) g++;
+  while (g > 0 && sym_units_before(g, ntiles) > pos) g--;
+  return (int)g;
+}
 
 // ---- small math -------------------------------------------------------------
 struct f3 {

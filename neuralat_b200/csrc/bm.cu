@@ -1,0 +1,729 @@
+// Fused Burton-Miller assembly: both matrices of the reference's
+// neumann2dirichlet (src/bem/solver.py:118-126) in one pass,
+//   lhs = BM_LHS + 1/2 M,     rhs = BM_RHS - (i / (2k)) M,
+// at the <2,3> rules of its "_approx" bindings (bind.cu:204-215): the 3-point
+// degree-2 triangle rule for regular pairs, 2-point Gauss-Legendre
+// Sauter-Schwab quadrature for touching pairs.
+//
+// Kernels (potential.h:42-65, integrand.h:94-101,216-221,314-322), x on the
+// test triangle i, y on the trial triangle j, G = e^{ikr}/r and
+// H = (1 - ikr) e^{ikr} / r^3 (the 1/(4 pi) applied last):
+//   BM_LHS(i,j) = -ik (n_i.n_j) G + H (y - x).n_j + (i/k) G (curl_i . curl_j)
+//   BM_RHS(i,j) = -G + (i/k) H (x - y).n_i
+// The curl term uses the P1 surface curls, constant per triangle, so the
+// Galerkin block needs only the weight sum of G over the pair.
+//
+// Regular pairs: G, H (y-x).n_j and H (x-y).n_i are symmetric / swapped under
+// i <-> j, so one evaluation of r and sincos per quadrature-point pair of an
+// UNORDERED pair gives all four blocks lhs_ij, lhs_ji, rhs_ij, rhs_ji:
+//   S = sum C C G,  T = sum C C H (y-x).n_j,  U = sum C C H (x-y).n_i
+//   lhs_ij = -ik nn S + T + (i/k) s cc      lhs_ji^T = -ik nn S + U + (i/k) s cc
+//   rhs_ij = -S + (i/k) U                   rhs_ji^T = -S + (i/k) T
+// with s = sum_ab S_ab (the P1 functions sum to one) and cc_ab the curl
+// products.  The work decomposition is the symmetric V/K assembly's: 32 test
+// triangles per CTA (one per lane), 16-triangle trial tiles double-buffered
+// in shared memory by bulk copies, one trial triangle per warp, corner slabs
+// reduced on chip onto distinct vertices, four vector atomics per entry.
+// Touching pairs: one warp per pair evaluates both kernels at each
+// Sauter-Schwab point (shared r and sincos); the coincident pass (FP64) adds
+// the mass terms.  A batch (meshes, wavenumbers) uses the same kernels with a
+// work queue over all problems.
+
+#include <atomic>
+#include <cmath>
+#include <cstring>
+
+#include "async_copy.cuh"
+#include "bem_common.cuh"
+#include "sauter_schwab.cuh"
+
+namespace bemb {
+
+namespace {
+
+constexpr int kBmThreads = 32 * kTile;       // 512: warp w takes trial triangle w
+constexpr int kBmTest = 32;                  // test triangles per CTA, one per lane
+constexpr int kBmCorners = 3 * kBmTest;      // 96
+constexpr int kBmStride = kTileCorners + 1;  // 49 float2: conflict-free column writes
+
+// 3-point rule: C(q, b) = w_q phi_b(q) = 1/3 * (q == b ? 2/3 : 1/6)
+__host__ __device__ constexpr float bm_c(int q, int b) { return q == b ? 2.0f / 9.0f : 1.0f / 18.0f; }
+
+struct BmSmem {
+  float2 slotL[kBmCorners][kBmStride];   // lhs_ij[a][b] at [3 lane + a][3 tt + b]
+  float2 slotLT[kBmCorners][kBmStride];  // lhs_ji[b][a], same indexing
+  float2 slotR[kBmCorners][kBmStride];
+  float2 slotRT[kBmCorners][kBmStride];
+  float xs[9][kBmTest];                  // test quadrature points [coordinate][lane]
+  float xc[9][kBmTest];                  // test curls [3 a + d][lane]
+  TriRec trial[2][kTile];                // trial tile, double-buffered
+  BmRec trialB[2][kTile];
+  TileRec tileJ[2];
+  TileRec tileI[2];
+  uint64_t tile_full[2];
+};
+
+// A bounded wait of the Burton-Miller kernels expired (read by bm_status).
+__device__ int g_bm_err;
+
+__device__ __forceinline__ void bm_copy_words(void* dst, const void* src, int bytes, int tid) {
+  const int4* s = (const int4*)src;
+  int4* d = (int4*)dst;
+  for (int i = tid; i < bytes / 16; i += kBmThreads) d[i] = s[i];
+}
+
+// Thread 0: bulk-copy trial tile jt (records, Burton-Miller records, vertex
+// table) into buffer b.
+__device__ __forceinline__ void bm_fetch_tile(BmSmem& sm, const GeomView& g, int jt, int b) {
+  const int ntri = min(kTile, g.nt - jt * kTile);
+  const uint32_t rb = (uint32_t)(ntri * sizeof(TriRec)), mb = (uint32_t)(ntri * sizeof(BmRec));
+  mbar_expect_tx(&sm.tile_full[b], rb + mb + (uint32_t)sizeof(TileRec));
+  bulk_load(sm.trial[b], &g.rec[jt * kTile], rb, &sm.tile_full[b]);
+  bulk_load(sm.trialB[b], &g.bm[jt * kTile], mb, &sm.tile_full[b]);
+  bulk_load(&sm.tileJ[b], &g.tiles[jt], (uint32_t)sizeof(TileRec), &sm.tile_full[b]);
+}
+
+// S, T, U blocks of one unordered pair under the 3x3 point rule (lane = test
+// triangle, points in xs; trial points yq, dq[q] = n_i . (c_i - y_q)).
+__device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int lane, const float (&yq)[9],
+                                              const float (&dq)[3], float njx, float njy, float njz, float cjx,
+                                              float cjy, float cjz, float k, float2 (&aS)[9], float2 (&aT)[9],
+                                              float2 (&aU)[9]) {
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    aS[e] = make_float2(0.f, 0.f);
+    aT[e] = make_float2(0.f, 0.f);
+    aU[e] = make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    const float px = xs[3 * p][lane], py = xs[3 * p + 1][lane], pz = xs[3 * p + 2][lane];
+    const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);  // (y - x).n_j on plane j
+    float2 tS[3], tT[3], tU[3];
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      tS[b] = make_float2(0.f, 0.f);
+      tT[b] = make_float2(0.f, 0.f);
+      tU[b] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const float dx = yq[3 * q] - px, dy = yq[3 * q + 1] - py, dz = yq[3 * q + 2] - pz;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float rinv = fminf(rsqrtf(r2), 1.0f / kEps);
+      const float r = fmaxf(r2 * rinv, kEps);
+      float s, c;
+      __sincosf(k * r, &s, &c);
+      const float gr = c * rinv, gi = s * rinv;
+      const float rinv2 = rinv * rinv;
+      const float hr = fmaf(k, s, gr) * rinv2;   // (c + kr s) / r^3
+      const float hi = fmaf(-k, c, gi) * rinv2;  // (s - kr c) / r^3
+      const float ur = dq[q] * hr, ui = dq[q] * hi;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        const float w = bm_c(q, b);
+        tS[b].x = fmaf(w, gr, tS[b].x);
+        tS[b].y = fmaf(w, gi, tS[b].y);
+        tT[b].x = fmaf(w, hr, tT[b].x);
+        tT[b].y = fmaf(w, hi, tT[b].y);
+        tU[b].x = fmaf(w, ur, tU[b].x);
+        tU[b].y = fmaf(w, ui, tU[b].y);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float wa = bm_c(p, a);
+      const float wt = wa * dn;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        aS[3 * a + b].x = fmaf(wa, tS[b].x, aS[3 * a + b].x);
+        aS[3 * a + b].y = fmaf(wa, tS[b].y, aS[3 * a + b].y);
+        aT[3 * a + b].x = fmaf(wt, tT[b].x, aT[3 * a + b].x);
+        aT[3 * a + b].y = fmaf(wt, tT[b].y, aT[3 * a + b].y);
+        aU[3 * a + b].x = fmaf(wa, tU[b].x, aU[3 * a + b].x);
+        aU[3 * a + b].y = fmaf(wa, tU[b].y, aU[3 * a + b].y);
+      }
+    }
+  }
+}
+
+// One work item: test group grp against trial tiles [jt_begin, jt_end).
+// `uses` counts the trial tiles this CTA has processed (buffer = uses & 1,
+// mbarrier parity = (uses >> 1) & 1).
+__device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, float2* __restrict__ L,
+                                        float2* __restrict__ Rm, int grp, int jt_begin, int jt_end,
+                                        unsigned& uses) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nt = g.nt, nv = g.nv;
+  const int tile0 = 2 * grp;
+  const bool has_t1 = tile0 + 1 < g.ntiles;
+  const int ti = grp * kBmTest + lane;
+  const bool valid_i = ti < nt;
+  const TriRec& ri = g.rec[valid_i ? ti : nt - 1];
+  const float area_i = ri.area;
+  const float nix = ri.n[0], niy = ri.n[1], niz = ri.n[2], cix = ri.c[0], ciy = ri.c[1], ciz = ri.c[2];
+  const int iv0 = ri.v[0], iv1 = ri.v[1], iv2 = ri.v[2];
+  const float kinv = 1.0f / k;
+
+  __syncthreads();  // the previous item is done with tileI, xs, xc and both trial buffers
+  if (tid == 0) bm_fetch_tile(sm, g, jt_begin, uses & 1);
+  bm_copy_words(&sm.tileI[0], &g.tiles[tile0], sizeof(TileRec), tid);
+  if (has_t1) bm_copy_words(&sm.tileI[1], &g.tiles[tile0 + 1], sizeof(TileRec), tid);
+  for (int e = tid; e < 18 * kBmTest; e += kBmThreads) {
+    const int c = e / kBmTest, l = e - c * kBmTest;
+    const int t = min(grp * kBmTest + l, nt - 1);
+    if (c < 9)
+      sm.xs[c][l] = g.bm[t].qp[c];
+    else
+      sm.xc[c - 9][l] = g.bm[t].curl[c - 9];
+  }
+
+  for (int jt = jt_begin; jt < jt_end; jt++, uses++) {
+    const int bf = uses & 1;
+    __syncthreads();  // the previous tile's gather is done with the slots and with buffer bf ^ 1
+    if (tid == 0 && jt + 1 < jt_end) bm_fetch_tile(sm, g, jt + 1, bf ^ 1);
+    if (!mbar_wait(&sm.tile_full[bf], (uses >> 1) & 1u, &g_bm_err)) {
+      // expired (flag raised): let the copy land before the buffer is reused
+      mbar_wait_drain(&sm.tile_full[bf], (uses >> 1) & 1u);
+    }
+    const TileRec& tileJ = sm.tileJ[bf];
+    const int ntriJ = min(kTile, nt - jt * kTile);
+
+    // ---- compute: warp w takes trial triangle w ----
+    const int tt = warp;
+    const int tj = jt * kTile + tt;
+    float aa = 0.f;
+    if (tt < ntriJ) {
+      const TriRec& rj = sm.trial[bf][tt];
+      const int j0 = rj.v[0], j1 = rj.v[1], j2 = rj.v[2];
+      const bool touching = (iv0 == j0) | (iv0 == j1) | (iv0 == j2) | (iv1 == j0) | (iv1 == j1) | (iv1 == j2) |
+                            (iv2 == j0) | (iv2 == j1) | (iv2 == j2);
+      const bool once = jt >= tile0 + 2 || tj > ti;  // on the group's own tiles each unordered pair once
+      aa = (valid_i && !touching && once) ? area_i * rj.area : 0.f;
+    }
+    if (tt < ntriJ && __any_sync(0xffffffffu, aa != 0.f)) {
+      const TriRec& rj = sm.trial[bf][tt];
+      const BmRec& bj = sm.trialB[bf][tt];
+      float yq[9];
+#pragma unroll
+      for (int e = 0; e < 9; e++) yq[e] = bj.qp[e];
+      float dq[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+        dq[q] = nix * (cix - yq[3 * q]) + niy * (ciy - yq[3 * q + 1]) + niz * (ciz - yq[3 * q + 2]);
+      float2 aS[9], aT[9], aU[9];
+      bm_pair_block(sm.xs, lane, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aS, aT, aU);
+      const float sc = aa * kInv4Pi;
+      float2 s9 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int e = 0; e < 9; e++) {
+        s9.x += aS[e].x;
+        s9.y += aS[e].y;
+      }
+      s9.x *= sc * kinv;  // (i/k) s = (-s.y / k, s.x / k), scaled
+      s9.y *= sc * kinv;
+      const float knn = k * (nix * rj.n[0] + niy * rj.n[1] + niz * rj.n[2]);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          const float cc = sm.xc[3 * a][lane] * bj.curl[3 * b] + sm.xc[3 * a + 1][lane] * bj.curl[3 * b + 1] +
+                           sm.xc[3 * a + 2][lane] * bj.curl[3 * b + 2];
+          const float Sx = aS[3 * a + b].x * sc, Sy = aS[3 * a + b].y * sc;
+          const float Tx = aT[3 * a + b].x * sc, Ty = aT[3 * a + b].y * sc;
+          const float Ux = aU[3 * a + b].x * sc, Uy = aU[3 * a + b].y * sc;
+          const float lx = fmaf(knn, Sy, -s9.y * cc), ly = fmaf(-knn, Sx, s9.x * cc);
+          sm.slotL[3 * lane + a][3 * tt + b] = make_float2(lx + Tx, ly + Ty);
+          sm.slotLT[3 * lane + a][3 * tt + b] = make_float2(lx + Ux, ly + Uy);
+          sm.slotR[3 * lane + a][3 * tt + b] = make_float2(fmaf(-Uy, kinv, -Sx), fmaf(Ux, kinv, -Sy));
+          sm.slotRT[3 * lane + a][3 * tt + b] = make_float2(fmaf(-Ty, kinv, -Sx), fmaf(Tx, kinv, -Sy));
+        }
+    } else if (tt < ntriJ) {
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          sm.slotL[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotLT[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotR[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotRT[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+
+    // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
+    const int nI0 = sm.tileI[0].nlv;
+    const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
+    const int nJ = tileJ.nlv;
+    const int total = (nI0 + nI1) * nJ;
+    for (int e = tid; e < total; e += kBmThreads) {
+      const int ai = e / nJ;
+      const int b = e - ai * nJ;
+      const int s = ai >= nI0;
+      const int a = ai - s * nI0;
+      const TileRec& TI = sm.tileI[s];
+      float2 l = make_float2(0.f, 0.f), lt = l, rr = l, rt = l;
+      const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+      const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
+      for (int ca = ca0; ca < ca1; ca++) {
+        const int row = s * kTileCorners + TI.lv_corner[ca];
+        for (int cb = cb0; cb < cb1; cb++) {
+          const int col = tileJ.lv_corner[cb];
+          l.x += sm.slotL[row][col].x;
+          l.y += sm.slotL[row][col].y;
+          lt.x += sm.slotLT[row][col].x;
+          lt.y += sm.slotLT[row][col].y;
+          rr.x += sm.slotR[row][col].x;
+          rr.y += sm.slotR[row][col].y;
+          rt.x += sm.slotRT[row][col].x;
+          rt.y += sm.slotRT[row][col].y;
+        }
+      }
+      const int A = TI.vid[a], B = tileJ.vid[b];
+      if (l.x != 0.f || l.y != 0.f || lt.x != 0.f || lt.y != 0.f || rr.x != 0.f || rr.y != 0.f || rt.x != 0.f ||
+          rt.y != 0.f) {
+        atomicAdd(&L[(size_t)A * nv + B], l);
+        atomicAdd(&L[(size_t)B * nv + A], lt);
+        atomicAdd(&Rm[(size_t)A * nv + B], rr);
+        atomicAdd(&Rm[(size_t)B * nv + A], rt);
+      }
+    }
+  }
+}
+
+// Splits units [pos, end) of one problem at test-group boundaries.
+__device__ __forceinline__ void bm_units(BmSmem& sm, const GeomView& g, float k, float2* L, float2* Rm,
+                                         long long pos, long long end, unsigned& uses) {
+  const int ngroups = (g.nt + kBmTest - 1) / kBmTest;
+  while (pos < end) {  // uniform over the block
+    const int grp = sym_group_of(pos, g.ntiles, ngroups);
+    const long long base = sym_units_before(grp, g.ntiles);
+    const long long gend = base + (g.ntiles - 2 * grp);
+    const long long stop = end < gend ? end : gend;
+    const int jt0 = 2 * grp + (int)(pos - base);
+    bm_item(sm, g, k, L, Rm, grp, jt0, jt0 + (int)(stop - pos), uses);
+    pos = stop;
+  }
+}
+
+// ---- problem descriptors (one problem, or a batch) ----
+struct BmProblem {
+  GeomView g;
+  float k;
+  int chunk;                // units per work item
+  long long n_units;        // used (test group, trial tile) units
+  long long item_begin;     // prefix sum of work items
+  long long pair_begin[3];  // prefix sums of coincident / edge / vertex pairs
+  float2* L;
+  float2* R;
+};
+
+struct BmHeader {
+  unsigned long long next_item;  // queue head (zeroed before each launch)
+  int nproblems;
+  int pad;
+  long long total_items;
+  long long total_pairs[3];
+};
+
+__device__ __forceinline__ int bm_find(const BmProblem* probs, int np, long long x, int which) {
+  int lo = 0, hi = np - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long b = which < 0 ? probs[mid].item_begin : probs[mid].pair_begin[which];
+    if (b <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void bm_init_barriers(BmSmem& sm) {
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.tile_full[0], 1);
+    mbar_init(&sm.tile_full[1], 1);
+    mbar_init_fence();
+  }
+}
+
+// Regular pairs of one problem: equal work items dealt round-robin to a
+// persistent grid.
+__global__ void __launch_bounds__(kBmThreads, 1)
+    regular_bm_kernel(const __grid_constant__ BmProblem P, int n_items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BmSmem& sm = *reinterpret_cast<BmSmem*>(smem_raw);
+  bm_init_barriers(sm);
+  unsigned uses = 0;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const long long pos = (long long)item * P.chunk;
+    const long long end = pos + P.chunk < P.n_units ? pos + P.chunk : P.n_units;
+    bm_units(sm, P.g, P.k, P.L, P.R, pos, end, uses);
+  }
+}
+
+// Regular pairs of a batch: CTAs drain one queue of work items.
+__global__ void __launch_bounds__(kBmThreads, 1)
+    regular_bm_batch_kernel(BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BmSmem& sm = *reinterpret_cast<BmSmem*>(smem_raw);
+  __shared__ long long s_item;
+  bm_init_barriers(sm);
+  const int np = hdr->nproblems;
+  const long long total = hdr->total_items;
+  unsigned uses = 0;
+  for (;;) {
+    __syncthreads();  // everyone has read s_item of the previous round
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(&hdr->next_item, 1ull);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= total) break;
+    const BmProblem& P = probs[bm_find(probs, np, item, -1)];
+    const long long pos = (item - P.item_begin) * P.chunk;
+    const long long end = pos + P.chunk < P.n_units ? pos + P.chunk : P.n_units;
+    bm_units(sm, P.g, P.k, P.L, P.R, pos, end, uses);
+  }
+}
+
+__device__ __forceinline__ void bm_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+__device__ __forceinline__ void bm_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+
+// Both Burton-Miller kernels at d = y - x, without the 1/(4 pi):
+// lhs_main = -ik nn G + H d.n_j, aux = (i/k) G, rhs = -G + (i/k) H (-d).n_i.
+template <typename R>
+__device__ __forceinline__ void bm_eval(R dx, R dy, R dz, const R (&ni)[3], const R (&nj)[3], R nn, R k, R kinv,
+                                        R& lr, R& li, R& ar, R& ai, R& rr, R& ri) {
+  R r = sqrt(dx * dx + dy * dy + dz * dz);
+  if (r < R(kEps)) r = R(kEps);
+  R s, c;
+  bm_sincos(k * r, &s, &c);
+  const R ir = R(1) / r;
+  const R kr = k * r;
+  const R gr = c * ir, gi = s * ir;
+  const R ir2 = ir * ir;
+  const R hr = (c + kr * s) * ir * ir2, hi = (s - kr * c) * ir * ir2;
+  const R dnj = dx * nj[0] + dy * nj[1] + dz * nj[2];     // (y - x).n_j
+  const R dni = -(dx * ni[0] + dy * ni[1] + dz * ni[2]);  // (x - y).n_i
+  lr = k * nn * gi + hr * dnj;
+  li = -k * nn * gr + hi * dnj;
+  ar = -gi * kinv;
+  ai = gr * kinv;
+  rr = -gr - hi * dni * kinv;
+  ri = -gi + hr * dni * kinv;
+}
+
+// One touching pair (index `local` of its type), one warp; the coincident
+// pass also adds 1/2 M to lhs and -(i/(2k)) M to rhs.
+template <typename R, int NCOMMON>
+__device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local) {
+  constexpr int LN = 2;
+  const int lane = threadIdx.x & 31;
+  const GeomView& g = P.g;
+  int ti = local, tj = local;
+  if (NCOMMON == 2) {
+    ti = g.edge_pairs[local].x;
+    tj = g.edge_pairs[local].y;
+  } else if (NCOMMON == 1) {
+    ti = g.vert_pairs[local].x;
+    tj = g.vert_pairs[local].y;
+  }
+  const int s0 = g.triangles[3 * ti], s1 = g.triangles[3 * ti + 1], s2 = g.triangles[3 * ti + 2];
+  const int t0 = g.triangles[3 * tj], t1 = g.triangles[3 * tj + 1], t2 = g.triangles[3 * tj + 2];
+  const Perm6 pm = reorder6<NCOMMON>(s0, s1, s2, t0, t1, t2);
+  const int pi_[3] = {pm.i0, pm.i1, pm.i2}, pj_[3] = {pm.j0, pm.j1, pm.j2};
+  const int sv[3] = {s0, s1, s2}, tv[3] = {t0, t1, t2};
+  R a[3][3], b[3][3], oa[3][3], ob[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int va = sel3(s0, s1, s2, pi_[c]), vb = sel3(t0, t1, t2, pj_[c]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      a[c][d] = (R)g.vertices[3 * va + d];
+      b[c][d] = (R)g.vertices[3 * vb + d];
+      oa[c][d] = (R)g.vertices[3 * sv[c] + d];
+      ob[c][d] = (R)g.vertices[3 * tv[c] + d];
+    }
+  }
+  R ni[3], nj[3], Ji, Jj;
+  {
+    const R e1[3] = {oa[1][0] - oa[0][0], oa[1][1] - oa[0][1], oa[1][2] - oa[0][2]};
+    const R e2[3] = {oa[2][0] - oa[0][0], oa[2][1] - oa[0][1], oa[2][2] - oa[0][2]};
+    const R cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    Ji = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    for (int d = 0; d < 3; d++) ni[d] = cr[d] / Ji;
+  }
+  {
+    const R e1[3] = {ob[1][0] - ob[0][0], ob[1][1] - ob[0][1], ob[1][2] - ob[0][2]};
+    const R e2[3] = {ob[2][0] - ob[0][0], ob[2][1] - ob[0][1], ob[2][2] - ob[0][2]};
+    const R cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    Jj = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    for (int d = 0; d < 3; d++) nj[d] = cr[d] / Jj;
+  }
+  const R kk = (R)P.k, kinv = R(1) / kk;
+  const R nn = ni[0] * nj[0] + ni[1] * nj[1] + ni[2] * nj[2];
+  R accL[18], accR[18], aux[2] = {0, 0};
+#pragma unroll
+  for (int e = 0; e < 18; e++) accL[e] = accR[e] = 0;
+  auto region = [&](R x1, R x2, R y1, R y2, R ww) {
+    const R lx[3] = {R(1) - x1, x1 - x2, x2};
+    const R ly[3] = {R(1) - y1, y1 - y2, y2};
+    R xp[3], yp[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      xp[d] = lx[0] * a[0][d] + lx[1] * a[1][d] + lx[2] * a[2][d];
+      yp[d] = ly[0] * b[0][d] + ly[1] * b[1][d] + ly[2] * b[2][d];
+    }
+    R lr, li, ar, ai, rr, ri;
+    bm_eval<R>(yp[0] - xp[0], yp[1] - xp[1], yp[2] - xp[2], ni, nj, nn, kk, kinv, lr, li, ar, ai, rr, ri);
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+      for (int jj = 0; jj < 3; jj++) {
+        const R f = lx[ii] * ly[jj] * ww;
+        accL[2 * (3 * ii + jj)] += lr * f;
+        accL[2 * (3 * ii + jj) + 1] += li * f;
+        accR[2 * (3 * ii + jj)] += rr * f;
+        accR[2 * (3 * ii + jj) + 1] += ri * f;
+      }
+    aux[0] += ar * ww;
+    aux[1] += ai * ww;
+  };
+  const R jw = Ji * Jj / R(16);
+  constexpr int NPT = LN * LN * LN * LN;
+#pragma unroll 1
+  for (int pt = lane; pt < NPT; pt += 32) {
+    const int i0 = pt / (LN * LN * LN), i1 = (pt / (LN * LN)) % LN, i2 = (pt / LN) % LN, i3 = pt % LN;
+    const R xi = R(0.5) * (R(gl_x<LN>(i0)) + R(1)), e1 = R(0.5) * (R(gl_x<LN>(i1)) + R(1));
+    const R e2 = R(0.5) * (R(gl_x<LN>(i2)) + R(1)), e3 = R(0.5) * (R(gl_x<LN>(i3)) + R(1));
+    const R w0 = R(gl_w<LN>(i0)) * R(gl_w<LN>(i1)) * R(gl_w<LN>(i2)) * R(gl_w<LN>(i3)) * jw;
+    ss_regions<NCOMMON, R>(xi, e1, e2, e3, w0, region);
+  }
+#pragma unroll
+  for (int e = 0; e < 18; e++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      accL[e] += __shfl_xor_sync(0xffffffffu, accL[e], o);
+      accR[e] += __shfl_xor_sync(0xffffffffu, accR[e], o);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    aux[0] += __shfl_xor_sync(0xffffffffu, aux[0], o);
+    aux[1] += __shfl_xor_sync(0xffffffffu, aux[1], o);
+  }
+  if (lane < 9) {
+    const int ii = lane / 3, jj = lane % 3;  // re-ordered slots
+    const int ia = pi_[ii], jb = pj_[jj];    // original local vertices
+    R cp = 0;
+    for (int d = 0; d < 3; d++) cp += (R)g.curls[9 * ti + 3 * ia + d] * (R)g.curls[9 * tj + 3 * jb + d];
+    R lre = accL[2 * lane] + aux[0] * cp, lim = accL[2 * lane + 1] + aux[1] * cp;
+    R rre = accR[2 * lane], rim = accR[2 * lane + 1];
+    const R sc = R(kInv4Pi);
+    lre *= sc;
+    lim *= sc;
+    rre *= sc;
+    rim *= sc;
+    if (NCOMMON == 3) {  // P1 mass: area (1 + [a == b]) / 12
+      const R m = R(0.5) * Ji * (ia == jb ? R(2) : R(1)) / R(12);
+      lre += R(0.5) * m;
+      rim -= R(0.5) * kinv * m;
+    }
+    const size_t at = (size_t)sel3(s0, s1, s2, ia) * g.nv + sel3(t0, t1, t2, jb);
+    atomicAdd(&P.L[at], make_float2((float)lre, (float)lim));
+    atomicAdd(&P.R[at], make_float2((float)rre, (float)rim));
+  }
+}
+
+template <typename R, int NCOMMON>
+__global__ void __launch_bounds__(128) singular_bm_kernel(const __grid_constant__ BmProblem P, int npairs) {
+  const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pair >= npairs) return;
+  singular_bm_pair<R, NCOMMON>(P, pair);
+}
+
+template <typename R, int NCOMMON>
+__global__ void __launch_bounds__(128)
+    singular_bm_batch_kernel(const BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
+  constexpr int which = NCOMMON == 3 ? 0 : (NCOMMON == 2 ? 1 : 2);
+  const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pair >= hdr->total_pairs[which]) return;
+  const BmProblem& P = probs[bm_find(probs, hdr->nproblems, pair, which)];
+  singular_bm_pair<R, NCOMMON>(P, (int)(pair - P.pair_begin[which]));
+}
+
+inline size_t al256(size_t x) { return (x + 255) / 256 * 256; }
+
+int bm_sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+// Host staging of the batch descriptors (pinned, reused; one per host thread).
+struct BmStage {
+  void* buf = nullptr;
+  size_t cap = 0;
+  cudaEvent_t ev = nullptr;
+  ~BmStage() {
+    if (buf) cudaFreeHost(buf);
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+thread_local BmStage t_bm_stage;
+
+int bm_check(float k, const float2* L, const float2* R) {
+  if (!L || !R) return BEM_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(k)) return BEM_ERR_NONFINITE;
+  if (k == 0.f) return BEM_ERR_INVALID_ARGUMENT;  // the Burton-Miller coupling i/k
+  return BEM_OK;
+}
+
+// Persistent grid of a regular kernel (shared-memory attribute set once).
+template <typename KernelT>
+int bm_grid(KernelT kernel, std::atomic<bool>& attr, long long* grid) {
+  const int smem = (int)sizeof(BmSmem);
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr.store(true, std::memory_order_release);
+  }
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBmThreads, smem));
+  *grid = (long long)bm_sm_count() * (occ > 0 ? occ : 1);
+  return BEM_OK;
+}
+
+long long bm_units_of(const GeomView& g) {
+  const long long ngroups = (g.nt + kBmTest - 1) / kBmTest;
+  return ngroups * g.ntiles - ngroups * (ngroups - 1);
+}
+
+}  // namespace
+
+size_t bm_workspace_bytes(int np) {
+  return al256(sizeof(BmHeader)) + al256(sizeof(BmProblem) * (size_t)(np > 0 ? np : 1));
+}
+
+// lhs = BM_LHS + 1/2 M and rhs = BM_RHS - (i/(2k)) M of one problem (both
+// nv x nv complex64, overwritten).
+int assemble_bm(const GeomView& g, float k, float2* L, float2* R, cudaStream_t s) {
+  int rc = bm_check(k, L, R);
+  if (rc) return rc;
+  static std::atomic<bool> attr{false};
+  long long grid = 0;
+  if ((rc = bm_grid(regular_bm_kernel, attr, &grid))) return rc;
+  BEM_CUDA_TRY(cudaMemsetAsync(L, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
+  BEM_CUDA_TRY(cudaMemsetAsync(R, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
+  BmProblem P;
+  std::memset(&P, 0, sizeof(P));
+  P.g = g;
+  P.k = k;
+  P.n_units = bm_units_of(g);
+  const long long chunk = (P.n_units + 8 * grid - 1) / (8 * grid);  // 8 equal items per CTA
+  P.chunk = (int)(chunk < 1 ? 1 : chunk);
+  P.L = L;
+  P.R = R;
+  const long long items = (P.n_units + P.chunk - 1) / P.chunk;
+  if (items > 0)
+    (regular_bm_kernel<<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(P, (int)items),
+     count_launch());
+  const int wpb = 4;
+  (singular_bm_kernel<double, 3><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.nt), count_launch());
+  if (g.n_edge)
+    (singular_bm_kernel<float, 2><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_edge), count_launch());
+  if (g.n_vert)
+    (singular_bm_kernel<float, 1><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_vert), count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+// The same for many problems: one queue-driven launch over every problem's
+// regular pairs, one launch per touching-pair type.
+int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls, float2* const* Rs, int np,
+                      void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (np <= 0 || !views || !ks || !Ls || !Rs) return BEM_ERR_INVALID_ARGUMENT;
+  if (!ws || ws_bytes < bm_workspace_bytes(np)) return BEM_ERR_WORKSPACE;
+  int rc;
+  for (int p = 0; p < np; p++)
+    if ((rc = bm_check(ks[p], Ls[p], Rs[p]))) return rc;
+  static std::atomic<bool> attr{false};
+  long long grid = 0;
+  if ((rc = bm_grid(regular_bm_batch_kernel, attr, &grid))) return rc;
+
+  const size_t hbytes = al256(sizeof(BmHeader)), pbytes = sizeof(BmProblem) * (size_t)np;
+  BmStage& st = t_bm_stage;
+  if (!st.ev) BEM_CUDA_TRY(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
+  BEM_CUDA_TRY(cudaEventSynchronize(st.ev));  // the previous upload from the staging buffer is done
+  if (st.cap < hbytes + pbytes) {
+    if (st.buf) cudaFreeHost(st.buf);
+    st.buf = nullptr;
+    st.cap = 0;
+    BEM_CUDA_TRY(cudaHostAlloc(&st.buf, 2 * (hbytes + pbytes), cudaHostAllocDefault));
+    st.cap = 2 * (hbytes + pbytes);
+  }
+  BmHeader* hh = (BmHeader*)st.buf;
+  BmProblem* hp = (BmProblem*)((char*)st.buf + hbytes);
+  std::memset(hh, 0, sizeof(BmHeader));
+  std::memset(hp, 0, pbytes);
+  hh->nproblems = np;
+  long long units_all = 0;
+  for (int p = 0; p < np; p++) units_all += bm_units_of(views[p]);
+  // about 8 items per CTA over the whole batch, at most 64 units per item
+  long long chunk = (units_all + 8 * grid - 1) / (8 * grid);
+  chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
+  long long items = 0, pairs[3] = {0, 0, 0};
+  for (int p = 0; p < np; p++) {
+    const GeomView& g = views[p];
+    BEM_CUDA_TRY(cudaMemsetAsync(Ls[p], 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
+    BEM_CUDA_TRY(cudaMemsetAsync(Rs[p], 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
+    BmProblem& P = hp[p];
+    P.g = g;
+    P.k = ks[p];
+    P.n_units = bm_units_of(g);
+    P.chunk = (int)chunk;
+    P.item_begin = items;
+    items += (P.n_units + P.chunk - 1) / P.chunk;
+    P.pair_begin[0] = pairs[0];
+    P.pair_begin[1] = pairs[1];
+    P.pair_begin[2] = pairs[2];
+    pairs[0] += g.nt;
+    pairs[1] += g.n_edge;
+    pairs[2] += g.n_vert;
+    P.L = Ls[p];
+    P.R = Rs[p];
+  }
+  hh->total_items = items;
+  for (int t = 0; t < 3; t++) hh->total_pairs[t] = pairs[t];
+  BmHeader* dh = (BmHeader*)ws;
+  BmProblem* dp = (BmProblem*)((char*)ws + hbytes);
+  BEM_CUDA_TRY(cudaMemcpyAsync(ws, st.buf, hbytes + pbytes, cudaMemcpyHostToDevice, s));
+  BEM_CUDA_TRY(cudaEventRecord(st.ev, s));
+  if (items > 0)
+    (regular_bm_batch_kernel<<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(dh, dp),
+     count_launch());
+  const int wpb = 4;
+  if (pairs[0])
+    (singular_bm_batch_kernel<double, 3><<<(unsigned)((pairs[0] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+     count_launch());
+  if (pairs[1])
+    (singular_bm_batch_kernel<float, 2><<<(unsigned)((pairs[1] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+     count_launch());
+  if (pairs[2])
+    (singular_bm_batch_kernel<float, 1><<<(unsigned)((pairs[2] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+     count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+// Reads and clears the flag that a Burton-Miller kernel's bounded wait
+// expired (synchronises the stream).
+int bm_status(int* err_host, cudaStream_t s) {
+  int zero = 0;
+  BEM_CUDA_TRY(cudaMemcpyFromSymbolAsync(err_host, g_bm_err, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaMemcpyToSymbolAsync(g_bm_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  return BEM_OK;
+}
+
+}  // namespace bemb

@@ -18,6 +18,11 @@ int get_tuning(int key);
 size_t batch_workspace_bytes(int np);
 int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs, float2* const* Ks, int np,
                       float mass_coeff, float k_coeff, void* ws, size_t ws_bytes, cudaStream_t s);
+int assemble_bm(const GeomView& g, float k, float2* L, float2* R, cudaStream_t s);
+size_t bm_workspace_bytes(int np);
+int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls, float2* const* Rs, int np,
+                      void* ws, size_t ws_bytes, cudaStream_t s);
+int bm_status(int* err_host, cudaStream_t s);
 }  // namespace bemb
 
 namespace bemb {
@@ -85,7 +90,35 @@ extern "C" int bem_identity_matrix(const void* geom, void* out, bem_stream_t str
 
 extern "C" int bem_set_tuning(int key, int value) { return set_tuning(key, value); }
 extern "C" int bem_get_tuning(int key) { return get_tuning(key); }
-extern "C" size_t bem_batch_workspace_bytes(int nproblems) { return batch_workspace_bytes(nproblems); }
+extern "C" size_t bem_batch_workspace_bytes(int nproblems) {
+  const size_t a = batch_workspace_bytes(nproblems), b = bm_workspace_bytes(nproblems);
+  return a > b ? a : b;
+}
+
+extern "C" int bem_boundary_matrices_bm(const void* geom, float k, void* lhs_out, void* rhs_out,
+                                        bem_stream_t stream) {
+  GeomView g;
+  int rc = geom_view(geom, &g, nullptr);
+  if (rc) return rc;
+  return assemble_bm(g, k, (float2*)lhs_out, (float2*)rhs_out, (cudaStream_t)stream);
+}
+
+extern "C" int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproblems, void* workspace,
+                                     size_t workspace_bytes, bem_stream_t stream) {
+  if (!problems || nproblems <= 0) return BEM_ERR_INVALID_ARGUMENT;
+  std::vector<GeomView> views(nproblems);
+  std::vector<float> ks(nproblems);
+  std::vector<float2*> Ls(nproblems), Rs(nproblems);
+  for (int p = 0; p < nproblems; p++) {
+    int rc = geom_view(problems[p].geom, &views[p], nullptr);
+    if (rc) return rc;
+    ks[p] = problems[p].k;
+    Ls[p] = (float2*)problems[p].lhs_out;
+    Rs[p] = (float2*)problems[p].rhs_out;
+  }
+  return assemble_bm_batch(views.data(), ks.data(), Ls.data(), Rs.data(), nproblems, workspace, workspace_bytes,
+                           (cudaStream_t)stream);
+}
 
 extern "C" int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, float mass_coeff, float k_coeff,
                                      void* workspace, size_t workspace_bytes, bem_stream_t stream) {
@@ -105,8 +138,9 @@ extern "C" int bem_batch_matrices_vk(const bem_batch_problem* problems, int npro
 }
 
 extern "C" int bem_assembly_status(bem_stream_t stream) {
-  int err = 0;
-  const int rc = assembly_status(&err, (cudaStream_t)stream);
+  int err = 0, err_bm = 0;
+  int rc = assembly_status(&err, (cudaStream_t)stream);
   if (rc) return rc;
-  return err ? BEM_ERR_CUDA : BEM_OK;
+  if ((rc = bm_status(&err_bm, (cudaStream_t)stream))) return rc;
+  return (err || err_bm) ? BEM_ERR_CUDA : BEM_OK;
 }

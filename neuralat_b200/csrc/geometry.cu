@@ -212,6 +212,7 @@ int analyse_host(HostGeom& g) {
   h.off_trirec_orig = take(sizeof(TriRec) * (size_t)nt);
   h.off_normals = take(sizeof(float) * 3 * (size_t)nt);
   h.off_curls = take(sizeof(float) * 9 * (size_t)nt);
+  h.off_bmrec = take(sizeof(BmRec) * (size_t)nt);
   h.bytes = off;
   return BEM_OK;
 }
@@ -220,7 +221,7 @@ int analyse_host(HostGeom& g) {
 __global__ void geom_records_kernel(int nt, const float* __restrict__ verts, const int* __restrict__ tris,
                                     const int* __restrict__ perm, TriRec* __restrict__ rec_sorted,
                                     TriRec* __restrict__ rec_orig, float* __restrict__ normals,
-                                    float* __restrict__ curls) {
+                                    float* __restrict__ curls, BmRec* __restrict__ bm) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nt) return;
   int i = perm[s];
@@ -271,12 +272,22 @@ __global__ void geom_records_kernel(int nt, const float* __restrict__ verts, con
   d3 c1 = {i11 * e1.x + i12 * e2.x, i11 * e1.y + i12 * e2.y, i11 * e1.z + i12 * e2.z};
   d3 c2 = {i12 * e1.x + i22 * e2.x, i12 * e1.y + i22 * e2.y, i12 * e1.z + i22 * e2.z};
   d3 gr[3] = {{-(c1.x + c2.x), -(c1.y + c2.y), -(c1.z + c2.z)}, c1, c2};
+  BmRec m;
   for (int b = 0; b < 3; b++) {
     d3 c = cross3(n, gr[b]);
-    curls[9 * i + 3 * b] = (float)c.x;
-    curls[9 * i + 3 * b + 1] = (float)c.y;
-    curls[9 * i + 3 * b + 2] = (float)c.z;
+    curls[9 * i + 3 * b] = m.curl[3 * b] = (float)c.x;
+    curls[9 * i + 3 * b + 1] = m.curl[3 * b + 1] = (float)c.y;
+    curls[9 * i + 3 * b + 2] = m.curl[3 * b + 2] = (float)c.z;
   }
+  // 3-point degree-2 rule: point q = 2/3 vertex q + 1/6 (each other vertex)
+  for (int q = 0; q < 3; q++) {
+    const double own = 2.0 / 3.0 - 1.0 / 6.0, all = 1.0 / 6.0;
+    m.qp[3 * q] = (float)(all * (p[0].x + p[1].x + p[2].x) + own * p[q].x);
+    m.qp[3 * q + 1] = (float)(all * (p[0].y + p[1].y + p[2].y) + own * p[q].y);
+    m.qp[3 * q + 2] = (float)(all * (p[0].z + p[1].z + p[2].z) + own * p[q].z);
+  }
+  m.pad[0] = m.pad[1] = 0.f;
+  bm[s] = m;
 }
 
 }  // namespace
@@ -326,6 +337,7 @@ int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr) {
   v->vert_pairs = (const int2*)(b + h.off_vert_pairs);
   v->normals = (const float*)(b + h.off_normals);
   v->curls = (const float*)(b + h.off_curls);
+  v->bm = (const BmRec*)(b + h.off_bmrec);
   if (out_hdr) *out_hdr = h;
   return BEM_OK;
 }
@@ -366,7 +378,7 @@ extern "C" int bem_geometry_build(const float* vertices, int nv, const int* tria
   (geom_records_kernel<<<(nt + 127) / 128, 128, 0, s>>>(
       nt, (const float*)(b + h.off_vertices), (const int*)(b + h.off_triangles), (const int*)(b + h.off_perm),
       (TriRec*)(b + h.off_trirec), (TriRec*)(b + h.off_trirec_orig), (float*)(b + h.off_normals),
-      (float*)(b + h.off_curls)), count_launch());
+      (float*)(b + h.off_curls), (BmRec*)(b + h.off_bmrec)), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
   BEM_CUDA_TRY(cudaStreamSynchronize(s));  // staging buffer is pageable host memory
   cache_put(geom, h);
