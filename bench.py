@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--validate", action="store_true", help="also compare against the FP64 oracle (minutes)")
-    ap.add_argument("--kernel-case", choices=["assemble", "solve", "eval"], default=None,
+    ap.add_argument("--kernel-case", choices=["assemble", "assemble_bm", "solve", "eval"], default=None,
                     help="profiling case: one stage on an icosphere of --subdiv, after one warm-up launch")
     ap.add_argument("--subdiv", type=int, default=4)
     ap.add_argument("--large-case", action="store_true",
@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--batch-meshes", type=int, default=16)
     ap.add_argument("--batch-k", type=int, default=4)
     ap.add_argument("--batch-max-subdiv", type=int, default=4)
+    ap.add_argument("--modal-case", action="store_true",
+                    help="multi-mode workload (EditableModalSound.solve): one object, --modal-modes modes at "
+                         "log-uniform 200-8000 Hz, Burton-Miller solve per mode, 256 listeners")
+    ap.add_argument("--modal-subdiv", type=int, default=4)
+    ap.add_argument("--modal-modes", type=int, default=64)
     return ap.parse_args()
 
 
@@ -463,6 +468,8 @@ def run_kernel_case(args):
     for _ in range(2):
         if args.kernel_case == "assemble":
             s.assemble_vk(k)
+        elif args.kernel_case == "assemble_bm":
+            s.assemble_bm(k)
         elif args.kernel_case == "solve":
             gmres(A, rhs, rtol=1e-6, precision=args.precision)
         else:
@@ -634,9 +641,66 @@ def run_grad_case(args):
     print(json.dumps(line), flush=True)
 
 
+def run_modal_case(args):
+    """The reference's multi-mode loop (src/scene.py:384-397) three ways, each
+    mode a Burton-Miller solve plus listener evaluation: the reference's
+    operator structure on this library's kernels (bm_lhs, bm_rhs and the
+    identity assembled separately and combined elementwise, FP32 GMRES), the
+    fused assembly per mode (``neumann2dirichlet``), and ``solve_modes``."""
+    import torch
+
+    from neuralat_b200.bem import BEM_Solver, solve_linear_equation, solve_modes
+    from neuralat_b200.bem import meshes as M
+
+    rng = np.random.default_rng(11)
+    v, t = M.icosphere(args.modal_subdiv, 0.15)
+    v = (v * rng.uniform(0.7, 1.3, size=3)).astype(np.float32)
+    nm = args.modal_modes
+    ks = [M.wavenumber(f) for f in np.sort(10.0 ** rng.uniform(np.log10(200.0), np.log10(8000.0), nm))]
+    neu = torch.from_numpy(M.smoothed_gaussian_field(v.shape[0], t, nm, seed=3).T.copy().astype(np.complex64)).cuda()
+    pts = torch.from_numpy(M.sphere_points(256, 0.5, seed=0).astype(np.float32)).cuda()
+    s = BEM_Solver(v, t)
+
+    def operator_path():
+        out = []
+        for i, k in enumerate(ks):
+            Id = s.identity_matrix()
+            lhs = (s.assemble_boundary_matrix(k, "bm_lhs", approx=True) + 0.5 * Id).contiguous()
+            rhs_m = (s.assemble_boundary_matrix(k, "bm_rhs", approx=True) - (0.5j / k) * Id).contiguous()
+            u = solve_linear_equation(lhs, rhs_m @ neu[i])
+            out.append(s.boundary2potential(k, neu[i], u, pts))
+        return torch.stack(out)
+
+    def fused_loop():
+        return torch.stack([s.boundary2potential(k, neu[i], s.neumann2dirichlet(k, neu[i]), pts)
+                            for i, k in enumerate(ks)])
+
+    def batched():
+        return solve_modes(s, ks, neu, pts)
+
+    times, outs = {}, {}
+    for name, fn in (("operator_path", operator_path), ("fused_loop", fused_loop), ("solve_modes", batched)):
+        fn()  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outs[name] = fn()
+        torch.cuda.synchronize()
+        times[name] = time.perf_counter() - t0
+    ref = outs["operator_path"]
+    line = {"case": "modal", "N": int(v.shape[0]), "T": int(t.shape[0]), "modes": nm, "listeners": int(pts.shape[0]),
+            "modes_per_s": {k_: nm / t_ for k_, t_ in times.items()},
+            "speedup_vs_operator_path": {k_: times["operator_path"] / t_ for k_, t_ in times.items()},
+            "max_rel_diff_vs_operator_path": {k_: float(((o - ref).abs().max(dim=1).values /
+                                                          ref.abs().max(dim=1).values).max())
+                                              for k_, o in outs.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.grad_case:
+    if args.modal_case:
+        run_modal_case(args)
+    elif args.grad_case:
         run_grad_case(args)
     elif args.large_case:
         run_large_case(args)
