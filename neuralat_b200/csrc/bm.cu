@@ -20,10 +20,13 @@
 //   lhs_ij = -ik nn S + T + (i/k) s cc      lhs_ji^T = -ik nn S + U + (i/k) s cc
 //   rhs_ij = -S + (i/k) U                   rhs_ji^T = -S + (i/k) T
 // with s = sum_ab S_ab (the P1 functions sum to one) and cc_ab the curl
-// products.  The work decomposition is the symmetric V/K assembly's: 32 test
-// triangles per CTA (one per lane), 16-triangle trial tiles double-buffered
-// in shared memory by bulk copies, one trial triangle per warp, corner slabs
-// reduced on chip onto distinct vertices, four vector atomics per entry.
+// products.  Work decomposition: a CTA of 8 warps owns one 16-triangle test
+// tile (test triangle = lane & 15) and sweeps 16-triangle trial tiles,
+// double-buffered in shared memory by bulk copies, each warp taking two trial
+// triangles (one per half-warp); the 3x3 blocks go to corner slabs that are
+// reduced on chip onto the tiles' distinct vertices, four vector atomics per
+// entry.  The slabs are small enough for two CTAs per SM, so one CTA's
+// reduction and barriers overlap the other's evaluation.
 // Touching pairs: one warp per pair evaluates both kernels at each
 // Sauter-Schwab point (shared r and sincos); the coincident pass (FP64) adds
 // the mass terms.  A batch (meshes, wavenumbers) uses the same kernels with a
@@ -41,25 +44,25 @@ namespace bemb {
 
 namespace {
 
-constexpr int kBmThreads = 32 * kTile;       // 512: warp w takes trial triangle w
-constexpr int kBmTest = 32;                  // test triangles per CTA, one per lane
-constexpr int kBmCorners = 3 * kBmTest;      // 96
+constexpr int kBmThreads = 16 * kTile;       // 256: warp w takes trial triangles 2w, 2w + 1
+constexpr int kBmTest = kTile;               // test triangles per CTA (one tile), lane & 15
+constexpr int kBmCorners = 3 * kBmTest;      // 48
 constexpr int kBmStride = kTileCorners + 1;  // 49 float2: conflict-free column writes
 
 // 3-point rule: C(q, b) = w_q phi_b(q) = 1/3 * (q == b ? 2/3 : 1/6)
 __host__ __device__ constexpr float bm_c(int q, int b) { return q == b ? 2.0f / 9.0f : 1.0f / 18.0f; }
 
 struct BmSmem {
-  float2 slotL[kBmCorners][kBmStride];   // lhs_ij[a][b] at [3 lane + a][3 tt + b]
+  float2 slotL[kBmCorners][kBmStride];   // lhs_ij[a][b] at [3 tl + a][3 tt + b]
   float2 slotLT[kBmCorners][kBmStride];  // lhs_ji[b][a], same indexing
   float2 slotR[kBmCorners][kBmStride];
   float2 slotRT[kBmCorners][kBmStride];
-  float xs[9][kBmTest];                  // test quadrature points [coordinate][lane]
-  float xc[9][kBmTest];                  // test curls [3 a + d][lane]
+  float xs[9][kBmTest];                  // test quadrature points [coordinate][tl]
+  float xc[9][kBmTest];                  // test curls [3 a + d][tl]
   TriRec trial[2][kTile];                // trial tile, double-buffered
   BmRec trialB[2][kTile];
   TileRec tileJ[2];
-  TileRec tileI[2];
+  TileRec tileI;
   uint64_t tile_full[2];
 };
 
@@ -83,9 +86,9 @@ __device__ __forceinline__ void bm_fetch_tile(BmSmem& sm, const GeomView& g, int
   bulk_load(&sm.tileJ[b], &g.tiles[jt], (uint32_t)sizeof(TileRec), &sm.tile_full[b]);
 }
 
-// S, T, U blocks of one unordered pair under the 3x3 point rule (lane = test
-// triangle, points in xs; trial points yq, dq[q] = n_i . (c_i - y_q)).
-__device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int lane, const float (&yq)[9],
+// S, T, U blocks of one unordered pair under the 3x3 point rule (test
+// triangle tl, points in xs; trial points yq, dq[q] = n_i . (c_i - y_q)).
+__device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl, const float (&yq)[9],
                                               const float (&dq)[3], float njx, float njy, float njz, float cjx,
                                               float cjy, float cjz, float k, float2 (&aS)[9], float2 (&aT)[9],
                                               float2 (&aU)[9]) {
@@ -97,7 +100,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int la
   }
 #pragma unroll
   for (int p = 0; p < 3; p++) {
-    const float px = xs[3 * p][lane], py = xs[3 * p + 1][lane], pz = xs[3 * p + 2][lane];
+    const float px = xs[3 * p][tl], py = xs[3 * p + 1][tl], pz = xs[3 * p + 2][tl];
     const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);  // (y - x).n_j on plane j
     float2 tS[3], tT[3], tU[3];
 #pragma unroll
@@ -147,17 +150,17 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int la
   }
 }
 
-// One work item: test group grp against trial tiles [jt_begin, jt_end).
-// `uses` counts the trial tiles this CTA has processed (buffer = uses & 1,
-// mbarrier parity = (uses >> 1) & 1).
+// One work item: test tile grp against trial tiles [jt_begin, jt_end), all
+// at or after grp.  `uses` counts the trial tiles this CTA has processed
+// (buffer = uses & 1, mbarrier parity = (uses >> 1) & 1).
 __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, float2* __restrict__ L,
                                         float2* __restrict__ Rm, int grp, int jt_begin, int jt_end,
                                         unsigned& uses) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tl = lane & 15;               // test triangle of this lane
+  const int tt = 2 * warp + (lane >> 4);  // trial triangle of this half-warp
   const int nt = g.nt, nv = g.nv;
-  const int tile0 = 2 * grp;
-  const bool has_t1 = tile0 + 1 < g.ntiles;
-  const int ti = grp * kBmTest + lane;
+  const int ti = grp * kBmTest + tl;
   const bool valid_i = ti < nt;
   const TriRec& ri = g.rec[valid_i ? ti : nt - 1];
   const float area_i = ri.area;
@@ -167,8 +170,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
 
   __syncthreads();  // the previous item is done with tileI, xs, xc and both trial buffers
   if (tid == 0) bm_fetch_tile(sm, g, jt_begin, uses & 1);
-  bm_copy_words(&sm.tileI[0], &g.tiles[tile0], sizeof(TileRec), tid);
-  if (has_t1) bm_copy_words(&sm.tileI[1], &g.tiles[tile0 + 1], sizeof(TileRec), tid);
+  bm_copy_words(&sm.tileI, &g.tiles[grp], sizeof(TileRec), tid);
   for (int e = tid; e < 18 * kBmTest; e += kBmThreads) {
     const int c = e / kBmTest, l = e - c * kBmTest;
     const int t = min(grp * kBmTest + l, nt - 1);
@@ -189,8 +191,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
     const TileRec& tileJ = sm.tileJ[bf];
     const int ntriJ = min(kTile, nt - jt * kTile);
 
-    // ---- compute: warp w takes trial triangle w ----
-    const int tt = warp;
+    // ---- compute: half-warp h of warp w takes trial triangle 2w + h ----
     const int tj = jt * kTile + tt;
     float aa = 0.f;
     if (tt < ntriJ) {
@@ -198,10 +199,11 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       const int j0 = rj.v[0], j1 = rj.v[1], j2 = rj.v[2];
       const bool touching = (iv0 == j0) | (iv0 == j1) | (iv0 == j2) | (iv1 == j0) | (iv1 == j1) | (iv1 == j2) |
                             (iv2 == j0) | (iv2 == j1) | (iv2 == j2);
-      const bool once = jt >= tile0 + 2 || tj > ti;  // on the group's own tiles each unordered pair once
+      const bool once = jt > grp || tj > ti;  // on the test tile itself each unordered pair once
       aa = (valid_i && !touching && once) ? area_i * rj.area : 0.f;
     }
-    if (tt < ntriJ && __any_sync(0xffffffffu, aa != 0.f)) {
+    const bool any = __any_sync(0xffffffffu, aa != 0.f);  // every lane, before the half-warp branch
+    if (tt < ntriJ && any) {
       const TriRec& rj = sm.trial[bf][tt];
       const BmRec& bj = sm.trialB[bf][tt];
       float yq[9];
@@ -212,7 +214,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       for (int q = 0; q < 3; q++)
         dq[q] = nix * (cix - yq[3 * q]) + niy * (ciy - yq[3 * q + 1]) + niz * (ciz - yq[3 * q + 2]);
       float2 aS[9], aT[9], aU[9];
-      bm_pair_block(sm.xs, lane, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aS, aT, aU);
+      bm_pair_block(sm.xs, tl, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aS, aT, aU);
       const float sc = aa * kInv4Pi;
       float2 s9 = make_float2(0.f, 0.f);
 #pragma unroll
@@ -227,46 +229,42 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-          const float cc = sm.xc[3 * a][lane] * bj.curl[3 * b] + sm.xc[3 * a + 1][lane] * bj.curl[3 * b + 1] +
-                           sm.xc[3 * a + 2][lane] * bj.curl[3 * b + 2];
+          const float cc = sm.xc[3 * a][tl] * bj.curl[3 * b] + sm.xc[3 * a + 1][tl] * bj.curl[3 * b + 1] +
+                           sm.xc[3 * a + 2][tl] * bj.curl[3 * b + 2];
           const float Sx = aS[3 * a + b].x * sc, Sy = aS[3 * a + b].y * sc;
           const float Tx = aT[3 * a + b].x * sc, Ty = aT[3 * a + b].y * sc;
           const float Ux = aU[3 * a + b].x * sc, Uy = aU[3 * a + b].y * sc;
           const float lx = fmaf(knn, Sy, -s9.y * cc), ly = fmaf(-knn, Sx, s9.x * cc);
-          sm.slotL[3 * lane + a][3 * tt + b] = make_float2(lx + Tx, ly + Ty);
-          sm.slotLT[3 * lane + a][3 * tt + b] = make_float2(lx + Ux, ly + Uy);
-          sm.slotR[3 * lane + a][3 * tt + b] = make_float2(fmaf(-Uy, kinv, -Sx), fmaf(Ux, kinv, -Sy));
-          sm.slotRT[3 * lane + a][3 * tt + b] = make_float2(fmaf(-Ty, kinv, -Sx), fmaf(Tx, kinv, -Sy));
+          sm.slotL[3 * tl + a][3 * tt + b] = make_float2(lx + Tx, ly + Ty);
+          sm.slotLT[3 * tl + a][3 * tt + b] = make_float2(lx + Ux, ly + Uy);
+          sm.slotR[3 * tl + a][3 * tt + b] = make_float2(fmaf(-Uy, kinv, -Sx), fmaf(Ux, kinv, -Sy));
+          sm.slotRT[3 * tl + a][3 * tt + b] = make_float2(fmaf(-Ty, kinv, -Sx), fmaf(Tx, kinv, -Sy));
         }
     } else if (tt < ntriJ) {
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-          sm.slotL[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
-          sm.slotLT[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
-          sm.slotR[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
-          sm.slotRT[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotL[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotLT[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotR[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotRT[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
         }
     }
     __syncthreads();
 
     // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
-    const int nI0 = sm.tileI[0].nlv;
-    const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
+    const TileRec& TI = sm.tileI;
     const int nJ = tileJ.nlv;
-    const int total = (nI0 + nI1) * nJ;
+    const int total = TI.nlv * nJ;
     for (int e = tid; e < total; e += kBmThreads) {
-      const int ai = e / nJ;
-      const int b = e - ai * nJ;
-      const int s = ai >= nI0;
-      const int a = ai - s * nI0;
-      const TileRec& TI = sm.tileI[s];
+      const int a = e / nJ;
+      const int b = e - a * nJ;
       float2 l = make_float2(0.f, 0.f), lt = l, rr = l, rt = l;
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
       for (int ca = ca0; ca < ca1; ca++) {
-        const int row = s * kTileCorners + TI.lv_corner[ca];
+        const int row = TI.lv_corner[ca];
         for (int cb = cb0; cb < cb1; cb++) {
           const int col = tileJ.lv_corner[cb];
           l.x += sm.slotL[row][col].x;
@@ -291,16 +289,31 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
   }
 }
 
-// Splits units [pos, end) of one problem at test-group boundaries.
+// Units (test tile g, trial tile jt >= g) in order: tile g owns the
+// ntiles - g trial tiles from itself on, so U(g) = g ntiles - g (g - 1) / 2
+// units come before it.
+__device__ __forceinline__ long long tile_units_before(long long g, long long n) { return g * n - g * (g - 1) / 2; }
+
+__device__ __forceinline__ int tile_group_of(long long pos, int n) {
+  const double b = 2.0 * n + 1.0;
+  const double disc = b * b - 8.0 * (double)pos;
+  long long g = (long long)((b - sqrt(disc > 0.0 ? disc : 0.0)) * 0.5);
+  if (g < 0) g = 0;
+  if (g > n - 1) g = n - 1;
+  while (g + 1 < n && tile_units_before(g + 1, n) <= pos) g++;
+  while (g > 0 && tile_units_before(g, n) > pos) g--;
+  return (int)g;
+}
+
+// Splits units [pos, end) of one problem at test-tile boundaries.
 __device__ __forceinline__ void bm_units(BmSmem& sm, const GeomView& g, float k, float2* L, float2* Rm,
                                          long long pos, long long end, unsigned& uses) {
-  const int ngroups = (g.nt + kBmTest - 1) / kBmTest;
   while (pos < end) {  // uniform over the block
-    const int grp = sym_group_of(pos, g.ntiles, ngroups);
-    const long long base = sym_units_before(grp, g.ntiles);
-    const long long gend = base + (g.ntiles - 2 * grp);
+    const int grp = tile_group_of(pos, g.ntiles);
+    const long long base = tile_units_before(grp, g.ntiles);
+    const long long gend = base + (g.ntiles - grp);
     const long long stop = end < gend ? end : gend;
-    const int jt0 = 2 * grp + (int)(pos - base);
+    const int jt0 = grp + (int)(pos - base);
     bm_item(sm, g, k, L, Rm, grp, jt0, jt0 + (int)(stop - pos), uses);
     pos = stop;
   }
@@ -346,7 +359,7 @@ __device__ __forceinline__ void bm_init_barriers(BmSmem& sm) {
 
 // Regular pairs of one problem: equal work items dealt round-robin to a
 // persistent grid.
-__global__ void __launch_bounds__(kBmThreads, 1)
+__global__ void __launch_bounds__(kBmThreads, 2)
     regular_bm_kernel(const __grid_constant__ BmProblem P, int n_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BmSmem& sm = *reinterpret_cast<BmSmem*>(smem_raw);
@@ -360,7 +373,7 @@ __global__ void __launch_bounds__(kBmThreads, 1)
 }
 
 // Regular pairs of a batch: CTAs drain one queue of work items.
-__global__ void __launch_bounds__(kBmThreads, 1)
+__global__ void __launch_bounds__(kBmThreads, 2)
     regular_bm_batch_kernel(BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BmSmem& sm = *reinterpret_cast<BmSmem*>(smem_raw);
@@ -594,10 +607,7 @@ int bm_grid(KernelT kernel, std::atomic<bool>& attr, long long* grid) {
   return BEM_OK;
 }
 
-long long bm_units_of(const GeomView& g) {
-  const long long ngroups = (g.nt + kBmTest - 1) / kBmTest;
-  return ngroups * g.ntiles - ngroups * (ngroups - 1);
-}
+long long bm_units_of(const GeomView& g) { return (long long)g.ntiles * (g.ntiles + 1) / 2; }
 
 }  // namespace
 
