@@ -18,7 +18,7 @@ from .. import _lib as L
 from .batch import assemble_batch
 
 CHUNKS = (2, 4, 8, 16, 32, 64)
-CTAS = (1,)  # the symmetric regular-pair kernel holds one CTA per SM
+CTAS = (1, 2)  # persistent CTAs per SM of the symmetric regular-pair kernel (at most two fit)
 
 
 def _cache_path() -> str:

@@ -261,23 +261,26 @@ __global__ void __launch_bounds__(kRegThreads, 2)
 //   V_ji = V_ij^T,
 //   K_ij uses the trial plane of j (dn_j(p) = n_j . (c_j - x_p)),
 //   K_ji uses the plane of i at the trial points (dn_i(q) = n_i . (c_i - y_q)),
-// both from the same r, sincos and kernel values.  A work item is a test group
-// (2 tiles, 32 triangles: one per lane) against a chunk of trial tiles; only
-// trial tiles at or after the group's first tile are used, and on the group's
-// own tiles only pairs j > i.  One warp per trial triangle (16 warps); the
-// test points are staged structure-of-arrays in shared memory.
+// both from the same r, sincos and kernel values.  A work item is one test
+// tile (16 triangles, test triangle = lane & 15) against a chunk of trial
+// tiles at or after it; on the test tile itself only pairs j > i.  Each of
+// the 8 warps takes two trial triangles (one per half-warp); the test points
+// are staged structure-of-arrays in shared memory.  The slabs fit two CTAs
+// per SM, so one CTA's reduction and barriers overlap the other's evaluation.
 // ---------------------------------------------------------------------------
-constexpr int kSymThreads = 32 * kTile;  // 512: warp w takes trial triangle w
+constexpr int kSymThreads = 16 * kTile;         // 256: warp w takes trial triangles 2w, 2w + 1
+constexpr int kSymTest = kTile;                 // test triangles per CTA (one tile)
+constexpr int kSymCorners = 3 * kSymTest;       // 48
 
 struct SymSmem {
-  float2 slotV[kTestCorners][kSlotStride];
-  float2 slotK[kTestCorners][kSlotStride];
-  float2 slotM[kTestCorners][kSlotStride];  // K_ji^T, indexed like slotK
-  float xs[18][kTestTris];                  // test quadrature points, [coordinate][lane]
-  TriRec trial[2][kTile];                   // trial tile records, double-buffered
+  float2 slotV[kSymCorners][kSlotStride];
+  float2 slotK[kSymCorners][kSlotStride];
+  float2 slotM[kSymCorners][kSlotStride];  // K_ji^T, indexed like slotK
+  float xs[18][kSymTest];                  // test quadrature points, [coordinate][tl]
+  TriRec trial[2][kTile];                  // trial tile records, double-buffered
   TileRec tileJ[2];
-  TileRec tileI[2];
-  uint64_t tile_full[2];                    // bulk-copy completion of each trial buffer
+  TileRec tileI;
+  uint64_t tile_full[2];                   // bulk-copy completion of each trial buffer
 };
 
 // A bounded wait of the assembly kernels expired (read by bem_assembly_status).
@@ -293,7 +296,7 @@ __device__ __forceinline__ void sym_fetch_tile(SymSmem& sm, const GeomView& g, i
 }
 
 // aV, aK as pair_block; aM[3a+b] = sum_pq C_ap C_bq dn_i(q) Gk(r_pq) = K_ji[b][a].
-__device__ __forceinline__ void pair_block_sym(const float (*xs)[kTestTris], int lane, const float (&yq)[18],
+__device__ __forceinline__ void pair_block_sym(const float (*xs)[kSymTest], int tl, const float (&yq)[18],
                                                const float (&dq)[6], float njx, float njy, float njz, float cjx,
                                                float cjy, float cjz, float k, float2 (&aV)[9], float2 (&aK)[9],
                                                float2 (&aM)[9]) {
@@ -305,7 +308,7 @@ __device__ __forceinline__ void pair_block_sym(const float (*xs)[kTestTris], int
   }
 #pragma unroll
   for (int p = 0; p < 6; p++) {
-    const float px = xs[3 * p][lane], py = xs[3 * p + 1][lane], pz = xs[3 * p + 2][lane];
+    const float px = xs[3 * p][tl], py = xs[3 * p + 1][tl], pz = xs[3 * p + 2][tl];
     const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);
     float2 tV[3], tK[3], uK[3];
 #pragma unroll
@@ -361,10 +364,10 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
                                                  float2* __restrict__ K, float v_scale, float k_scale, int grp,
                                                  int jt_begin, int jt_end, unsigned& uses) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tl = lane & 15;               // test triangle of this lane
+  const int tt = 2 * warp + (lane >> 4);  // trial triangle of this half-warp
   const int nt = g.nt, nv = g.nv;
-  const int tile0 = 2 * grp;
-  const bool has_t1 = tile0 + 1 < g.ntiles;
-  const int ti = grp * kTestTris + lane;
+  const int ti = grp * kSymTest + tl;
   const bool valid_i = ti < nt;
   const TriRec& ri = g.rec[valid_i ? ti : nt - 1];
   const float area_i = ri.area;
@@ -373,11 +376,10 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
 
   __syncthreads();  // the previous item is done with tileI, xs and both trial buffers
   if (tid == 0) sym_fetch_tile(sm, g, jt_begin, uses & 1);
-  copy_words(&sm.tileI[0], &g.tiles[tile0], sizeof(TileRec), tid, kSymThreads);
-  if (has_t1) copy_words(&sm.tileI[1], &g.tiles[tile0 + 1], sizeof(TileRec), tid, kSymThreads);
-  for (int e = tid; e < 18 * kTestTris; e += kSymThreads) {
-    const int c = e / kTestTris, l = e - c * kTestTris;
-    const int t = min(grp * kTestTris + l, nt - 1);
+  copy_words(&sm.tileI, &g.tiles[grp], sizeof(TileRec), tid, kSymThreads);
+  for (int e = tid; e < 18 * kSymTest; e += kSymThreads) {
+    const int c = e / kSymTest, l = e - c * kSymTest;
+    const int t = min(grp * kSymTest + l, nt - 1);
     sm.xs[c][l] = g.rec[t].qp[c];
   }
 
@@ -393,8 +395,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     const TileRec& tileJ = sm.tileJ[bf];
     const int ntriJ = min(kTile, nt - jt * kTile);
 
-    // ---- compute: warp w takes trial triangle w ----
-    const int tt = warp;
+    // ---- compute: half-warp h of warp w takes trial triangle 2w + h ----
     const int tj = jt * kTile + tt;
     float aa = 0.f;
     if (tt < ntriJ) {
@@ -402,11 +403,12 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
       const int j0 = rj.v[0], j1 = rj.v[1], j2 = rj.v[2];
       const bool touching = (iv0 == j0) | (iv0 == j1) | (iv0 == j2) | (iv1 == j0) | (iv1 == j1) | (iv1 == j2) |
                             (iv2 == j0) | (iv2 == j1) | (iv2 == j2);
-      // on the group's own tiles each unordered pair once (j > i)
-      const bool once = jt >= tile0 + 2 || tj > ti;
+      // on the test tile itself each unordered pair once (j > i)
+      const bool once = jt > grp || tj > ti;
       aa = (valid_i && !touching && once) ? area_i * rj.area : 0.f;
     }
-    if (tt < ntriJ && __any_sync(0xffffffffu, aa != 0.f)) {
+    const bool any = __any_sync(0xffffffffu, aa != 0.f);  // every lane, before the half-warp branch
+    if (tt < ntriJ && any) {
       const TriRec& rj = trial[tt];
       float yq[18];
 #pragma unroll
@@ -416,44 +418,40 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
       for (int q = 0; q < 6; q++)
         dq[q] = nix * (cix - yq[3 * q]) + niy * (ciy - yq[3 * q + 1]) + niz * (ciz - yq[3 * q + 2]);
       float2 aV[9], aK[9], aM[9];
-      pair_block_sym(sm.xs, lane, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aV, aK, aM);
+      pair_block_sym(sm.xs, tl, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aV, aK, aM);
       const float sv = aa * v_scale, sk = aa * k_scale;
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-          sm.slotV[3 * lane + a][3 * tt + b] = make_float2(aV[3 * a + b].x * sv, aV[3 * a + b].y * sv);
-          sm.slotK[3 * lane + a][3 * tt + b] = make_float2(aK[3 * a + b].x * sk, aK[3 * a + b].y * sk);
-          sm.slotM[3 * lane + a][3 * tt + b] = make_float2(aM[3 * a + b].x * sk, aM[3 * a + b].y * sk);
+          sm.slotV[3 * tl + a][3 * tt + b] = make_float2(aV[3 * a + b].x * sv, aV[3 * a + b].y * sv);
+          sm.slotK[3 * tl + a][3 * tt + b] = make_float2(aK[3 * a + b].x * sk, aK[3 * a + b].y * sk);
+          sm.slotM[3 * tl + a][3 * tt + b] = make_float2(aM[3 * a + b].x * sk, aM[3 * a + b].y * sk);
         }
     } else if (tt < ntriJ) {
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-          sm.slotV[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
-          sm.slotK[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
-          sm.slotM[3 * lane + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotV[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotK[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
+          sm.slotM[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
         }
     }
     __syncthreads();
 
     // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
-    const int nI0 = sm.tileI[0].nlv;
-    const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
+    const TileRec& TI = sm.tileI;
     const int nJ = tileJ.nlv;
-    const int total = (nI0 + nI1) * nJ;
+    const int total = TI.nlv * nJ;
     for (int e = tid; e < total; e += kSymThreads) {
-      const int ai = e / nJ;
-      const int b = e - ai * nJ;
-      const int s = ai >= nI0;
-      const int a = ai - s * nI0;
-      const TileRec& TI = sm.tileI[s];
+      const int a = e / nJ;
+      const int b = e - a * nJ;
       float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f), acc_m = make_float2(0.f, 0.f);
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
       for (int ca = ca0; ca < ca1; ca++) {
-        const int row = s * kTileCorners + TI.lv_corner[ca];
+        const int row = TI.lv_corner[ca];
         for (int cb = cb0; cb < cb1; cb++) {
           const int col = tileJ.lv_corner[cb];
           acc_v.x += sm.slotV[row][col].x;
@@ -476,17 +474,30 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
   }
 }
 
-// The used (group, trial tile) units in order: group g owns the ntiles - 2g
-// trial tiles from its first tile on, so the units before group g number
-// S(g) = g (ntiles - g + 1).  Items are equal runs of `chunk` consecutive
-// units (a run crossing a group boundary is split), dealt round-robin to a
-// persistent grid: every CTA gets the same amount of work.
-__global__ void __launch_bounds__(kSymThreads, 1)
+// Splits units [pos, end) of one problem at test-tile boundaries.
+__device__ __forceinline__ void regular_sym_units(SymSmem& sm, const GeomView& g, float k, float2* V, float2* K,
+                                                  float v_scale, float k_scale, long long pos, long long end,
+                                                  unsigned& uses) {
+  while (pos < end) {  // uniform over the block
+    const int grp = tile_group_of(pos, g.ntiles);
+    const long long base = tile_units_before(grp, g.ntiles);
+    const long long gend = base + (g.ntiles - grp);
+    const long long stop = end < gend ? end : gend;
+    const int jt0 = grp + (int)(pos - base);
+    regular_sym_item(sm, g, k, V, K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos), uses);
+    pos = stop;
+  }
+}
+
+// The (test tile, trial tile >= it) units in order (tile_units_before).
+// Items are equal runs of `chunk` consecutive units (a run crossing a test
+// tile is split), dealt round-robin to a persistent grid: every CTA gets the
+// same amount of work.
+__global__ void __launch_bounds__(kSymThreads, 2)
     regular_sym_kernel(GeomView g, float k, float2* __restrict__ V, float2* __restrict__ K, float v_scale,
                        float k_scale, long long chunk, long long n_units, int n_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SymSmem& sm = *reinterpret_cast<SymSmem*>(smem_raw);
-  const int ngroups = (g.nt + kTestTris - 1) / kTestTris;
   if (threadIdx.x == 0) {
     mbar_init(&sm.tile_full[0], 1);
     mbar_init(&sm.tile_full[1], 1);
@@ -494,17 +505,9 @@ __global__ void __launch_bounds__(kSymThreads, 1)
   }
   unsigned uses = 0;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    long long pos = (long long)item * chunk;
+    const long long pos = (long long)item * chunk;
     const long long end = pos + chunk < n_units ? pos + chunk : n_units;
-    while (pos < end) {  // uniform over the block
-      const int grp = sym_group_of(pos, g.ntiles, ngroups);
-      const long long base = sym_units_before(grp, g.ntiles);
-      const long long gend = base + (g.ntiles - 2 * grp);
-      const long long stop = end < gend ? end : gend;
-      const int jt0 = 2 * grp + (int)(pos - base);
-      regular_sym_item(sm, g, k, V, K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos), uses);
-      pos = stop;
-    }
+    regular_sym_units(sm, g, k, V, K, v_scale, k_scale, pos, end, uses);
   }
 }
 
@@ -804,7 +807,7 @@ __device__ __forceinline__ int find_problem(const BatchProblem* probs, int np, l
 
 // Each unordered regular pair of every problem once (the symmetric item of
 // regular_sym_kernel); items are runs of `chunk` units of one problem.
-__global__ void __launch_bounds__(kSymThreads, 1)
+__global__ void __launch_bounds__(kSymThreads, 2)
     regular_sym_batch_kernel(BatchHeader* __restrict__ hdr, const BatchProblem* __restrict__ probs, float v_scale,
                              float k_scale) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -825,19 +828,9 @@ __global__ void __launch_bounds__(kSymThreads, 1)
     const long long item = s_item;
     if (item >= total) break;
     const BatchProblem& P = probs[find_problem(probs, np, item, -1)];
-    const GeomView& g = P.g;
-    const int ngroups = (g.nt + kTestTris - 1) / kTestTris;
-    long long pos = (item - P.item_begin) * P.chunk;
+    const long long pos = (item - P.item_begin) * P.chunk;
     const long long end = pos + P.chunk < P.n_units ? pos + P.chunk : P.n_units;
-    while (pos < end) {  // uniform over the block
-      const int grp = sym_group_of(pos, g.ntiles, ngroups);
-      const long long base = sym_units_before(grp, g.ntiles);
-      const long long gend = base + (g.ntiles - 2 * grp);
-      const long long stop = end < gend ? end : gend;
-      const int jt0 = 2 * grp + (int)(pos - base);
-      regular_sym_item(sm, g, P.k, P.V, P.K, v_scale, k_scale, grp, jt0, jt0 + (int)(stop - pos), uses);
-      pos = stop;
-    }
+    regular_sym_units(sm, P.g, P.k, P.V, P.K, v_scale, k_scale, pos, end, uses);
   }
 }
 
@@ -941,11 +934,10 @@ int launch_regular_sym(const GeomView& g, float k, float2* V, float2* K, float v
     BEM_CUDA_TRY(cudaFuncSetAttribute(regular_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set.store(true, std::memory_order_release);
   }
-  const int n_groups = (g.nt + kTestTris - 1) / kTestTris;
   int occ = 0;
   BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regular_sym_kernel, kSymThreads, smem));
   const int grid = sm_count() * (occ > 0 ? occ : 1);
-  const long long n_units = (long long)n_groups * g.ntiles - (long long)n_groups * (n_groups - 1);
+  const long long n_units = (long long)g.ntiles * (g.ntiles + 1) / 2;
   // 8 equal items per CTA (a tuned chunk overrides)
   long long chunk = (n_units + 8LL * grid - 1) / (8LL * grid);
   if (chunk < 1) chunk = 1;
@@ -1089,8 +1081,7 @@ int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs,
     BatchProblem& P = hp[p];
     P.g = g;
     P.k = ks[p];
-    const long long ngroups = (g.nt + kTestTris - 1) / kTestTris;
-    P.n_units = ngroups * g.ntiles - ngroups * (ngroups - 1);
+    P.n_units = (long long)g.ntiles * (g.ntiles + 1) / 2;
     int chunk = g_tune_chunk > 0 ? g_tune_chunk : (g.ntiles / 8 < 1 ? 1 : (g.ntiles / 8 > 64 ? 64 : g.ntiles / 8));
     P.chunk = chunk;
     P.n_chunks = (int)((P.n_units + chunk - 1) / chunk);

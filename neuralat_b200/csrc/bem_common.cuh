@@ -117,19 +117,19 @@ struct GeomView {
   const BmRec* bm;         // sorted order
 };
 
-// Symmetric regular-pair work units: test group g (32 triangles = tiles 2g,
-// 2g+1) is paired with the ntiles - 2g trial tiles from its first tile on,
-// so the units before group g number S(g) = g (ntiles - g + 1).
-__device__ __forceinline__ long long sym_units_before(long long g, long long ntiles) { return g * (ntiles - g + 1); }
+// Symmetric regular-pair work units (test tile g, trial tile jt >= g) in
+// order: test tile g owns the ntiles - g trial tiles from itself on, so
+// U(g) = g ntiles - g (g - 1) / 2 units come before it.
+__device__ __forceinline__ long long tile_units_before(long long g, long long n) { return g * n - g * (g - 1) / 2; }
 
-__device__ __forceinline__ int sym_group_of(long long pos, int ntiles, int ngroups) {
-  const double b = (double)ntiles + 1.0;
-  const double disc = b * b - 4.0 * (double)pos;
+__device__ __forceinline__ int tile_group_of(long long pos, int n) {
+  const double b = 2.0 * n + 1.0;
+  const double disc = b * b - 8.0 * (double)pos;
   long long g = (long long)((b - sqrt(disc > 0.0 ? disc : 0.0)) * 0.5);
   if (g < 0) g = 0;
-  if (g > ngroups - 1) g = ngroups - 1;
-  while (g + 1 < ngroups && sym_units_before(g + 1, ntiles) <= pos) g++;
-  while (g > 0 && sym_units_before(g, ntiles) > pos) g--;
+  if (g > n - 1) g = n - 1;
+  while (g + 1 < n && tile_units_before(g + 1, n) <= pos) g++;
+  while (g > 0 && tile_units_before(g, n) > pos) g--;
   return (int)g;
 }
 

@@ -289,22 +289,6 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
   }
 }
 
-// Units (test tile g, trial tile jt >= g) in order: tile g owns the
-// ntiles - g trial tiles from itself on, so U(g) = g ntiles - g (g - 1) / 2
-// units come before it.
-__device__ __forceinline__ long long tile_units_before(long long g, long long n) { return g * n - g * (g - 1) / 2; }
-
-__device__ __forceinline__ int tile_group_of(long long pos, int n) {
-  const double b = 2.0 * n + 1.0;
-  const double disc = b * b - 8.0 * (double)pos;
-  long long g = (long long)((b - sqrt(disc > 0.0 ? disc : 0.0)) * 0.5);
-  if (g < 0) g = 0;
-  if (g > n - 1) g = n - 1;
-  while (g + 1 < n && tile_units_before(g + 1, n) <= pos) g++;
-  while (g > 0 && tile_units_before(g, n) > pos) g--;
-  return (int)g;
-}
-
 // Splits units [pos, end) of one problem at test-tile boundaries.
 __device__ __forceinline__ void bm_units(BmSmem& sm, const GeomView& g, float k, float2* L, float2* Rm,
                                          long long pos, long long end, unsigned& uses) {
