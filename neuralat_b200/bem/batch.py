@@ -142,13 +142,13 @@ class BatchRunner:
             st = self._local.stream = torch.cuda.Stream()
         return st
 
-    def _solve_lane(self, tasks, pts, want_u, ready):
-        """Solve tasks [(A, rhs, solver, k, g)] one after another on this worker's stream."""
+    def _solve_lane(self, tasks, want_u, ready):
+        """Solve tasks [(A, rhs, solver, k, g, points)] one after another on this worker's stream."""
         st = self._stream()
         st.wait_event(ready)
         out = []
         with torch.cuda.stream(st):
-            for A, rhs, solver, k, g in tasks:
+            for A, rhs, solver, k, g, pts in tasks:
                 info = {}
                 u = gmres(A, rhs, rtol=self.rtol, restart=self.restart, max_iters=self.max_iters,
                           precision=self.precision, info=info)
@@ -162,10 +162,18 @@ class BatchRunner:
         ks_per_mesh: list of wavenumber lists; neumann_per_mesh: per mesh an
         (N,) or (N, m) array shared by its wavenumbers, or a list with one
         such array per wavenumber (a vibration mode per wavenumber); points
-        (P, 3).  Results are (N, m) / (P, m) per problem, m = 1 for (N,)."""
+        (P, 3) for every problem, or a list with one (P_i, 3) array per mesh.
+        Results are (N, m) / (P, m) per problem, m = 1 for (N,)."""
         dev = torch.device("cuda", torch.cuda.current_device())
-        pts = (points.to(device=dev, dtype=torch.float32) if torch.is_tensor(points)
-               else torch.as_tensor(np.asarray(points, np.float32), device=dev)).contiguous()
+
+        def dev_points(x):
+            return (x.to(device=dev, dtype=torch.float32) if torch.is_tensor(x)
+                    else torch.as_tensor(np.asarray(x, np.float32), device=dev)).contiguous()
+
+        per_mesh_points = isinstance(points, (list, tuple))
+        if per_mesh_points and len(points) != len(meshes):
+            raise ValueError(f"{len(points)} point sets for {len(meshes)} meshes")
+        pts = [dev_points(x) for x in points] if per_mesh_points else dev_points(points)
         solvers = [m if isinstance(m, BEM_Solver) else BEM_Solver(np.asarray(m[0], np.float32),
                                                                    np.asarray(m[1], np.int32)) for m in meshes]
 
@@ -221,9 +229,10 @@ class BatchRunner:
             del pairs
             ready = torch.cuda.Event()
             ready.record()
-            tasks = [(A, rhs, solvers[mi], k, neumann(mi, ki)) for (mi, ki), A, rhs, k in zip(wave, mats, rhss, ks)]
+            tasks = [(A, rhs, solvers[mi], k, neumann(mi, ki), pts[mi] if per_mesh_points else pts)
+                     for (mi, ki), A, rhs, k in zip(wave, mats, rhss, ks)]
             lanes = [list(range(w, len(wave), conc)) for w in range(conc)]  # round-robin over workers
-            futs = [self._pool.submit(self._solve_lane, [tasks[i] for i in lane], pts, return_dirichlet, ready)
+            futs = [self._pool.submit(self._solve_lane, [tasks[i] for i in lane], return_dirichlet, ready)
                     for lane in lanes if lane]
             out = [None] * len(wave)
             for lane, f in zip([ln for ln in lanes if ln], futs):
@@ -238,3 +247,20 @@ class BatchRunner:
                               "seconds": time.perf_counter() - t0})
             del mats, rhss, tasks
         return res
+
+
+# Runners (with their worker threads, streams and per-thread host buffers)
+# kept across calls, one per device and setting.
+_SHARED: dict = {}
+_SHARED_LOCK = threading.Lock()
+
+
+def shared_runner(**kw) -> BatchRunner:
+    """A process-wide BatchRunner for these settings on the current device,
+    created on first use and reused by later calls."""
+    key = (torch.cuda.current_device(),) + tuple(sorted(kw.items()))
+    with _SHARED_LOCK:
+        r = _SHARED.get(key)
+        if r is None:
+            r = _SHARED[key] = BatchRunner(**kw)
+        return r

@@ -17,6 +17,9 @@ from torch's unseeded CUDA generator), so a dataset is reproducible; the
 mapping from the uniform draws to positions and frequencies is the
 reference's.  The meshes and the solver settings are arguments (the
 reference reads them from a dataset directory that is not part of it).
+With ``batch_size`` the samples go through the batch runner in groups (the
+Burton-Miller matrices of a group assembled in one launch family, the solves
+on concurrent streams); the draws and the outputs are the same.
 """
 from __future__ import annotations
 
@@ -25,6 +28,7 @@ import math
 import numpy as np
 import torch
 
+from .batch import shared_runner
 from .solver import BEM_Solver
 
 SPEED_OF_SOUND = 343.2  # generate.py:99
@@ -52,13 +56,17 @@ def log_frequency(fraction: float, freq_min: float, freq_max: float) -> float:
 def generate_audio_samples(vib_vertices, vib_triangles, static_vertices, static_triangles, *, src_pos_min,
                            src_pos_max, bbox_center, bbox_r: float, r_max: float, freq_min: float = 100.0,
                            freq_max: float = 10000.0, trg_sample_num: int = 1000, src_sample_num: int = 1000,
-                           vib_neumann=None, seed: int = 0, device=None, solve_kw: dict | None = None):
+                           vib_neumann=None, seed: int = 0, device=None, solve_kw: dict | None = None,
+                           batch_size: int = 0, workers: int = 4):
     """Return {"x": (S, P, 5) float32, "y": (S, P, 1) float32} as the reference writes them.
 
     vib_neumann: (Nv,) normal velocity of the vibrating object (default 1
     everywhere; the reference zeroes part of its specific mesh); the static
     object is rigid (0).  solve_kw: options of ``neumann2dirichlet`` (the
-    linear solver's tolerance, precision, ...)."""
+    linear solver's tolerance, precision, ...).  batch_size > 0: solve the
+    samples in groups of that size through the batch runner (GMRES with the
+    relative stopping test sqrt(tol) of ``solve_linear_equation``; ``nsteps``,
+    ``precision`` and ``restart`` as there)."""
     device = torch.device("cuda") if device is None else torch.device(device)
     vv = np.asarray(vib_vertices, np.float32)
     vt = np.asarray(vib_triangles, np.int32)
@@ -75,6 +83,33 @@ def generate_audio_samples(vib_vertices, vib_triangles, static_vertices, static_
     x = torch.zeros(S, P, 5, dtype=torch.float32)
     y = torch.zeros(S, P, 1, dtype=torch.float32)
     static_d = torch.from_numpy(sv).to(device)
+    if batch_size and batch_size > 0:
+        kw = dict(solve_kw or {})
+        if kw.get("solver", "gmres") != "gmres":
+            raise ValueError("batched generation solves with GMRES")
+        tri_np = np.concatenate([vt, st + nvib], axis=0)
+        with torch.cuda.device(device):
+            runner = shared_runner(workers=workers, precision=kw.get("precision", "fp32"),
+                                   rtol=math.sqrt(max(float(kw.get("tol", 1e-10)), 0.0)),
+                                   restart=int(kw.get("restart", 200)), max_iters=int(kw.get("nsteps", 500)),
+                                   formulation="burton_miller")
+            for b0 in range(0, S, batch_size):
+                meshes, ks, pts = [], [], []
+                for i in range(b0, min(S, b0 + batch_size)):
+                    src_base = rng.random(3)
+                    displacement = src_base * (hi - lo) + lo
+                    base = rng.random((P, 3))
+                    freq_base = float(rng.random())
+                    meshes.append((np.concatenate([(vv + displacement).astype(np.float32), sv]), tri_np))
+                    pts.append(shell_points(base, bbox_center, bbox_r, r_max).astype(np.float32))
+                    ks.append([2.0 * math.pi * log_frequency(freq_base, freq_min, freq_max) / SPEED_OF_SOUND])
+                    x[i, :, :3] = torch.from_numpy(base.astype(np.float32))
+                    x[i, :, 3] = float(src_base[1])
+                    x[i, :, 4] = freq_base
+                res = runner.run(meshes, ks, [neumann] * len(meshes), pts)
+                for (mi, _), p in zip(res.index, res.pressure):
+                    y[b0 + mi, :, 0] = p[:, 0].abs().cpu()
+        return {"x": x, "y": y}
     for i in range(S):
         src_base = rng.random(3)
         displacement = src_base * (hi - lo) + lo

@@ -10,25 +10,10 @@ evaluation on the solver's fused kernel.
 """
 from __future__ import annotations
 
-import threading
-
 import torch
 
-from .batch import BatchRunner
+from .batch import shared_runner
 from .solver import BEM_Solver
-
-# Runners (with their worker threads, streams and per-thread host buffers)
-# kept across calls, one per device and setting.
-_RUNNERS: dict = {}
-_RUNNERS_LOCK = threading.Lock()
-
-
-def _runner(key, **kw) -> BatchRunner:
-    with _RUNNERS_LOCK:
-        r = _RUNNERS.get(key)
-        if r is None:
-            r = _RUNNERS[key] = BatchRunner(**kw)
-        return r
 
 
 def solve_modes(solver: BEM_Solver, ks, neumanns, points, *, precision: str = "fp32", rtol: float = 1e-5,
@@ -45,10 +30,10 @@ def solve_modes(solver: BEM_Solver, ks, neumanns, points, *, precision: str = "f
     if len(ks) == 0:
         raise ValueError("no modes")
     rows = [neumanns[i] for i in range(len(ks))]
-    key = (solver.device.index, workers, precision, rtol, restart, max_iters, memory_budget_bytes)
-    runner = _runner(key, memory_budget_bytes=memory_budget_bytes, workers=workers, precision=precision, rtol=rtol,
-                     restart=restart, formulation="burton_miller", max_iters=max_iters)
-    res = runner.run([solver], [ks], [rows], points, return_dirichlet=return_dirichlet)
+    with torch.cuda.device(solver.device):
+        runner = shared_runner(memory_budget_bytes=memory_budget_bytes, workers=workers, precision=precision,
+                               rtol=rtol, restart=restart, formulation="burton_miller", max_iters=max_iters)
+        res = runner.run([solver], [ks], [rows], points, return_dirichlet=return_dirichlet)
     order = sorted(range(len(res.index)), key=lambda i: res.index[i][1])
     p = torch.stack([res.pressure[i][:, 0] for i in order])
     if info is not None:
