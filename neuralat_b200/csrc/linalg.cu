@@ -640,8 +640,7 @@ struct ArnSmem {
   uint64_t full[kRingStages];     // bulk-copy completion of each ring stage
   uint64_t empty[kRingStages];    // consumer warps done with the stage
   double red[kArnWarps][2 * kChunkMax];
-  double dred[2][kArnConsumerWarps][2 * kChunkMax];  // dot-pass partials per consumer warp, double-buffered
-  double part1[2 * kMaxRestart];  // this CTA's partial h1 (re, im), read by the whole cluster
+  double part1[2 * kMaxRestart];  // this CTA's partial h1 (re, im), read by the whole cluster; atomics
   double part2[2 * kMaxRestart];  // partial h2
   double part3[2];                // partial |w''|^2
   double2 c1[kMaxRestart];        // cluster totals h1, h2
@@ -706,15 +705,14 @@ struct ArnStream {
 // part[2l + c] = sum over this CTA's unknowns of conj(V[l]) w.  Each thread
 // forms its pairs' products for every row of the chunk in FP32 (w rounded
 // to FP32 like the stored basis), a warp reduce-scatter sums the lanes, and
-// the consumer warps' partials are added in FP64 behind one named barrier
-// (consumers only; the partial arrays are double-buffered by chunk parity).
-__device__ __forceinline__ void consumer_barrier() {
-  asm volatile("bar.sync 1, %0;" ::"r"(kArnConsumers) : "memory");
-}
+// each warp adds its partials to `part` (zeroed at launch) with FP64
+// shared-memory atomics: no barrier between the consumer warps, which run
+// through the chunks independently (the cluster barrier after the pass
+// orders the atomics before the totals are read).
 
-__device__ __forceinline__ void arn_dots(const ArnStream& T, ArnSmem& S, int pass, const double2* __restrict__ wsl,
-                                         int npairs, double* part) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+__device__ __forceinline__ void arn_dots(const ArnStream& T, int pass, const double2* __restrict__ wsl, int npairs,
+                                         double* part) {
+  const int tid = threadIdx.x, lane = tid & 31;
   for (int c = 0; c < T.nch; c++) {
     const float2* rows = T.acquire(pass, c);
     const int l0 = c * T.chunk, nl = min(T.chunk, T.k + 1 - l0);
@@ -735,16 +733,8 @@ __device__ __forceinline__ void arn_dots(const ArnStream& T, ArnSmem& S, int pas
       }
     }
     const float t = warp_reduce_scatter<2 * kChunkMax>(v, lane);
-    double (*red)[2 * kChunkMax] = S.dred[c & 1];
-    if ((lane & 1) == 0) red[warp][lane >> 1] = (double)t;
-    consumer_barrier();  // all partials written; every consumer is done with the stage
-    T.release(pass, c);
-    if (tid < 2 * nl) {
-      double sum = 0.0;
-#pragma unroll
-      for (int w = 0; w < kArnConsumerWarps; w++) sum += red[w][tid];
-      part[2 * l0 + tid] = sum;
-    }
+    T.release(pass, c);  // this warp is done with the stage
+    if ((lane & 1) == 0 && (lane >> 1) < 2 * nl) atomicAdd(&part[2 * l0 + (lane >> 1)], (double)t);
   }
 }
 
@@ -936,6 +926,10 @@ __global__ void __launch_bounds__(kArnThreads, 1) gm_arnoldi_kernel(GmPtrs P, in
     }
     wsl[2 * p + 1] = w1;
   }
+  for (int t = tid; t < 2 * (k + 1); t += kArnThreads) {  // the dots passes accumulate into these
+    S.part1[t] = 0.0;
+    S.part2[t] = 0.0;
+  }
   __syncthreads();
 
   // passes: dots h1, update; with reorth also dots h2, update.  The producer
@@ -956,7 +950,7 @@ __global__ void __launch_bounds__(kArnThreads, 1) gm_arnoldi_kernel(GmPtrs P, in
       first = min(kRingStages, T.nch);
       __syncwarp();
     } else if (dots) {
-      arn_dots(T, S, pass, wsl, npairs, part);
+      arn_dots(T, pass, wsl, npairs, part);
     } else {
       arn_update(T, pass, coef, wsl, npairs);
     }
