@@ -131,14 +131,18 @@ size_t bem_batch_workspace_bytes(int nproblems);
 int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, float mass_coeff, float k_coeff,
                           void* workspace, size_t workspace_bytes, bem_stream_t stream);
 
-/* Fused Burton-Miller assembly at the <2,3> rules: both matrices of
- * BEM_Solver.neumann2dirichlet (src/bem/solver.py:118-126) in one pass,
- *   lhs_out <- bm_lhs_boundary_matrix_approx + 1/2 M
- *   rhs_out <- bm_rhs_boundary_matrix_approx - (i / (2k)) M
- * (both required, nv x nv complex64, overwritten; k != 0).  Replaces the
- * two bindings bind.cu:204-215 plus identity_matrix and the elementwise
- * combination the reference does in Python. */
-int bem_boundary_matrices_bm(const void* geom, float k, void* lhs_out, void* rhs_out, bem_stream_t stream);
+/* Fused Burton-Miller assembly: both matrices of a Burton-Miller system
+ * with coupling i/k in one pass, at quadrature `order`,
+ *   lhs_out <- bm_lhs_boundary_matrix[order] + 1/2 M
+ *   rhs_out <- bm_rhs_boundary_matrix[order] - (i / (2k)) M
+ * (both required, nv x nv complex64, overwritten; k != 0).  With
+ * BEM_ORDER_APPROX these are BEM_Solver.neumann2dirichlet's matrices
+ * (src/bem/solver.py:118-126: the bindings bind.cu:204-215, identity_matrix
+ * and the elementwise combination done in Python); with BEM_ORDER_EXACT they
+ * equal BEM_Solver.HBIE's (solver.py:106-116): 1/2 M - K + (i/k) W and
+ * -V - (i/k)(K' + 1/2 M). */
+int bem_boundary_matrices_bm(const void* geom, int order, float k, void* lhs_out, void* rhs_out,
+                             bem_stream_t stream);
 
 /* Batched fused Burton-Miller assembly (one persistent launch over all
  * problems' regular pairs, one launch per touching-pair type).  `problems`
@@ -151,8 +155,8 @@ typedef struct bem_bm_problem {
   void* lhs_out;
   void* rhs_out;
 } bem_bm_problem;
-int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproblems, void* workspace, size_t workspace_bytes,
-                          bem_stream_t stream);
+int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproblems, int order, void* workspace,
+                          size_t workspace_bytes, bem_stream_t stream);
 
 /* BEM_OK, or BEM_ERR_CUDA if a bounded wait of an assembly kernel (the
  * bulk copies of trial tiles) expired since the last call; clears the flag

@@ -138,8 +138,8 @@ def lib():
         "bem_set_tuning": ([i, i], i),
         "bem_assembly_status": ([vp], i),
         "bem_get_tuning": ([i], i),
-        "bem_boundary_matrices_bm": ([vp, f, vp, vp, vp], i),
-        "bem_batch_matrices_bm": ([P(BmProblem), i, vp, sz, vp], i),
+        "bem_boundary_matrices_bm": ([vp, i, f, vp, vp, vp], i),
+        "bem_batch_matrices_bm": ([P(BmProblem), i, i, vp, sz, vp], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)

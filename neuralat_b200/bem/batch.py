@@ -31,7 +31,7 @@ import numpy as np
 import torch
 
 from .. import _lib as L
-from .solver import BEM_Solver, _stream, _vp, cmatmul, gmres
+from .solver import BEM_Solver, _order, _stream, _vp, cmatmul, gmres
 
 
 @dataclass
@@ -67,9 +67,9 @@ def assemble_batch(solvers, ks, mass_coeff=0.5, k_coeff=-1.0, stream=None):
     return outs
 
 
-def assemble_batch_bm(solvers, ks, stream=None):
-    """Fused Burton-Miller (lhs, rhs) matrices of ``neumann2dirichlet`` for
-    each (solver, k) in one launch family."""
+def assemble_batch_bm(solvers, ks, stream=None, approx=True):
+    """Fused Burton-Miller (lhs, rhs) matrices of ``neumann2dirichlet`` (or,
+    with approx=False, of ``HBIE``) for each (solver, k) in one launch family."""
     assert len(solvers) == len(ks) and len(ks) > 0
     lib = L.lib()
     dev = solvers[0].device
@@ -87,7 +87,7 @@ def assemble_batch_bm(solvers, ks, stream=None):
     ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):
         st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else _stream(dev)
-        L.check(lib.bem_batch_matrices_bm(probs, n, _vp(ws), nbytes, st), "bem_batch_matrices_bm")
+        L.check(lib.bem_batch_matrices_bm(probs, n, _order(approx), _vp(ws), nbytes, st), "bem_batch_matrices_bm")
     return outs
 
 

@@ -167,6 +167,13 @@ def solve_linear_equation(A_func, b, x=None, nsteps=500, tol=1e-10, atol=1e-16, 
                  restart=restart, precision=precision, info=info)
 
 
+def _order(approx):
+    """Quadrature order of the reference's ``approx`` argument."""
+    if not approx:
+        return L.ORDER_EXACT
+    return L.ORDER_APPROX_1 if approx in ("1", 1) and approx is not True else L.ORDER_APPROX
+
+
 class BEM_Solver:
     """Mesh holder and operator facade (solver.py:69-147)."""
 
@@ -191,8 +198,7 @@ class BEM_Solver:
     def assemble_boundary_matrix(self, wavenumber, layer_type, approx=False):
         """Dense (N, N) complex64 matrix; ``approx`` as in the reference
         (False: <4,6>, True: <2,3>, "1" or 1 (beyond the reference's bool): <2,1>)."""
-        order = L.ORDER_EXACT if not approx else (L.ORDER_APPROX_1 if approx in ("1", 1) and approx is not True
-                                                   else L.ORDER_APPROX)
+        order = _order(approx)
         out = self._new_matrix()
         with torch.cuda.device(self.device):
             L.check(L.lib().bem_boundary_matrix(self.geometry.ptr, _LAYERS[layer_type], order, float(wavenumber),
@@ -209,13 +215,15 @@ class BEM_Solver:
                                                      _stream(self.device)), "bem_boundary_matrices_vk")
         return V, A
 
-    def assemble_bm(self, wavenumber):
-        """Fused Burton-Miller matrices of ``neumann2dirichlet`` at the <2,3>
-        rules: (bm_lhs + 1/2 I, bm_rhs - (i/(2k)) I), one pass."""
+    def assemble_bm(self, wavenumber, approx=True):
+        """Fused Burton-Miller matrices (bm_lhs + 1/2 I, bm_rhs - (i/(2k)) I),
+        one pass; ``approx`` as in ``assemble_boundary_matrix`` (True: the
+        <2,3> rules of ``neumann2dirichlet``; False: <4,6>, which is the
+        ``HBIE`` system)."""
         lhs, rhs = self._new_matrix(), self._new_matrix()
         with torch.cuda.device(self.device):
-            L.check(L.lib().bem_boundary_matrices_bm(self.geometry.ptr, float(wavenumber), _vp(lhs), _vp(rhs),
-                                                     _stream(self.device)), "bem_boundary_matrices_bm")
+            L.check(L.lib().bem_boundary_matrices_bm(self.geometry.ptr, _order(approx), float(wavenumber), _vp(lhs),
+                                                     _vp(rhs), _stream(self.device)), "bem_boundary_matrices_bm")
         return lhs, rhs
 
     def identity_matrix(self):
@@ -237,15 +245,12 @@ class BEM_Solver:
         return gmres(lhs, rhs, rtol=rtol, max_iters=max_iters, restart=restart, precision=precision, info=info)
 
     def HBIE(self, k, neumann, **kw):
-        """Hypersingular BIE (solver.py:106-116)."""
-        identity = self.identity_matrix()
-        slp = self.assemble_boundary_matrix(k, "single")
-        dlp = self.assemble_boundary_matrix(k, "double")
-        adlp = self.assemble_boundary_matrix(k, "adjointdouble")
-        hyp = self.assemble_boundary_matrix(k, "hypersingular")
-        beta = 1j / k
-        lhs = (0.5 * identity - dlp + beta * hyp).contiguous()
-        rhs = cmatmul((-slp - beta * (adlp + 0.5 * identity)).contiguous(), neumann.to(torch.complex64))
+        """Hypersingular BIE (solver.py:106-116): 1/2 I - K + (i/k) W and
+        -V - (i/k)(K' + 1/2 I) are the Burton-Miller pair at the <4,6>
+        rules, assembled in one fused pass."""
+        lhs, rhs_m = self.assemble_bm(k, approx=False)
+        rhs = cmatmul(rhs_m, neumann.to(torch.complex64))
+        del rhs_m
         return solve_linear_equation(lhs, rhs, **kw)
 
     def neumann2dirichlet(self, k, neumann, **kw):

@@ -3,7 +3,12 @@
 //   lhs = BM_LHS + 1/2 M,     rhs = BM_RHS - (i / (2k)) M,
 // at the <2,3> rules of its "_approx" bindings (bind.cu:204-215): the 3-point
 // degree-2 triangle rule for regular pairs, 2-point Gauss-Legendre
-// Sauter-Schwab quadrature for touching pairs.
+// Sauter-Schwab quadrature for touching pairs.  At the exact <4,6> rules the
+// same pair is the reference's HBIE system (solver.py:106-116):
+//   1/2 M - K + (i/k) W = BM_LHS + 1/2 M   (W = curl term - k^2 n.n G),
+//   -V - (i/k)(K' + 1/2 M) = BM_RHS - (i/(2k)) M,
+// so the kernels are templated on the rule (TN points per triangle, LN
+// Gauss-Legendre points per Sauter-Schwab axis).
 //
 // Kernels (potential.h:42-65, integrand.h:94-101,216-221,314-322), x on the
 // test triangle i, y on the trial triangle j, G = e^{ikr}/r and
@@ -49,15 +54,26 @@ constexpr int kBmTest = kTile;               // test triangles per CTA (one tile
 constexpr int kBmCorners = 3 * kBmTest;      // 48
 constexpr int kBmStride = kTileCorners + 1;  // 49 float2: conflict-free column writes
 
-// 3-point rule: C(q, b) = w_q phi_b(q) = 1/3 * (q == b ? 2/3 : 1/6)
-__host__ __device__ constexpr float bm_c(int q, int b) { return q == b ? 2.0f / 9.0f : 1.0f / 18.0f; }
+// C(q, b) = w_q phi_b(q): centroid rule 1/3; 3-point rule 1/3 * (q == b ?
+// 2/3 : 1/6); 6-point rule as the V/K assembly.
+template <int TN>
+__host__ __device__ constexpr float bm_c(int q, int b) {
+  return TN == 1 ? 1.0f / 3.0f
+                 : (TN == 3 ? (q == b ? 2.0f / 9.0f : 1.0f / 18.0f) : (float)(tri6_w(q) * tri6_phi(q, b)));
+}
+
+// Coordinate c of the rule's points of a triangle (records in sorted order).
+template <int TN>
+__device__ __forceinline__ float bm_point(const TriRec& r, const BmRec& b, int c) {
+  return TN == 3 ? b.qp[c] : (TN == 6 ? r.qp[c] : r.c[c]);
+}
 
 struct BmSmem {
   float2 slotL[kBmCorners][kBmStride];   // lhs_ij[a][b] at [3 tl + a][3 tt + b]
   float2 slotLT[kBmCorners][kBmStride];  // lhs_ji[b][a], same indexing
   float2 slotR[kBmCorners][kBmStride];
   float2 slotRT[kBmCorners][kBmStride];
-  float xs[9][kBmTest];                  // test quadrature points [coordinate][tl]
+  float xs[18][kBmTest];                 // test quadrature points [coordinate][tl]
   float xc[9][kBmTest];                  // test curls [3 a + d][tl]
   TriRec trial[2][kTile];                // trial tile, double-buffered
   BmRec trialB[2][kTile];
@@ -86,10 +102,11 @@ __device__ __forceinline__ void bm_fetch_tile(BmSmem& sm, const GeomView& g, int
   bulk_load(&sm.tileJ[b], &g.tiles[jt], (uint32_t)sizeof(TileRec), &sm.tile_full[b]);
 }
 
-// S, T, U blocks of one unordered pair under the 3x3 point rule (test
+// S, T, U blocks of one unordered pair under the TN x TN point rule (test
 // triangle tl, points in xs; trial points yq, dq[q] = n_i . (c_i - y_q)).
-__device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl, const float (&yq)[9],
-                                              const float (&dq)[3], float njx, float njy, float njz, float cjx,
+template <int TN>
+__device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl, const float (&yq)[3 * TN],
+                                              const float (&dq)[TN], float njx, float njy, float njz, float cjx,
                                               float cjy, float cjz, float k, float2 (&aS)[9], float2 (&aT)[9],
                                               float2 (&aU)[9]) {
 #pragma unroll
@@ -99,7 +116,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
     aU[e] = make_float2(0.f, 0.f);
   }
 #pragma unroll
-  for (int p = 0; p < 3; p++) {
+  for (int p = 0; p < TN; p++) {
     const float px = xs[3 * p][tl], py = xs[3 * p + 1][tl], pz = xs[3 * p + 2][tl];
     const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);  // (y - x).n_j on plane j
     float2 tS[3], tT[3], tU[3];
@@ -110,7 +127,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
       tU[b] = make_float2(0.f, 0.f);
     }
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
+    for (int q = 0; q < TN; q++) {
       const float dx = yq[3 * q] - px, dy = yq[3 * q + 1] - py, dz = yq[3 * q + 2] - pz;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const float rinv = fminf(rsqrtf(r2), 1.0f / kEps);
@@ -124,7 +141,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
       const float ur = dq[q] * hr, ui = dq[q] * hi;
 #pragma unroll
       for (int b = 0; b < 3; b++) {
-        const float w = bm_c(q, b);
+        const float w = bm_c<TN>(q, b);
         tS[b].x = fmaf(w, gr, tS[b].x);
         tS[b].y = fmaf(w, gi, tS[b].y);
         tT[b].x = fmaf(w, hr, tT[b].x);
@@ -135,7 +152,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      const float wa = bm_c(p, a);
+      const float wa = bm_c<TN>(p, a);
       const float wt = wa * dn;
 #pragma unroll
       for (int b = 0; b < 3; b++) {
@@ -153,6 +170,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
 // One work item: test tile grp against trial tiles [jt_begin, jt_end), all
 // at or after grp.  `uses` counts the trial tiles this CTA has processed
 // (buffer = uses & 1, mbarrier parity = (uses >> 1) & 1).
+template <int TN>
 __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, float2* __restrict__ L,
                                         float2* __restrict__ Rm, int grp, int jt_begin, int jt_end,
                                         unsigned& uses) {
@@ -171,13 +189,13 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
   __syncthreads();  // the previous item is done with tileI, xs, xc and both trial buffers
   if (tid == 0) bm_fetch_tile(sm, g, jt_begin, uses & 1);
   bm_copy_words(&sm.tileI, &g.tiles[grp], sizeof(TileRec), tid);
-  for (int e = tid; e < 18 * kBmTest; e += kBmThreads) {
+  for (int e = tid; e < (3 * TN + 9) * kBmTest; e += kBmThreads) {
     const int c = e / kBmTest, l = e - c * kBmTest;
     const int t = min(grp * kBmTest + l, nt - 1);
-    if (c < 9)
-      sm.xs[c][l] = g.bm[t].qp[c];
+    if (c < 3 * TN)
+      sm.xs[c][l] = bm_point<TN>(g.rec[t], g.bm[t], c);
     else
-      sm.xc[c - 9][l] = g.bm[t].curl[c - 9];
+      sm.xc[c - 3 * TN][l] = g.bm[t].curl[c - 3 * TN];
   }
 
   for (int jt = jt_begin; jt < jt_end; jt++, uses++) {
@@ -206,15 +224,15 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
     if (tt < ntriJ && any) {
       const TriRec& rj = sm.trial[bf][tt];
       const BmRec& bj = sm.trialB[bf][tt];
-      float yq[9];
+      float yq[3 * TN];
 #pragma unroll
-      for (int e = 0; e < 9; e++) yq[e] = bj.qp[e];
-      float dq[3];
+      for (int e = 0; e < 3 * TN; e++) yq[e] = bm_point<TN>(rj, bj, e);
+      float dq[TN];
 #pragma unroll
-      for (int q = 0; q < 3; q++)
+      for (int q = 0; q < TN; q++)
         dq[q] = nix * (cix - yq[3 * q]) + niy * (ciy - yq[3 * q + 1]) + niz * (ciz - yq[3 * q + 2]);
       float2 aS[9], aT[9], aU[9];
-      bm_pair_block(sm.xs, tl, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aS, aT, aU);
+      bm_pair_block<TN>(sm.xs, tl, yq, dq, rj.n[0], rj.n[1], rj.n[2], rj.c[0], rj.c[1], rj.c[2], k, aS, aT, aU);
       const float sc = aa * kInv4Pi;
       float2 s9 = make_float2(0.f, 0.f);
 #pragma unroll
@@ -290,6 +308,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
 }
 
 // Splits units [pos, end) of one problem at test-tile boundaries.
+template <int TN>
 __device__ __forceinline__ void bm_units(BmSmem& sm, const GeomView& g, float k, float2* L, float2* Rm,
                                          long long pos, long long end, unsigned& uses) {
   while (pos < end) {  // uniform over the block
@@ -298,7 +317,7 @@ __device__ __forceinline__ void bm_units(BmSmem& sm, const GeomView& g, float k,
     const long long gend = base + (g.ntiles - grp);
     const long long stop = end < gend ? end : gend;
     const int jt0 = grp + (int)(pos - base);
-    bm_item(sm, g, k, L, Rm, grp, jt0, jt0 + (int)(stop - pos), uses);
+    bm_item<TN>(sm, g, k, L, Rm, grp, jt0, jt0 + (int)(stop - pos), uses);
     pos = stop;
   }
 }
@@ -343,6 +362,7 @@ __device__ __forceinline__ void bm_init_barriers(BmSmem& sm) {
 
 // Regular pairs of one problem: equal work items dealt round-robin to a
 // persistent grid.
+template <int TN>
 __global__ void __launch_bounds__(kBmThreads, 2)
     regular_bm_kernel(const __grid_constant__ BmProblem P, int n_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -352,11 +372,12 @@ __global__ void __launch_bounds__(kBmThreads, 2)
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const long long pos = (long long)item * P.chunk;
     const long long end = pos + P.chunk < P.n_units ? pos + P.chunk : P.n_units;
-    bm_units(sm, P.g, P.k, P.L, P.R, pos, end, uses);
+    bm_units<TN>(sm, P.g, P.k, P.L, P.R, pos, end, uses);
   }
 }
 
 // Regular pairs of a batch: CTAs drain one queue of work items.
+template <int TN>
 __global__ void __launch_bounds__(kBmThreads, 2)
     regular_bm_batch_kernel(BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -375,7 +396,7 @@ __global__ void __launch_bounds__(kBmThreads, 2)
     const BmProblem& P = probs[bm_find(probs, np, item, -1)];
     const long long pos = (item - P.item_begin) * P.chunk;
     const long long end = pos + P.chunk < P.n_units ? pos + P.chunk : P.n_units;
-    bm_units(sm, P.g, P.k, P.L, P.R, pos, end, uses);
+    bm_units<TN>(sm, P.g, P.k, P.L, P.R, pos, end, uses);
   }
 }
 
@@ -408,9 +429,8 @@ __device__ __forceinline__ void bm_eval(R dx, R dy, R dz, const R (&ni)[3], cons
 
 // One touching pair (index `local` of its type), one warp; the coincident
 // pass also adds 1/2 M to lhs and -(i/(2k)) M to rhs.
-template <typename R, int NCOMMON>
+template <typename R, int NCOMMON, int LN>
 __device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local) {
-  constexpr int LN = 2;
   const int lane = threadIdx.x & 31;
   const GeomView& g = P.g;
   int ti = local, tj = local;
@@ -528,21 +548,21 @@ __device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local) 
   }
 }
 
-template <typename R, int NCOMMON>
+template <typename R, int NCOMMON, int LN>
 __global__ void __launch_bounds__(128) singular_bm_kernel(const __grid_constant__ BmProblem P, int npairs) {
   const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (pair >= npairs) return;
-  singular_bm_pair<R, NCOMMON>(P, pair);
+  singular_bm_pair<R, NCOMMON, LN>(P, pair);
 }
 
-template <typename R, int NCOMMON>
+template <typename R, int NCOMMON, int LN>
 __global__ void __launch_bounds__(128)
     singular_bm_batch_kernel(const BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
   constexpr int which = NCOMMON == 3 ? 0 : (NCOMMON == 2 ? 1 : 2);
   const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (pair >= hdr->total_pairs[which]) return;
   const BmProblem& P = probs[bm_find(probs, hdr->nproblems, pair, which)];
-  singular_bm_pair<R, NCOMMON>(P, (int)(pair - P.pair_begin[which]));
+  singular_bm_pair<R, NCOMMON, LN>(P, (int)(pair - P.pair_begin[which]));
 }
 
 inline size_t al256(size_t x) { return (x + 255) / 256 * 256; }
@@ -599,14 +619,74 @@ size_t bm_workspace_bytes(int np) {
   return al256(sizeof(BmHeader)) + al256(sizeof(BmProblem) * (size_t)(np > 0 ? np : 1));
 }
 
-// lhs = BM_LHS + 1/2 M and rhs = BM_RHS - (i/(2k)) M of one problem (both
-// nv x nv complex64, overwritten).
-int assemble_bm(const GeomView& g, float k, float2* L, float2* R, cudaStream_t s) {
-  int rc = bm_check(k, L, R);
-  if (rc) return rc;
+namespace {
+
+template <int TN>
+int bm_single_grid(long long* grid) {
   static std::atomic<bool> attr{false};
+  return bm_grid(regular_bm_kernel<TN>, attr, grid);
+}
+
+template <int TN>
+int bm_batch_grid(long long* grid) {
+  static std::atomic<bool> attr{false};
+  return bm_grid(regular_bm_batch_kernel<TN>, attr, grid);
+}
+
+int bm_rule(int order, int* tn) {
+  if (order == BEM_ORDER_EXACT) *tn = 6;
+  else if (order == BEM_ORDER_APPROX) *tn = 3;
+  else if (order == BEM_ORDER_APPROX_1) *tn = 1;
+  else return BEM_ERR_INVALID_ARGUMENT;
+  return BEM_OK;
+}
+
+template <int TN, int LN>
+void bm_single_launch(const BmProblem& P, long long grid, long long items, cudaStream_t s) {
+  const GeomView& g = P.g;
+  if (items > 0)
+    (regular_bm_kernel<TN><<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(P, (int)items),
+     count_launch());
+  const int wpb = 4;
+  (singular_bm_kernel<double, 3, LN><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.nt), count_launch());
+  if (g.n_edge)
+    (singular_bm_kernel<float, 2, LN><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_edge),
+     count_launch());
+  if (g.n_vert)
+    (singular_bm_kernel<float, 1, LN><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_vert),
+     count_launch());
+}
+
+template <int TN, int LN>
+void bm_batch_launch(BmHeader* dh, BmProblem* dp, long long grid, long long items, const long long* pairs,
+                     cudaStream_t s) {
+  if (items > 0)
+    (regular_bm_batch_kernel<TN><<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(dh, dp),
+     count_launch());
+  const int wpb = 4;
+  if (pairs[0])
+    (singular_bm_batch_kernel<double, 3, LN><<<(unsigned)((pairs[0] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+     count_launch());
+  if (pairs[1])
+    (singular_bm_batch_kernel<float, 2, LN><<<(unsigned)((pairs[1] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+     count_launch());
+  if (pairs[2])
+    (singular_bm_batch_kernel<float, 1, LN><<<(unsigned)((pairs[2] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+     count_launch());
+}
+
+}  // namespace
+
+// lhs = BM_LHS + 1/2 M and rhs = BM_RHS - (i/(2k)) M of one problem (both
+// nv x nv complex64, overwritten) at `order` (the reference's <2,3> for
+// neumann2dirichlet; <4,6> gives its HBIE system).
+int assemble_bm(const GeomView& g, int order, float k, float2* L, float2* R, cudaStream_t s) {
+  int rc = bm_check(k, L, R), tn = 0;
+  if (rc) return rc;
+  if ((rc = bm_rule(order, &tn))) return rc;
   long long grid = 0;
-  if ((rc = bm_grid(regular_bm_kernel, attr, &grid))) return rc;
+  rc = tn == 6 ? bm_single_grid<6>(&grid) : (tn == 3 ? bm_single_grid<3>(&grid) : bm_single_grid<1>(&grid));
+  if (rc) return rc;
   BEM_CUDA_TRY(cudaMemsetAsync(L, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
   BEM_CUDA_TRY(cudaMemsetAsync(R, 0, sizeof(float2) * (size_t)g.nv * g.nv, s));
   BmProblem P;
@@ -619,31 +699,29 @@ int assemble_bm(const GeomView& g, float k, float2* L, float2* R, cudaStream_t s
   P.L = L;
   P.R = R;
   const long long items = (P.n_units + P.chunk - 1) / P.chunk;
-  if (items > 0)
-    (regular_bm_kernel<<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(P, (int)items),
-     count_launch());
-  const int wpb = 4;
-  (singular_bm_kernel<double, 3><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.nt), count_launch());
-  if (g.n_edge)
-    (singular_bm_kernel<float, 2><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_edge), count_launch());
-  if (g.n_vert)
-    (singular_bm_kernel<float, 1><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_vert), count_launch());
+  if (tn == 6)
+    bm_single_launch<6, 4>(P, grid, items, s);
+  else if (tn == 3)
+    bm_single_launch<3, 2>(P, grid, items, s);
+  else
+    bm_single_launch<1, 2>(P, grid, items, s);
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }
 
 // The same for many problems: one queue-driven launch over every problem's
 // regular pairs, one launch per touching-pair type.
-int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls, float2* const* Rs, int np,
+int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls, float2* const* Rs, int np, int order,
                       void* ws, size_t ws_bytes, cudaStream_t s) {
   if (np <= 0 || !views || !ks || !Ls || !Rs) return BEM_ERR_INVALID_ARGUMENT;
   if (!ws || ws_bytes < bm_workspace_bytes(np)) return BEM_ERR_WORKSPACE;
-  int rc;
+  int rc, tn = 0;
   for (int p = 0; p < np; p++)
     if ((rc = bm_check(ks[p], Ls[p], Rs[p]))) return rc;
-  static std::atomic<bool> attr{false};
+  if ((rc = bm_rule(order, &tn))) return rc;
   long long grid = 0;
-  if ((rc = bm_grid(regular_bm_batch_kernel, attr, &grid))) return rc;
+  rc = tn == 6 ? bm_batch_grid<6>(&grid) : (tn == 3 ? bm_batch_grid<3>(&grid) : bm_batch_grid<1>(&grid));
+  if (rc) return rc;
 
   const size_t hbytes = al256(sizeof(BmHeader)), pbytes = sizeof(BmProblem) * (size_t)np;
   BmStage& st = t_bm_stage;
@@ -693,19 +771,12 @@ int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls,
   BmProblem* dp = (BmProblem*)((char*)ws + hbytes);
   BEM_CUDA_TRY(cudaMemcpyAsync(ws, st.buf, hbytes + pbytes, cudaMemcpyHostToDevice, s));
   BEM_CUDA_TRY(cudaEventRecord(st.ev, s));
-  if (items > 0)
-    (regular_bm_batch_kernel<<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(dh, dp),
-     count_launch());
-  const int wpb = 4;
-  if (pairs[0])
-    (singular_bm_batch_kernel<double, 3><<<(unsigned)((pairs[0] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
-     count_launch());
-  if (pairs[1])
-    (singular_bm_batch_kernel<float, 2><<<(unsigned)((pairs[1] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
-     count_launch());
-  if (pairs[2])
-    (singular_bm_batch_kernel<float, 1><<<(unsigned)((pairs[2] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
-     count_launch());
+  if (tn == 6)
+    bm_batch_launch<6, 4>(dh, dp, grid, items, pairs, s);
+  else if (tn == 3)
+    bm_batch_launch<3, 2>(dh, dp, grid, items, pairs, s);
+  else
+    bm_batch_launch<1, 2>(dh, dp, grid, items, pairs, s);
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
 }

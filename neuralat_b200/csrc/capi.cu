@@ -18,9 +18,9 @@ int get_tuning(int key);
 size_t batch_workspace_bytes(int np);
 int assemble_vk_batch(const GeomView* views, const float* ks, float2* const* Vs, float2* const* Ks, int np,
                       float mass_coeff, float k_coeff, void* ws, size_t ws_bytes, cudaStream_t s);
-int assemble_bm(const GeomView& g, float k, float2* L, float2* R, cudaStream_t s);
+int assemble_bm(const GeomView& g, int order, float k, float2* L, float2* R, cudaStream_t s);
 size_t bm_workspace_bytes(int np);
-int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls, float2* const* Rs, int np,
+int assemble_bm_batch(const GeomView* views, const float* ks, float2* const* Ls, float2* const* Rs, int np, int order,
                       void* ws, size_t ws_bytes, cudaStream_t s);
 int bm_status(int* err_host, cudaStream_t s);
 }  // namespace bemb
@@ -95,15 +95,15 @@ extern "C" size_t bem_batch_workspace_bytes(int nproblems) {
   return a > b ? a : b;
 }
 
-extern "C" int bem_boundary_matrices_bm(const void* geom, float k, void* lhs_out, void* rhs_out,
+extern "C" int bem_boundary_matrices_bm(const void* geom, int order, float k, void* lhs_out, void* rhs_out,
                                         bem_stream_t stream) {
   GeomView g;
   int rc = geom_view(geom, &g, nullptr);
   if (rc) return rc;
-  return assemble_bm(g, k, (float2*)lhs_out, (float2*)rhs_out, (cudaStream_t)stream);
+  return assemble_bm(g, order, k, (float2*)lhs_out, (float2*)rhs_out, (cudaStream_t)stream);
 }
 
-extern "C" int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproblems, void* workspace,
+extern "C" int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproblems, int order, void* workspace,
                                      size_t workspace_bytes, bem_stream_t stream) {
   if (!problems || nproblems <= 0) return BEM_ERR_INVALID_ARGUMENT;
   std::vector<GeomView> views(nproblems);
@@ -116,8 +116,8 @@ extern "C" int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproble
     Ls[p] = (float2*)problems[p].lhs_out;
     Rs[p] = (float2*)problems[p].rhs_out;
   }
-  return assemble_bm_batch(views.data(), ks.data(), Ls.data(), Rs.data(), nproblems, workspace, workspace_bytes,
-                           (cudaStream_t)stream);
+  return assemble_bm_batch(views.data(), ks.data(), Ls.data(), Rs.data(), nproblems, order, workspace,
+                           workspace_bytes, (cudaStream_t)stream);
 }
 
 extern "C" int bem_batch_matrices_vk(const bem_batch_problem* problems, int nproblems, float mass_coeff, float k_coeff,

@@ -50,6 +50,41 @@ def test_fused_bm_matches_reference_kernels(path):
         assert relfro(rhs, z[f"k{ki}_bm_rhs_approx"] - (0.5j / k) * I) <= 3e-5, k
 
 
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(f) for f in GOLDEN])
+def test_fused_exact_order_is_the_reference_hbie_system(path):
+    """<4,6>: lhs = 1/2 I - K + (i/k) W, rhs = -V - (i/k)(K' + 1/2 I) from the
+    reference's own kernels (solver.py:106-116); <2,1> against its bm_*_approx_1."""
+    z = dict(np.load(path))
+    s = BEM_Solver(z["vertices"], z["triangles"])
+    I = z["identity"]
+    for ki, k in enumerate(z["ks"]):
+        beta = 1j / k
+        lhs, rhs = s.assemble_bm(float(k), approx=False)
+        ref_l = 0.5 * I - z[f"k{ki}_double"] + beta * z[f"k{ki}_hypersingular"]
+        ref_r = -z[f"k{ki}_single"] - beta * (z[f"k{ki}_adjointdouble"] + 0.5 * I)
+        assert relfro(lhs, ref_l) <= 3e-5, k
+        assert relfro(rhs, ref_r) <= 3e-5, k
+        lhs1, rhs1 = s.assemble_bm(float(k), approx="1")
+        assert relfro(lhs1, z[f"k{ki}_bm_lhs_approx_1"] + 0.5 * I) <= 3e-5, k
+        assert relfro(rhs1, z[f"k{ki}_bm_rhs_approx_1"] - (0.5j / k) * I) <= 3e-5, k
+
+
+@pytest.mark.parametrize("k", [18.3, -100.6])
+def test_fused_exact_order_matches_oracle(k):
+    v, t = ellipsoid(2)
+    s = BEM_Solver(v, t)
+    vd = v.astype(np.float64)
+    I = O.identity_matrix(vd, t)
+    beta = 1j / k
+    lhs, rhs = s.assemble_bm(k, approx=False)
+    ref_l = 0.5 * I - O.boundary_matrix("double", vd, t, k) + beta * O.boundary_matrix("hypersingular", vd, t, k)
+    ref_r = -O.boundary_matrix("single", vd, t, k) - beta * (O.boundary_matrix("adjointdouble", vd, t, k) + 0.5 * I)
+    assert relfro(lhs, ref_l) <= 1e-5
+    assert relfro(rhs, ref_r) <= 1e-5
+    (lb, rb), = assemble_batch_bm([s], [k], approx=False)
+    assert relfro(lb, lhs) <= 1e-6 and relfro(rb, rhs) <= 1e-6
+
+
 @pytest.mark.parametrize("k", [18.3, 73.27, -100.6])
 def test_fused_bm_matches_oracle_and_operator_path(k):
     v, t = ellipsoid(2)
