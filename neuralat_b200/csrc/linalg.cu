@@ -79,7 +79,7 @@ struct MMRows {
 // MODE 1: Y[i, s] = B[i, s] - sum_j A[i, j] X[j, s], norm2[s] += |Y[i,s]|^2
 // X, Y, B are (n, ldx/ldy) row-major; MR right-hand sides per pass.
 template <typename T, int MR, int MODE>
-__global__ void __launch_bounds__(kMMThreads)
+__global__ void __launch_bounds__(kMMThreads, 2)
     cmatmul_kernel(const float2* __restrict__ A, int n, const typename C2<T>::type* __restrict__ X, int ldx,
                    int m, typename C2<T>::type* __restrict__ Y, int ldy, const float2* __restrict__ B, int ldb,
                    double* __restrict__ norm2, const int* __restrict__ active) {
