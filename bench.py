@@ -146,6 +146,16 @@ def regular_pair_evals(triangles) -> float:
     return 36.0 * (nt * nt - touching)
 
 
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json beside
+    this file), else the earlier pool measurement."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return {"gbs": float(json.load(f)["hbm_gbs"]), "source": "measured copy bandwidth (MEASURED_PEAKS.json)"}
+    except (OSError, ValueError, KeyError):
+        return {"gbs": 6650.0, "source": "fallback 6.65 TB/s (earlier measurement on this pool)"}
+
+
 def fp32_peak_tflops(sm_max_mhz=None):
     import torch
 
@@ -401,6 +411,38 @@ def run_ours(args):
                           "evaluates each unordered pair once); peak = nominal FP32 (SMs x 128 FMA x 2 x max SM "
                           "clock; no measured FP32 peak available); traffic scaled from an s4 ncu capture"}
 
+    # ---- roofline of the solve's dominant kernel (tensor-core matvec) ----------
+    roofline_matvec = None
+    if args.precision in ("fp16x3", "bf16x3", "bf16"):
+        prec = {"fp16x3": L.PREC_FP16X3, "bf16x3": L.PREC_BF16X3, "bf16": L.PREC_BF16}[args.precision]
+        s = BEM_Solver(v_d, t_d)
+        _, A = s.assemble_vk(k, single=False)
+        n, m = A.shape[0], g.shape[1]
+        nbytes = int(lib.bem_tc_operator_bytes(n, m, prec))
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        L.check(lib.bem_tc_operator_prepare(_vp(A), n, prec, _vp(ws), nbytes, _stream(dev)))
+        del A
+        X = torch.randn(n, m, dtype=torch.complex64, device=dev)
+        Y = torch.empty_like(X)
+        for _ in range(3):
+            L.check(lib.bem_tc_matmul(_vp(ws), nbytes, n, prec, _vp(X), m, _vp(Y), _stream(dev)))
+        nrep = 20
+        m0 = ev()
+        for _ in range(nrep):  # the 16-bit planes (839 MB at s5) are far larger than L2
+            L.check(lib.bem_tc_matmul(_vp(ws), nbytes, n, prec, _vp(X), m, _vp(Y), _stream(dev)))
+        m1 = ev()
+        torch.cuda.synchronize()
+        L.check(lib.bem_tc_status(_vp(ws), _stream(dev)))
+        us = m0.elapsed_time(m1) / nrep * 1e3
+        planes = 2 if args.precision != "bf16" else 1
+        alg = planes * 2 * n * (2 * n)  # 16-bit planes of the (n x 2n) real form of A
+        hbm = measured_hbm_gbs()
+        roofline_matvec = {"bound": "hbm", "achieved": alg / (us * 1e-6) / 1e9, "peak": hbm["gbs"], "unit": "GB/s",
+                           "frac": alg / (us * 1e-6) / 1e9 / hbm["gbs"], "traffic": None, "us_per_launch": us,
+                           "kernel": f"tc_gemm_kernel ({args.precision}, {m} RHS), {alg / 1e6:.0f} MB of operator "
+                                     f"planes per launch, timed alone over {nrep} launches; peak = {hbm['source']}"}
+        del ws
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(v, t, k, g, pts)
@@ -415,7 +457,7 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": args.precision, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (two 839 MB matrices per step)"},
-            "roofline": roofline, "cpu_baseline": cpu,
+            "roofline": roofline, "roofline_matvec": roofline_matvec, "cpu_baseline": cpu,
             "e2e": {"value": e2e_ms / 1e3 / world, "unit": "s/problem", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(l1 - l0),
