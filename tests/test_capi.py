@@ -86,3 +86,15 @@ def test_tuning_knobs_and_batch_sizes():
     assert lib.bem_batch_matrices_vk(None, 1, 0.5, -1.0, None, 0, None) == L.BEM_ERR_INVALID_ARGUMENT
     probs = (L.BatchProblem * 1)()
     assert lib.bem_batch_matrices_vk(probs, 0, 0.5, -1.0, None, 0, None) == L.BEM_ERR_INVALID_ARGUMENT
+
+
+def test_burton_miller_entry_points_reject_bad_arguments_on_host():
+    lib = L.lib()
+    # no geometry: rejected before any device work, whatever the order
+    for order in (L.ORDER_EXACT, L.ORDER_APPROX, L.ORDER_APPROX_1):
+        assert lib.bem_boundary_matrices_bm(None, order, 10.0, None, None, None) == L.BEM_ERR_WORKSPACE
+    assert lib.bem_batch_matrices_bm(None, 1, L.ORDER_APPROX, None, 0, None) == L.BEM_ERR_INVALID_ARGUMENT
+    probs = (L.BmProblem * 1)()
+    assert lib.bem_batch_matrices_bm(probs, 0, L.ORDER_APPROX, None, 0, None) == L.BEM_ERR_INVALID_ARGUMENT
+    # the batch workspace covers both batched assemblies
+    assert lib.bem_batch_workspace_bytes(64) >= 64 * ctypes.sizeof(L.BmProblem)
