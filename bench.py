@@ -17,6 +17,15 @@ the path has no data exchange); times are the max over ranks.
 ``--impl reference`` times the FP64 CPU restatement of the reference's
 algorithm (the reference has no CPU implementation of its own) on a bounded
 sample of the same workload.
+
+Besides the metric line: ``roofline`` (fused assembly, FP32 issue) and
+``roofline_matvec`` (tensor-core matvec timed alone, HBM).  Other workloads,
+one JSON line each: ``--batch-case`` (meshes x wavenumbers through the batch
+runner), ``--modal-case`` (many vibration modes of one object, Burton-Miller),
+``--grad-case`` (forward + adjoint backward), ``--large-case`` (s6, 64 RHS),
+``--kernel-case assemble|assemble_bm|solve|eval`` (one stage on a smaller
+mesh, for profiler captures), ``--validate`` (listener error against the FP64
+oracle).
 """
 from __future__ import annotations
 
