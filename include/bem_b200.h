@@ -171,8 +171,10 @@ enum {
   BEM_TUNE_TC_PROMOTE = 3,           /* tensor-core matvec: K blocks (64 reals) accumulated in tensor
                                         memory before the partial sum leaves it (0: automatic) */
   BEM_TUNE_GMRES_REORTH = 4,         /* Arnoldi Gram-Schmidt passes: 0 automatic (one), 1 one, 2 two */
-  BEM_TUNE_ARNOLDI_CLUSTER = 5       /* largest thread-block cluster (<= 16 CTAs) per Krylov column in
+  BEM_TUNE_ARNOLDI_CLUSTER = 5,      /* largest thread-block cluster (<= 16 CTAs) per Krylov column in
                                         the Arnoldi kernel (0: automatic) */
+  BEM_TUNE_ARNOLDI_MODE = 6          /* Arnoldi step: 0 automatic, 1 one cluster kernel per step,
+                                        2 three streamed kernels over all SMs (large n) */
 };
 int bem_set_tuning(int key, int value);
 int bem_get_tuning(int key);

@@ -52,6 +52,7 @@ class BEMError(RuntimeError):
 
 
 TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE, TUNE_GMRES_REORTH, TUNE_ARNOLDI_CLUSTER = 1, 2, 3, 4, 5
+TUNE_ARNOLDI_MODE = 6
 
 
 class BatchProblem(ctypes.Structure):

@@ -39,6 +39,7 @@ int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr);
 extern int g_tc_promote;    // tensor-core matvec accumulator segment (tc_matvec.cu)
 extern int g_gmres_reorth;  // Gram-Schmidt passes of the Arnoldi step (linalg.cu)
 extern int g_arn_max_cluster;  // largest Arnoldi cluster size (linalg.cu)
+extern int g_arn_mode;         // Arnoldi step variant (linalg.cu)
 
 namespace {
 extern int g_tune_chunk;
@@ -1028,6 +1029,10 @@ int set_tuning(int key, int value) {
       if (value > 16) return BEM_ERR_INVALID_ARGUMENT;
       g_arn_max_cluster = value;
       return BEM_OK;
+    case BEM_TUNE_ARNOLDI_MODE:
+      if (value > 2) return BEM_ERR_INVALID_ARGUMENT;
+      g_arn_mode = value;
+      return BEM_OK;
   }
   return BEM_ERR_INVALID_ARGUMENT;
 }
@@ -1039,6 +1044,7 @@ int get_tuning(int key) {
     case BEM_TUNE_TC_PROMOTE: return g_tc_promote;
     case BEM_TUNE_GMRES_REORTH: return g_gmres_reorth;
     case BEM_TUNE_ARNOLDI_CLUSTER: return g_arn_max_cluster;
+    case BEM_TUNE_ARNOLDI_MODE: return g_arn_mode;
   }
   return -1;
 }

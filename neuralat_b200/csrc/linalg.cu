@@ -36,6 +36,7 @@ namespace cg = cooperative_groups;
 
 int g_gmres_reorth = 0;     // Gram-Schmidt passes: 0 automatic, 1 one pass (CGS), 2 two passes (CGS2); a tuning knob
 int g_arn_max_cluster = 0;  // largest Arnoldi cluster size tried (0: 16); a tuning knob
+int g_arn_mode = 0;         // Arnoldi step: 0 automatic, 1 cluster kernel, 2 streamed kernels; a tuning knob
 
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
@@ -535,6 +536,8 @@ struct GmPtrs {
   double* y;       // [m][R]
   GmState* st;
   double* bnorm2;  // [m]
+  double* hacc;    // [2][m][2][2 (R+1)]  streamed step: h sums of the two passes, by step parity
+  double* nacc;    // [2][m][3]           streamed step: |w|^2 before and after each pass, by parity
 };
 
 // ---------------------------------------------------------------------------
@@ -703,8 +706,10 @@ struct ArnStream {
 
 // Dots pass (consumer threads own pairs, as in the update pass):
 // part[2l + c] = sum over this CTA's unknowns of conj(V[l]) w.  Each thread
-// forms its pairs' products for every row of the chunk in FP32 (w rounded
-// to FP32 like the stored basis), a warp reduce-scatter sums the lanes, and
+// forms its pairs' products for every row of the chunk in FP64 (exact for the
+// FP32 basis: the projections carry no rounding that the Gram-Schmidt
+// cancellation ||w|| / ||w'|| would amplify into lost orthogonality), a warp
+// reduce-scatter sums the lanes, and
 // each warp adds its partials to `part` (zeroed at launch) with FP64
 // shared-memory atomics: no barrier between the consumer warps, which run
 // through the chunks independently (the cluster barrier after the pass
@@ -716,25 +721,25 @@ __device__ __forceinline__ void arn_dots(const ArnStream& T, int pass, const dou
   for (int c = 0; c < T.nch; c++) {
     const float2* rows = T.acquire(pass, c);
     const int l0 = c * T.chunk, nl = min(T.chunk, T.k + 1 - l0);
-    float v[2 * kChunkMax];
+    double v[2 * kChunkMax];
 #pragma unroll
-    for (int q = 0; q < 2 * kChunkMax; q++) v[q] = 0.f;
+    for (int q = 0; q < 2 * kChunkMax; q++) v[q] = 0.0;
     for (int p = tid; p < npairs; p += kArnConsumers) {
       const bool pad = T.i0 + 2 * p + 1 >= T.P->n;
-      const double2 w0d = wsl[2 * p], w1d = wsl[2 * p + 1];
-      const float4 w = make_float4((float)w0d.x, (float)w0d.y, (float)w1d.x, (float)w1d.y);
+      const double2 w0 = wsl[2 * p], w1 = wsl[2 * p + 1];
 #pragma unroll
       for (int li = 0; li < kChunkMax; li++) {
         if (li < nl) {
           const float4 a = staged_pair(rows, li, T.units, p, pad);
-          v[2 * li] = fmaf(a.x, w.x, fmaf(a.y, w.y, fmaf(a.z, w.z, fmaf(a.w, w.w, v[2 * li]))));
-          v[2 * li + 1] = fmaf(a.x, w.y, fmaf(-a.y, w.x, fmaf(a.z, w.w, fmaf(-a.w, w.z, v[2 * li + 1]))));
+          const double ax = a.x, ay = a.y, az = a.z, aw = a.w;
+          v[2 * li] = fma(ax, w0.x, fma(ay, w0.y, fma(az, w1.x, fma(aw, w1.y, v[2 * li]))));
+          v[2 * li + 1] = fma(ax, w0.y, fma(-ay, w0.x, fma(az, w1.y, fma(-aw, w1.x, v[2 * li + 1]))));
         }
       }
     }
-    const float t = warp_reduce_scatter<2 * kChunkMax>(v, lane);
+    const double t = warp_reduce_scatter<2 * kChunkMax>(v, lane);
     T.release(pass, c);  // this warp is done with the stage
-    if ((lane & 1) == 0 && (lane >> 1) < 2 * nl) atomicAdd(&part[2 * l0 + (lane >> 1)], (double)t);
+    if ((lane & 1) == 0 && (lane >> 1) < 2 * nl) atomicAdd(&part[2 * l0 + (lane >> 1)], t);
   }
 }
 
@@ -1008,6 +1013,235 @@ __global__ void __launch_bounds__(kArnThreads, 1) gm_arnoldi_kernel(GmPtrs P, in
   }
 }
 
+// ---------------------------------------------------------------------------
+// Streamed Arnoldi step: launches over all SMs, no clusters, classical
+// Gram-Schmidt with selective reorthogonalisation (the criterion of Daniel,
+// Gragg, Kaufman and Stewart): a column gets a second pass only when the
+// first one removed most of w, |w'|^2 < |w|^2 / 2.
+//   gm_st_dots_kernel<0>    h1 = V^H Y (Y = this step's matvec output) and |Y|^2:
+//                           FP32 products per thread, FP64 block sums, FP64 atomics
+//   gm_st_update_kernel<0>  w' = Y - V h1 in FP64 -> P.w, Y cleared, |w'|^2
+//   gm_st_dots_kernel<1>,   for the columns that need it: h2 = V^H w',
+//   gm_st_update_kernel<1>  w'' = w' - V h2 -> P.w, |w''|^2
+//   gm_st_finish_kernel     v_{k+1} = w / |w| -> basis and the next matvec operand
+//   gm_st_givens_kernel     one warp per column: Givens rotation of h1 + h2 and
+//                           the step record (k + 1, activity); a separate
+//                           launch because every block of the other kernels
+//                           reads k and the activity flag that it advances
+// The sums are double-buffered by the column's step parity: a step's finish
+// kernel clears the other buffer for the next step (the cycle start clears
+// both).
+// ---------------------------------------------------------------------------
+constexpr int kStThreads = 256;
+constexpr int kStRows = 8;  // basis rows per register chunk of the dots pass
+
+__device__ __forceinline__ double* st_hacc(const GmPtrs& P, int buf, int s, int pass) {
+  return P.hacc + (((size_t)buf * P.m + s) * 2 + pass) * 2 * (P.R + 1);
+}
+// j = 0: |w|^2 before the first pass, 1: after it, 2: after the second
+__device__ __forceinline__ double* st_nacc(const GmPtrs& P, int buf, int s, int j) {
+  return P.nacc + ((size_t)buf * P.m + s) * 3 + j;
+}
+__device__ __forceinline__ bool st_reorth(const GmPtrs& P, int buf, int s) {
+  return *st_nacc(P, buf, s, 1) < 0.5 * *st_nacc(P, buf, s, 0);
+}
+
+// Block sum of v (all threads), added to *dst by thread 0; red: kStThreads / 32 doubles.
+__device__ __forceinline__ void st_block_add(double v, double* red, double* dst) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kStThreads / 32; w++) t += red[w];
+    atomicAdd(dst, t);
+  }
+}
+
+// Row l, unknowns i, i+1 of column s's basis; the padding entry of an odd n reads as zero.
+__device__ __forceinline__ float4 st_pair(const GmPtrs& P, int s, int l, int i) {
+  float4 v = *reinterpret_cast<const float4*>(vrow(P, s, l) + i);
+  if (i + 1 >= P.n) {
+    v.z = 0.f;
+    v.w = 0.f;
+  }
+  return v;
+}
+
+// Work item q of a streamed kernel: column q / nb, pairs [b span, (b+1) span)
+// of it, b = q % nb; persistent grids loop over the items.
+template <int PASS>
+__global__ void __launch_bounds__(kStThreads) gm_st_dots_kernel(GmPtrs P, int span, int nb) {
+  extern __shared__ __align__(16) double4 wst[];  // the item's w, span pairs
+  __shared__ double hs[2 * kMaxRestart];
+  __shared__ double red[kStThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int npairs = (P.n + 1) / 2;
+  for (int q = blockIdx.x; q < P.m * nb; q += gridDim.x) {  // uniform over the block
+    const int s = q / nb, p0 = (q - s * nb) * span, p1 = min(npairs, p0 + span);
+    if (!P.active[s] || p0 >= p1) continue;
+    const int k = P.kcol[s];
+    if (PASS == 1 && !st_reorth(P, k & 1, s)) continue;
+    __syncthreads();  // the previous item is done with hs, red and wst
+    for (int t = tid; t < 2 * (k + 1); t += kStThreads) hs[t] = 0.0;
+    double n2 = 0.0;
+    for (int p = p0 + tid; p < p1; p += kStThreads) {
+      const int i = 2 * p;
+      double4 w;
+      if (PASS == 0) {
+        const float2 y0 = P.Y[(size_t)i * P.m + s];
+        const float2 y1 = i + 1 < P.n ? P.Y[(size_t)(i + 1) * P.m + s] : make_float2(0.f, 0.f);
+        w = make_double4(y0.x, y0.y, y1.x, y1.y);
+        n2 += w.x * w.x + w.y * w.y + w.z * w.z + w.w * w.w;
+      } else {
+        const double2 a0 = P.w[(size_t)s * P.n + i];
+        const double2 a1 = i + 1 < P.n ? P.w[(size_t)s * P.n + i + 1] : make_double2(0.0, 0.0);
+        w = make_double4(a0.x, a0.y, a1.x, a1.y);
+      }
+      wst[p - p0] = w;
+    }
+    if (PASS == 0) st_block_add(n2, red, st_nacc(P, k & 1, s, 0));  // syncs the block
+    __syncthreads();
+    for (int c0 = 0; c0 <= k; c0 += kStRows) {
+      const int nl = min(kStRows, k + 1 - c0);
+      double v[2 * kStRows];
+#pragma unroll
+      for (int r = 0; r < 2 * kStRows; r++) v[r] = 0.0;
+      for (int p = p0 + tid; p < p1; p += kStThreads) {
+        const double4 w = wst[p - p0];
+#pragma unroll
+        for (int li = 0; li < kStRows; li++) {
+          if (li < nl) {
+            const float4 a = st_pair(P, s, c0 + li, 2 * p);
+            const double ax = a.x, ay = a.y, az = a.z, aw = a.w;
+            v[2 * li] = fma(ax, w.x, fma(ay, w.y, fma(az, w.z, fma(aw, w.w, v[2 * li]))));
+            v[2 * li + 1] = fma(ax, w.y, fma(-ay, w.x, fma(az, w.w, fma(-aw, w.z, v[2 * li + 1]))));
+          }
+        }
+      }
+      const double t = warp_reduce_scatter<2 * kStRows>(v, lane);
+      if ((lane & 1) == 0 && (lane >> 1) < 2 * nl) atomicAdd(&hs[2 * c0 + (lane >> 1)], t);
+    }
+    __syncthreads();
+    double* hacc = st_hacc(P, k & 1, s, PASS);
+    for (int t = tid; t < 2 * (k + 1); t += kStThreads) atomicAdd(&hacc[t], hs[t]);
+  }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kStThreads) gm_st_update_kernel(GmPtrs P, int span, int nb) {
+  __shared__ double2 h[kMaxRestart];
+  __shared__ double red[kStThreads / 32];
+  const int tid = threadIdx.x;
+  const int npairs = (P.n + 1) / 2;
+  for (int q = blockIdx.x; q < P.m * nb; q += gridDim.x) {  // uniform over the block
+    const int s = q / nb, p0 = (q - s * nb) * span, p1 = min(npairs, p0 + span);
+    if (!P.active[s] || p0 >= p1) continue;
+    const int k = P.kcol[s];
+    if (PASS == 1 && !st_reorth(P, k & 1, s)) continue;
+    const double* hacc = st_hacc(P, k & 1, s, PASS);
+    __syncthreads();  // the previous item is done with h and red
+    for (int l = tid; l <= k; l += kStThreads) h[l] = make_double2(hacc[2 * l], hacc[2 * l + 1]);
+    __syncthreads();
+    double n2 = 0.0;
+    for (int p = p0 + tid; p < p1; p += kStThreads) {
+      const int i = 2 * p;
+      double2 a0, a1;
+      if (PASS == 0) {
+        float2* y0p = P.Y + (size_t)i * P.m + s;
+        const float2 y0 = *y0p;
+        *y0p = make_float2(0.f, 0.f);
+        float2 y1 = make_float2(0.f, 0.f);
+        if (i + 1 < P.n) {
+          float2* y1p = P.Y + (size_t)(i + 1) * P.m + s;
+          y1 = *y1p;
+          *y1p = make_float2(0.f, 0.f);
+        }
+        a0 = make_double2(y0.x, y0.y);
+        a1 = make_double2(y1.x, y1.y);
+      } else {
+        a0 = P.w[(size_t)s * P.n + i];
+        a1 = i + 1 < P.n ? P.w[(size_t)s * P.n + i + 1] : make_double2(0.0, 0.0);
+      }
+#pragma unroll 4
+      for (int l = 0; l <= k; l++) {
+        const float4 v = st_pair(P, s, l, i);
+        const double2 cc = h[l];
+        a0.x -= (double)v.x * cc.x - (double)v.y * cc.y;
+        a0.y -= (double)v.x * cc.y + (double)v.y * cc.x;
+        a1.x -= (double)v.z * cc.x - (double)v.w * cc.y;
+        a1.y -= (double)v.z * cc.y + (double)v.w * cc.x;
+      }
+      P.w[(size_t)s * P.n + i] = a0;
+      if (i + 1 < P.n) P.w[(size_t)s * P.n + i + 1] = a1;
+      n2 += a0.x * a0.x + a0.y * a0.y + a1.x * a1.x + a1.y * a1.y;
+    }
+    st_block_add(n2, red, st_nacc(P, k & 1, s, 1 + PASS));
+  }
+}
+
+__global__ void __launch_bounds__(kStThreads) gm_st_finish_kernel(GmPtrs P, int span, int nb) {
+  const int tid = threadIdx.x;
+  const int npairs = (P.n + 1) / 2;
+  for (int q = blockIdx.x; q < P.m * nb; q += gridDim.x) {
+    const int s = q / nb, b = q - s * nb, p0 = b * span, p1 = min(npairs, p0 + span);
+    if (!P.active[s]) continue;
+    const int k = P.kcol[s];
+    const int buf = k & 1;
+    const double hn = sqrt(*st_nacc(P, buf, s, st_reorth(P, buf, s) ? 2 : 1));
+    const double inv = hn > 0.0 ? 1.0 / hn : 0.0;
+    float2* vk1 = P.Vb + ((size_t)s * (P.R + 1) + k + 1) * P.ldv;
+    for (int p = p0 + tid; p < p1; p += kStThreads) {
+      const int i = 2 * p;
+      const double2 a0 = P.w[(size_t)s * P.n + i];
+      const double2 a1 = i + 1 < P.n ? P.w[(size_t)s * P.n + i + 1] : make_double2(0.0, 0.0);
+      const float2 f0 = make_float2((float)(a0.x * inv), (float)(a0.y * inv));
+      const float2 f1 =
+          i + 1 < P.n ? make_float2((float)(a1.x * inv), (float)(a1.y * inv)) : make_float2(0.f, 0.f);
+      *reinterpret_cast<float4*>(vk1 + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+      store_operand(P, i, s, f0, f1);
+    }
+    if (b == 0) {  // the next step's sums start from zero (nobody reads that buffer now)
+      double* hnext = st_hacc(P, buf ^ 1, s, 0);  // both passes, contiguous
+      for (int t = tid; t < 4 * (P.R + 1); t += kStThreads) hnext[t] = 0.0;
+      if (tid < 3) *st_nacc(P, buf ^ 1, s, tid) = 0.0;
+    }
+  }
+}
+
+// One warp (block) per column, after gm_st_finish_kernel.
+__global__ void __launch_bounds__(32) gm_st_givens_kernel(GmPtrs P) {
+  extern __shared__ __align__(16) unsigned char st_raw[];  // ArnSmem
+  const int s = blockIdx.x, lane = threadIdx.x;
+  const int k = P.kcol[s];
+  if (!P.active[s]) {
+    if (lane == 0) column_done(P, s, k, false);
+    return;
+  }
+  const int buf = k & 1;
+  const bool two = st_reorth(P, buf, s);
+  const double hn = sqrt(*st_nacc(P, buf, s, two ? 2 : 1));
+  ArnSmem& S = *reinterpret_cast<ArnSmem*>(st_raw);
+  const double* h1 = st_hacc(P, buf, s, 0);
+  const double* h2 = st_hacc(P, buf, s, 1);
+  for (int l = lane; l <= k; l += 32) {
+    S.c1[l] = make_double2(h1[2 * l], h1[2 * l + 1]);
+    S.c2[l] = two ? make_double2(h2[2 * l], h2[2 * l + 1]) : make_double2(0.0, 0.0);
+  }
+  for (int l = lane; l < k; l += 32) {
+    S.csv[l] = P.cs[s * P.R + l];
+    S.snv[l] = P.sn[s * P.R + l];
+  }
+  if (lane == 0) {
+    S.gk = P.g[(size_t)s * (P.R + 1) + k];
+    S.tol = P.tol[s];
+  }
+  __syncwarp();
+  const bool still = arn_givens(P, S, s, k, hn);
+  if (lane == 0) column_done(P, s, k + 1, still);
+}
+
 // Back substitution H y = g on the Givens-reduced Hessenberg matrix, one
 // warp per column, column-oriented: y_j = g_j / H_jj, then the lanes update
 // g_0..g_{j-1} -= y_j H_{0..j-1, j} (column j of H is contiguous).
@@ -1185,7 +1419,7 @@ inline size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
 struct Layout {
   size_t Vb, H, cs, sn, g, w, d, x, r, X, Y, norm2, rnorm2, beta, tol, resid, active, kend, kcol, colstep, y, st,
-      bnorm2, tc, total;
+      bnorm2, hacc, nacc, tc, total;
 };
 
 Layout layout(int n, int m, int R, int precision) {
@@ -1219,6 +1453,8 @@ Layout layout(int n, int m, int R, int precision) {
   L.colstep = take(sizeof(int) * m);
   L.y = take(sizeof(double2) * (size_t)m * R);
   L.bnorm2 = take(sizeof(double) * m);
+  L.hacc = take(sizeof(double) * 2 * (size_t)m * 4 * (R + 1));
+  L.nacc = take(sizeof(double) * 2 * (size_t)m * 3);
   L.tc = take(precision == BEM_PREC_FP32 ? 0 : tc_workspace_bytes(n, m, precision));
   L.total = o;
   return L;
@@ -1303,6 +1539,17 @@ struct ArnShape {
   int chunk = 0;
   size_t smem = 0;
 };
+
+int sm_count_linalg() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
 
 int arnoldi_shape(int n, int m, ArnShape* out) {
   static std::atomic<bool> attr{false};
@@ -1419,6 +1666,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   P.y = (double*)(w + L.y);
   P.st = (GmState*)(w + L.st);
   P.bnorm2 = (double*)(w + L.bnorm2);
+  P.hacc = (double*)(w + L.hacc);
+  P.nacc = (double*)(w + L.nacc);
   double* rnorm2 = (double*)(w + L.rnorm2);
   void* tcws = w + L.tc;
   const int prec = params->precision;
@@ -1457,6 +1706,26 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int rc0 = arnoldi_shape(n, m, &shape);
     if (rc0) return rc0;
   }
+  // The streamed step (launches over all SMs, selective second pass) when
+  // the mode key asks for it; the cluster kernel is faster at s5 and s6.
+  const bool streamed = reorth == 0 && g_arn_mode == 2;
+  const int npairs_all = (n + 1) / 2;
+  // about 8 work items per SM over all columns, each of 128 to 4096 pairs
+  // (w of an item in FP64: at most 128 KB of shared memory)
+  const long long st_target = (long long)npairs_all * m / (8LL * sm_count_linalg());
+  const int st_span = (int)std::max(128LL, std::min(4096LL, st_target));
+  const int st_nb = (npairs_all + st_span - 1) / st_span;
+  const int st_grid = std::min(m * st_nb, 3 * sm_count_linalg());  // persistent: up to 3 blocks per SM
+  if (streamed) {
+    static std::atomic<bool> st_attr{false};
+    if (!st_attr.load(std::memory_order_acquire)) {
+      BEM_CUDA_TRY(cudaFuncSetAttribute(gm_st_dots_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(sizeof(double4) * 4096)));
+      BEM_CUDA_TRY(cudaFuncSetAttribute(gm_st_dots_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(sizeof(double4) * 4096)));
+      st_attr.store(true, std::memory_order_release);
+    }
+  }
   // one Arnoldi step: the matvec reads the operand that gm_arnoldi_kernel (or
   // gm_start_norm_kernel) wrote and accumulates into Y, which
   // gm_arnoldi_kernel clears again after reading it
@@ -1465,6 +1734,18 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
                  ? launch_cgemv((const float2*)A, n, P.X, m, P.Y, P.active, st, &P.st->err)
                  : tc_gemm(tcws, n, prec, m, P.Y, P.active, st);
     if (r2) return r2;
+    if (streamed) {
+      (gm_st_dots_kernel<0><<<st_grid, kStThreads, sizeof(double4) * st_span, st>>>(P, st_span, st_nb),
+       count_launch());
+      (gm_st_update_kernel<0><<<st_grid, kStThreads, 0, st>>>(P, st_span, st_nb), count_launch());
+      (gm_st_dots_kernel<1><<<st_grid, kStThreads, sizeof(double4) * st_span, st>>>(P, st_span, st_nb),
+       count_launch());
+      (gm_st_update_kernel<1><<<st_grid, kStThreads, 0, st>>>(P, st_span, st_nb), count_launch());
+      (gm_st_finish_kernel<<<st_grid, kStThreads, 0, st>>>(P, st_span, st_nb), count_launch());
+      (gm_st_givens_kernel<<<m, 32, sizeof(ArnSmem), st>>>(P), count_launch());
+      BEM_CUDA_TRY(cudaGetLastError());
+      return BEM_OK;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)shape.cluster, (unsigned)m, 1);
     cfg.blockDim = dim3(kArnThreads, 1, 1);
@@ -1545,6 +1826,10 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     bool first_cycle = true;
     while (total_iters < params->max_iters) {
       BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
+      if (streamed) {  // both parity buffers of the streamed step's sums
+        BEM_CUDA_TRY(cudaMemsetAsync(P.hacc, 0, sizeof(double) * 2 * (size_t)m * 4 * (R + 1), s));
+        BEM_CUDA_TRY(cudaMemsetAsync(P.nacc, 0, sizeof(double) * 2 * (size_t)m * 3, s));
+      }
       if (!first_cycle) {
         (gm_pack_d_kernel<<<gv, 256, 0, s>>>(P), count_launch());
         if ((rc = inner_matvec())) return rc;
