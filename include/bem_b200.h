@@ -47,7 +47,7 @@ typedef enum bem_status {
   BEM_ERR_NOT_CONVERGED = 6,    /* iteration limit reached before tolerance */
   BEM_ERR_BREAKDOWN = 7,        /* Krylov breakdown / singular system */
   BEM_ERR_CUDA = 8,             /* CUDA runtime error (incl. no device) */
-  BEM_ERR_UNSUPPORTED = 9       /* valid request this build does not support */
+  BEM_ERR_UNSUPPORTED = 9       /* valid request the library does not support */
 } bem_status;
 
 /* Operator types, same order as the reference's PotentialType
