@@ -189,7 +189,7 @@ def test_solve_linear_equation_bicgstab_and_gmres(solvers):
     # GMRES verifies its stopping test with an FP64 residual
     x = solve_linear_equation(lhs, rhs).cpu().numpy()
     assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.05e-5
-    # BiCGSTAB (matrix or callable) judges ||r|| in FP32 like the reference
+    # BiCGSTAB (matrix or callable) measures ||r|| in FP32 like the reference
     for x in (solve_linear_equation(lhs, rhs, solver="bicgstab"),
               solve_linear_equation(lambda z: cmatmul(lhs, z), rhs)):
         x = x.cpu().numpy()
