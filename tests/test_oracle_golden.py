@@ -64,3 +64,21 @@ def test_curls_match_reference_preprocess(golden):
     n = np.cross(p1 - p0, p2 - p0)
     n /= np.linalg.norm(n, axis=1, keepdims=True)
     assert np.abs(n - golden["normals"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("suffix", SUFFIXES)
+def test_burton_miller_operators_are_the_hbie_combination(golden, suffix):
+    """bm_lhs = -K + (i/k) W and bm_rhs = -V - (i/k) K' at every order: the
+    identity behind assembling HBIE (solver.py:106-116) as the Burton-Miller
+    pair.  Exact to rounding in the FP64 restatement (all operators share
+    their quadrature points), within FP32 rounding in the reference's own
+    kernels."""
+    v, t = golden["vertices"], golden["triangles"]
+    for ki, k in enumerate(golden["ks"]):
+        beta = 1j / k
+        mats = {l: O.boundary_matrix(l, v, t, k, approx=suffix) for l in LAYERS}
+        assert relfro(mats["bm_lhs"], -mats["double"] + beta * mats["hypersingular"]) <= 1e-12, (suffix, k)
+        assert relfro(mats["bm_rhs"], -mats["single"] - beta * mats["adjointdouble"]) <= 1e-12, (suffix, k)
+        g = {l: golden[f"k{ki}_{l}{suffix}"] for l in LAYERS}
+        assert relfro(g["bm_lhs"], -g["double"] + beta * g["hypersingular"]) <= TOL, (suffix, k)
+        assert relfro(g["bm_rhs"], -g["single"] - beta * g["adjointdouble"]) <= TOL, (suffix, k)
