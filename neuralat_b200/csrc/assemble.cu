@@ -14,9 +14,13 @@
 //   * one pass evaluates each quadrature-point pair once for BOTH operators
 //     (shared r, rsqrt and sincos), with the 6-point rule's constant weights
 //     folded into immediate FMA operands;
-//   * a CTA owns 32 test triangles (one per lane) x one 16-triangle trial
-//     tile; all 8 warps share the test triangles and broadcast their trial
-//     triangles from shared memory;
+//   * V and K together (regular_sym_kernel): each unordered pair once, a
+//     CTA owns one 16-triangle test tile (lane & 15) and sweeps the trial
+//     tiles at or after it, two trial triangles per warp, tiles
+//     double-buffered by bulk copies, two CTAs per SM; one operator alone
+//     (regular_vk_kernel): a CTA owns 32 test triangles (one per lane) x one
+//     16-triangle trial tile, the 8 warps broadcasting their trial triangles
+//     from shared memory;
 //   * pair blocks go to a shared-memory "corner" slab (test corner x trial
 //     corner) and are reduced on chip onto the tile's distinct vertices, so
 //     each matrix entry receives ~0.8 vector atomics per triangle pair instead
