@@ -58,11 +58,16 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", default="fp16x3", choices=["fp32", "bf16x3", "bf16", "fp16x3"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison timing")
+    ap.add_argument("--plain-steps", type=int, default=5, help="timed steps of the plain-FP32 comparison (>= 5)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU kernels (B0) beside the CPU line")
     ap.add_argument("--validate", action="store_true", help="also compare against the FP64 oracle (minutes)")
     ap.add_argument("--kernel-case", choices=["assemble", "assemble_bm", "solve", "eval"], default=None,
                     help="profiling case: one stage on an icosphere of --subdiv, after one warm-up launch")
     ap.add_argument("--subdiv", type=int, default=4)
+    ap.add_argument("--cpu-validate", action="store_true",
+                    help="sampled CPU model vs one whole measured FP64 CPU problem on an icosphere of --subdiv")
     ap.add_argument("--large-case", action="store_true",
                     help="large multi-RHS configuration: icosphere s6 (N=40962) with 5%% radial noise, 64 RHS, "
                          "8 kHz, 4096 listeners (stage times, solver info, FP64 residual)")
@@ -174,7 +179,27 @@ def fp32_peak_tflops(sm_max_mhz=None):
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(v, t, k, g, pts, budget_s=20.0):
+def host_cpu():
+    """CPU model and logical core count of this host (for the CPU baseline record)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+# The sampled CPU model below was checked against one full FP64 problem on an
+# icosphere s4 workload (``--cpu-validate``): the ratio model / full is
+# recorded in the line of that case and quoted in ``sample``.
+CPU_MODEL_CHECK = "model checked against a full FP64 s4 problem by bench.py --cpu-validate"
+
+
+def cpu_baseline(v, t, k, g, pts, rows_sampled=48):
     """FP64 CPU restatement (oracle) timed on a bounded sample, extrapolated to
     one full problem: assembly of sampled rows of V and K, a dense complex128
     LU solve of a smaller system (scaled by n^3), listener evaluation for a
@@ -184,7 +209,7 @@ def cpu_baseline(v, t, k, g, pts, budget_s=20.0):
     O.build()
     nv, nt = v.shape[0], t.shape[0]
     v64 = v.astype(np.float64)
-    rows = np.linspace(0, nv - 1, 48).astype(np.int32)
+    rows = np.linspace(0, nv - 1, min(rows_sampled, nv)).astype(np.int32)
     mask = np.zeros(nv, bool)
     mask[rows] = True
     frac_tris = float(np.any(mask[t], axis=1).sum()) / nt
@@ -192,7 +217,7 @@ def cpu_baseline(v, t, k, g, pts, budget_s=20.0):
     O.boundary_matrix("single", v64, t, k, rows=rows)
     O.boundary_matrix("double", v64, t, k, rows=rows)
     t_asm = (time.perf_counter() - t0) / frac_tris
-    ns = 2048
+    ns = min(2048, nv)
     rng = np.random.default_rng(0)
     A = rng.standard_normal((ns, ns)) + 1j * rng.standard_normal((ns, ns))
     B = rng.standard_normal((ns, g.shape[1])) + 1j * rng.standard_normal((ns, g.shape[1]))
@@ -209,9 +234,31 @@ def cpu_baseline(v, t, k, g, pts, budget_s=20.0):
         "value": total, "unit": "s/problem", "cores": int(O.num_threads()), "kind": "port",
         "sample": (f"FP64 oracle: V+K rows of {rows.size} vertices ({frac_tris:.4f} of test triangles) "
                    f"extrapolated; complex128 LU {ns}x{ns} x{g.shape[1]} RHS scaled by (N/{ns})^3; "
-                   f"{pp.shape[0]} of {pts.shape[0]} listeners scaled"),
+                   f"{pp.shape[0]} of {pts.shape[0]} listeners scaled; {CPU_MODEL_CHECK}"),
         "stages_s": {"assemble": t_asm, "solve": t_solve, "eval": t_eval},
+        **host_cpu(),
     }
+
+
+def cpu_full(v, t, k, g, pts):
+    """One whole FP64 CPU problem on the oracle, every stage measured: full V,
+    K and M assembly, the dense complex128 solve of the CBIE (LAPACK) and all
+    listeners."""
+    from oracle import oracle as O
+
+    O.build()
+    v64 = v.astype(np.float64)
+    t0 = time.perf_counter()
+    V = O.boundary_matrix("single", v64, t, k)
+    K = O.boundary_matrix("double", v64, t, k)
+    M = O.identity_matrix(v64, t)
+    t1 = time.perf_counter()
+    u = np.linalg.solve(0.5 * M - K, -V @ g.astype(np.complex128))
+    t2 = time.perf_counter()
+    p = O.boundary2potential(v64, t, k, g.astype(np.complex128), u, pts.astype(np.float64))
+    t3 = time.perf_counter()
+    return {"value": t3 - t0, "stages_s": {"assemble": t1 - t0, "solve": t2 - t1, "eval": t3 - t2},
+            "cores": int(O.num_threads()), "pressure_norm": float(np.linalg.norm(p))}
 
 
 # Multi-rank plumbing ("replicas only": every rank solves its own problem, no
@@ -242,6 +289,95 @@ def whole_job_seconds_per_problem(ms_per_step: float, world: int) -> float:
     return (ms_per_step / 1e3) / world
 
 
+def reference_preprocess(torch, vertices, triangles):
+    """Unit normals and surface curls as the reference's ``preprocess``
+    computes them with torch (src/bem/solver.py:40-58): edge vectors, the
+    batched inverse metric, gradients of the three P1 functions, n x grad."""
+    v0, v1, v2 = (vertices[triangles[:, i].long()] for i in range(3))
+    n = torch.linalg.cross(v1 - v0, v2 - v0, dim=1)
+    n = n / torch.norm(n, dim=1, keepdim=True)
+    J = torch.stack([v1 - v0, v2 - v0], dim=2)
+    jit = torch.bmm(J, torch.inverse(torch.bmm(J.transpose(1, 2), J)))
+    rg = torch.tensor([[-1.0, 1.0, 0.0], [-1.0, 0.0, 1.0]], dtype=torch.float32, device=vertices.device)
+    grads = torch.matmul(jit, rg).transpose(1, 2)
+    return n.contiguous(), torch.linalg.cross(n.unsqueeze(1), grads, dim=2).contiguous()
+
+
+def reference_gpu(v, t, k, g, pts, steps=1):
+    """B0: the reference's own CUDA kernels (src/bem/cuda/bind.cu, built
+    unmodified into oracle/_ref by oracle/build_ref.py) on this workload,
+    driven the way its ``BEM_Solver.CBIE`` + ``boundary2potential`` drive
+    them (src/bem/solver.py:83-147): torch preprocess, identity / single /
+    double boundary matrices, 0.5 I - K and -V g with torch (cuBLAS), the
+    reference's BiCGSTAB per right-hand side with its defaults (500 steps,
+    tol 1e-10 on ||r||^2 / ||b||^2), then the two potential matrices and
+    their products.  Per-stage CUDA-event times after one warm-up problem,
+    and the listener error against the same FP64 fixture as our line."""
+    import torch
+
+    from neuralat_b200.bem.bicgstab import BiCGSTAB
+    from oracle import build_ref
+
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    ref = build_ref.load_prebuilt()
+    if ref is None:
+        return {"unavailable": "oracle/_ref/neuralat_ref_bem.so not built"}
+    dev = torch.device("cuda", 0)
+    vt = torch.from_numpy(v).to(dev)
+    tt = torch.from_numpy(t).to(dev)
+    gt = torch.from_numpy(g).to(dev)
+    pt = torch.from_numpy(pts).to(dev)
+    kf = float(k)
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        return e
+
+    def problem():
+        e = [ev()]
+        normals, curls = reference_preprocess(torch, vt, tt)
+        e.append(ev())
+        identity = ref.identity_matrix(vt, tt)
+        V = ref.single_boundary_matrix(vt, tt, normals, curls, kf)
+        K = ref.double_boundary_matrix(vt, tt, normals, curls, kf)
+        e.append(ev())
+        A = 0.5 * identity - K
+        del identity, K
+        b = -V @ gt
+        del V
+        e.append(ev())
+        iters = []
+        us = []
+        for j in range(gt.shape[1]):
+            solver = BiCGSTAB(lambda x: A @ x)
+            us.append(solver.solve(b[:, j].contiguous(), nsteps=500, tol=1e-10, atol=1e-16))
+            iters.append(solver.iterations)
+        u = torch.stack(us, dim=1)
+        del A
+        e.append(ev())
+        S = ref.single_boundary_potential(vt, tt, pt, kf)
+        D = ref.double_boundary_potential(vt, tt, pt, kf)
+        p = -S @ gt + D @ u
+        e.append(ev())
+        torch.cuda.synchronize()
+        return e, p, iters
+
+    problem()
+    times, p, iters = [], None, None
+    for _ in range(max(1, steps)):
+        e, p, iters = problem()
+        times.append([e[i].elapsed_time(e[i + 1]) for i in range(len(e) - 1)])
+    names = ["preprocess", "assemble", "rhs", "solve", "eval"]
+    stage_ms = {n: float(np.mean([tm[i] for tm in times])) for i, n in enumerate(names)}
+    return {"s_per_problem": sum(stage_ms.values()) / 1e3, "stages_ms": stage_ms, "steps": len(times),
+            "bicgstab_iterations": iters,
+            "listener_err_vs_fp64": listener_error_vs_fixture(v, t, k, g, p, None).get("mixed"),
+            "what": "reference src/bem kernels (bind.cu, unmodified, oracle/_ref) + torch/cuBLAS + the reference's "
+                    "BiCGSTAB per RHS with its defaults; FP32; one B200"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -261,9 +397,14 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "parallelism": "host cores"},
         "cpu_baseline": {"value": value, "unit": "s/problem", "cores": cb["cores"], "kind": cb["kind"],
-                         "sample": cb["sample"]},
+                         "sample": cb["sample"], "cpu_model": cb["cpu_model"], "nproc": cb["nproc"]},
         "e2e": {"value": value, "unit": "s/problem", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        try:
+            line["reference_gpu"] = reference_gpu(v, t, k, g, pts)
+        except Exception as e:  # a reported side measurement; the CPU line stands
+            line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
 
 
@@ -308,7 +449,8 @@ def run_ours(args):
         e0 = ev()
         s = BEM_Solver(v_d, t_d)
         e1 = ev()
-        V, A = s.assemble_vk(k)
+        # the assembly's bounded-wait status is read once after the timed region
+        V, A = s.assemble_vk(k, check=False)
         e2 = ev()
         rhs = -cmatmul(V, g_d)
         del V
@@ -340,13 +482,16 @@ def run_ours(args):
         barrier()
         l0 = lib.bem_kernel_launches()
         t_start = ev()
+        last_p = None
         for _ in range(args.steps):
             inf = {}
-            step(rec, inf)
+            _, last_p = step(rec, inf)
             infos.append(inf)
         t_end = ev()
         barrier()
         l1 = lib.bem_kernel_launches()
+    # no bounded wait of any assembly kernel expired in the timed steps
+    L.check(lib.bem_assembly_status(_stream(dev)), "assembly in the timed steps")
     total_ms = max_over_ranks(t_start.elapsed_time(t_end))
     ms_per_step = total_ms / args.steps
     value = whole_job_seconds_per_problem(ms_per_step, world)
@@ -396,14 +541,15 @@ def run_ours(args):
         plain_step()
         torch.cuda.synchronize()
         ps = ev()
-        nplain = 2
+        nplain = max(5, args.plain_steps)
         for _ in range(nplain):
-            plain_step()
+            p_plain = plain_step()
         pe = ev()
         torch.cuda.synchronize()
-        plain = {"s_per_problem": ps.elapsed_time(pe) / nplain / 1e3, "steps": nplain,
+        plain = {"s_per_problem": ps.elapsed_time(pe) / nplain / 1e3, "steps": nplain, "warmup": 1,
                  "form": "separate V, K, M assembly; explicit 0.5M-K; one FP32 single-RHS GMRES per RHS; "
                          "explicit S, D potential matrices"}
+    err = listener_error_vs_fixture(v, t, k, g, last_p, p_plain if plain else None)
 
     # ---- roofline of the dominant kernel (fused regular V+K assembly) ----------
     clocks = clk.summary()
@@ -459,7 +605,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(v, t, k, g, pts)
-        cpu = {kk: cb[kk] for kk in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {kk: cb[kk] for kk in ("value", "unit", "cores", "kind", "sample", "cpu_model", "nproc")}
 
     if rank == 0:
         it = infos[-1] if infos else {}
@@ -479,6 +625,7 @@ def run_ours(args):
             "solver": {kk: it.get(kk) for kk in ("iterations", "refinements", "matvecs", "rel_residual", "status")},
             "plain_fp32": plain,
             "speedup_vs_plain_fp32": (plain["s_per_problem"] / (ms_per_step / 1e3)) if plain else None,
+            "listener_err_vs_fp64": err,
         }
         if args.validate:
             line["validation"] = validate(v, t, k, g, pts, dev, args.precision)
@@ -486,6 +633,39 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+FIXTURE = os.path.join(ROOT, "tests", "golden", "cfg2_pressures.npz")
+ERR_BAR = 1e-4
+
+
+def listener_error_vs_fixture(v, t, k, g, p_mixed, p_plain):
+    """Listener-pressure error of the timed pipeline's last step (and of one
+    plain-FP32 step) against the committed FP64-oracle pressures of this
+    workload (tests/golden/make_cfg2_reference.py): the max over right-hand
+    sides of ||p - p_fp64|| / ||p_fp64|| over the listeners."""
+    if not os.path.exists(FIXTURE):
+        return {"unavailable": f"{os.path.relpath(FIXTURE, ROOT)} missing"}
+    f = np.load(FIXTURE)
+    same = (int(f["nv"]) == v.shape[0] and int(f["nt"]) == t.shape[0] and abs(float(f["k"]) - float(np.float32(k))) <
+            1e-9 * abs(k) and abs(float(f["vertex_checksum"]) - float(np.abs(v.astype(np.float64)).sum())) <
+            1e-9 * float(f["vertex_checksum"]))
+    if not same:
+        return {"unavailable": "fixture was made for another workload"}
+    ref = f["pressures"]
+
+    def rel(p):
+        if p is None:
+            return None
+        p = p.detach().cpu().numpy().astype(np.complex128)
+        return float((np.linalg.norm(p - ref, axis=0) / np.linalg.norm(ref, axis=0)).max())
+
+    e_mixed, e_plain = rel(p_mixed), rel(p_plain)
+    return {"mixed": e_mixed, "plain": e_plain, "bar": ERR_BAR,
+            "both_within_bar": bool(e_mixed is not None and e_mixed <= ERR_BAR and
+                                    (e_plain is None or e_plain <= ERR_BAR)),
+            "measure": "max over the RHS of ||p - p_fp64||_2 / ||p_fp64||_2 over the listeners; p_fp64 = FP64 "
+                       "oracle (dense CBIE solve) on the same float32 inputs, tests/golden/cfg2_pressures.npz"}
 
 
 def validate(v, t, k, g, pts, dev, precision):
@@ -503,6 +683,28 @@ def validate(v, t, k, g, pts, dev, precision):
     p_ref = O.boundary2potential(v, t, k, g, u_ref, pts)
     err = np.linalg.norm(p - p_ref, axis=0) / np.linalg.norm(p_ref, axis=0)
     return {"listener_rel_err_per_rhs": err.tolist(), "max": float(err.max())}
+
+
+def run_cpu_validate(args):
+    """The sampled CPU model (``cpu_baseline``) against one whole measured
+    FP64 CPU problem on the same box: the benchmark workload's recipe on an
+    icosphere of --subdiv (default 4: N = 2562), where the full problem takes
+    about a minute."""
+    from neuralat_b200.bem import meshes as M
+
+    v, t = M.icosphere(args.subdiv, 0.15)
+    v = (v * np.random.default_rng(1).uniform(0.7, 1.3, size=3)).astype(np.float32)
+    t = t.astype(np.int32)
+    k = M.wavenumber(4000.0)
+    g = M.smoothed_gaussian_field(v.shape[0], t, 8, seed=2).astype(np.complex64)
+    pts = M.sphere_points(256, 0.5, seed=0).astype(np.float32)
+    model = cpu_baseline(v, t, k, g, pts)
+    full = cpu_full(v, t, k, g, pts)
+    line = {"case": "cpu_model_check", "N": int(v.shape[0]), "T": int(t.shape[0]), "rhs": 8, "listeners": 256,
+            "model_s": model["value"], "full_s": full["value"], "model_over_full": model["value"] / full["value"],
+            "model_stages_s": model["stages_s"], "full_stages_s": full["stages_s"], "cores": full["cores"],
+            **host_cpu()}
+    print(json.dumps(line), flush=True)
 
 
 def run_kernel_case(args):
@@ -637,11 +839,13 @@ def run_large_case(args):
         p = s.boundary2potential(k, g, u, pts)
         e.append(ev())
         torch.cuda.synchronize()
+        problem.last_u = u
         return e, p
 
     problem({})
     info = {}
     e, p = problem(info)
+    u_timed = problem.last_u
     names = ["geometry", "assemble", "rhs", "solve", "eval"]
     stages = {n: e[i].elapsed_time(e[i + 1]) for i, n in enumerate(names)}
     line = {"case": "large_multi_rhs", "N": int(v.shape[0]), "T": int(t.shape[0]), "rhs": int(g.shape[1]),
@@ -650,7 +854,70 @@ def run_large_case(args):
             "solver": {kk: info.get(kk) for kk in ("iterations", "refinements", "matvecs", "rel_residual", "status")},
             "pressure_finite": bool(torch.isfinite(torch.view_as_real(p)).all()),
             "peak_device_gb": torch.cuda.max_memory_allocated() / 1e9}
+    line["validation"] = validate_large(w, v, t, g, pts, k, u_timed, args.precision)
     print(json.dumps(line), flush=True)
+
+
+CFG5_ROWS = os.path.join(ROOT, "tests", "golden", "cfg5_rows.npz")
+
+
+def validate_large(w, v, t, g, pts, k, u, precision):
+    """Error of the large multi-RHS problem against FP64 references (after the
+    timed problem, not timed):
+      * rows: 64 seeded rows of V and 1/2 M - K against the FP64 oracle's,
+        through 16 random projections per row (tests/golden/cfg5_rows.npz,
+        made by tests/golden/make_cfg5_rows.py);
+      * per right-hand side, the FP64 residual ||b - A x|| / ||b|| of the
+        timed solution against the FP32-stored operator;
+      * an analytic monopole at the centre as one more right-hand side: the
+        listener pressures against e^{ikr}/(4 pi r) (P1 discretisation error)."""
+    import torch
+
+    from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
+    from neuralat_b200.bem import meshes as M
+
+    out = {}
+    s = BEM_Solver(v, t)
+    V, A = s.assemble_vk(k)
+    if os.path.exists(CFG5_ROWS):
+        f = np.load(CFG5_ROWS)
+        if int(f["nv"]) == v.shape[0] and abs(float(f["k"]) - float(np.float32(k))) < 1e-6 * abs(k):
+            rows = torch.from_numpy(f["rows"].astype(np.int64)).cuda()
+            rng = np.random.default_rng(66)
+            nv = v.shape[0]
+            Z = (rng.standard_normal((nv, 16)) + 1j * rng.standard_normal((nv, 16))) / np.sqrt(2.0)
+            pv = V[rows].cpu().numpy().astype(np.complex128) @ Z
+            pa = A[rows].cpu().numpy().astype(np.complex128) @ Z
+            out["rows_rel_err"] = {
+                "V": float(np.linalg.norm(pv - f["V_proj"]) / np.linalg.norm(f["V_proj"])),
+                "half_M_minus_K": float(np.linalg.norm(pa - f["A_proj"]) / np.linalg.norm(f["A_proj"])),
+                "rows": int(rows.numel()), "measure": "16 complex Gaussian projections per row, relative Frobenius"}
+    b = -cmatmul(V, g)
+    # FP64 residual per column, in row blocks (complex128 copies of 4096 rows at a time)
+    r2 = torch.zeros(g.shape[1], dtype=torch.float64, device=g.device)
+    u64 = u.to(torch.complex128)
+    for r0 in range(0, A.shape[0], 4096):
+        blk = A[r0:r0 + 4096].to(torch.complex128)
+        r2 += ((b[r0:r0 + 4096].to(torch.complex128) - blk @ u64).abs() ** 2).sum(dim=0)
+        del blk
+    rel = (r2.sqrt() / b.to(torch.complex128).abs().pow(2).sum(dim=0).sqrt()).cpu().numpy()
+    out["fp64_residual_per_rhs"] = {"max": float(rel.max()), "median": float(np.median(rel)), "all": rel.tolist()}
+    # analytic monopole (exact for any closed surface around the source)
+    vd = w["vertices"].astype(np.float32).astype(np.float64)
+    nrm = M.vertex_normals(vd, w["triangles"])
+    d = vd
+    rr = np.linalg.norm(d, axis=1)
+    ikr = 1j * k * rr
+    gm = (-np.exp(ikr) / (4 * np.pi * rr ** 3) * (1 - ikr) * np.sum(d * nrm, axis=1)).astype(np.complex64)
+    gm_d = torch.from_numpy(gm).cuda()
+    um = gmres(A, -cmatmul(V, gm_d), rtol=1e-6, precision=precision)
+    pm = s.boundary2potential(k, gm_d, um, pts).cpu().numpy()
+    pp = pts.cpu().numpy().astype(np.float64)
+    rp = np.linalg.norm(pp, axis=1)
+    exact = np.exp(1j * k * rp) / (4 * np.pi * rp)
+    out["monopole_listener_rel_err"] = float(np.linalg.norm(pm - exact) / np.linalg.norm(exact))
+    del V, A
+    return out
 
 
 def run_grad_case(args):
@@ -693,7 +960,28 @@ def run_grad_case(args):
             "k": k, "forward_ms": fwd, "backward_ms": bwd, "steps": len(runs),
             "grad_finite": bool(torch.isfinite(vg).all() and torch.isfinite(torch.view_as_real(gg)).all()),
             "grad_vertices_norm": float(vg.norm()), "grad_neumann_norm": float(gg.abs().norm())}
+    line["fd_check"] = grad_vs_fixture(w, vg.double().cpu().numpy(), gg.cpu().numpy())
     print(json.dumps(line), flush=True)
+
+
+CFG4_FD = os.path.join(ROOT, "tests", "golden", "cfg4_fd.npz")
+
+
+def grad_vs_fixture(w, gx, gg):
+    """Adjoint gradient against FP64 central differences of the oracle at 64
+    seeded vertex coordinates and 16 Neumann entries (tests/golden/cfg4_fd.npz,
+    made by tests/golden/make_cfg4_fd.py)."""
+    if not os.path.exists(CFG4_FD):
+        return {"unavailable": "tests/golden/cfg4_fd.npz missing"}
+    f = np.load(CFG4_FD)
+    if int(f["nv"]) != gx.shape[0]:
+        return {"unavailable": "fixture was made for another workload"}
+    adj_v = np.array([gx[a, c] for a, c in f["coords"]])
+    adj_g = np.stack([gg[f["neumann_index"]].real, gg[f["neumann_index"]].imag], axis=1)
+    return {"fd_rel_err_vertices": float(np.linalg.norm(adj_v - f["fd_vertices"]) / np.linalg.norm(f["fd_vertices"])),
+            "fd_rel_err_neumann": float(np.linalg.norm(adj_g - f["fd_neumann"]) / np.linalg.norm(f["fd_neumann"])),
+            "coordinates": int(len(f["coords"])), "neumann_entries": int(len(f["neumann_index"])), "bar": 1e-3,
+            "step": "1e-4 relative (mesh radius; max |g|), FP64 central differences on the oracle"}
 
 
 def run_modal_case(args):
@@ -763,6 +1051,8 @@ def main():
         run_batch_case(args)
     elif args.kernel_case:
         run_kernel_case(args)
+    elif args.cpu_validate:
+        run_cpu_validate(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -92,6 +92,19 @@ int bem_geometry_build(const float* vertices, int nv, const int* triangles, int 
 /* Copies the per-triangle unit normals (nt,3) and surface curls (nt,3,3)
  * (rows b: n x grad phi_b), solver.py:40-58.  Either output may be NULL. */
 int bem_geometry_normals(const void* geom, float* normals, float* curls, bem_stream_t stream);
+/* BEM_OK, or BEM_ERR_CUDA if a bounded wait of an assembly kernel (the bulk
+ * copies of trial tiles) expired while assembling on this geometry since the
+ * last call; a matrix assembled meanwhile may be wrong.  The status word lives
+ * in the geometry workspace (assembly kernels write it although the geometry
+ * is passed as const); this call clears it and synchronises `stream`.  No
+ * counterpart in the reference, whose kernels report no errors. */
+int bem_geometry_status(const void* geom, bem_stream_t stream);
+/* Forgets the host-side copy of the geometry header that the library keeps
+ * per workspace address.  Call it before freeing or reusing a geometry
+ * workspace; a later call that passes the same address then reads the header
+ * from the device again (and rejects a buffer that holds no geometry with
+ * BEM_ERR_WORKSPACE).  No counterpart in the reference. */
+int bem_geometry_release(const void* geom);
 
 /* ------------------------------------------------------------------------
  * Assembly on a built geometry.
@@ -158,9 +171,11 @@ typedef struct bem_bm_problem {
 int bem_batch_matrices_bm(const bem_bm_problem* problems, int nproblems, int order, void* workspace,
                           size_t workspace_bytes, bem_stream_t stream);
 
-/* BEM_OK, or BEM_ERR_CUDA if a bounded wait of an assembly kernel (the
- * bulk copies of trial tiles) expired since the last call; clears the flag
- * and synchronises `stream`.  No counterpart in the reference. */
+/* BEM_OK, or BEM_ERR_CUDA if a bounded wait of an assembly kernel (the bulk
+ * copies of trial tiles) expired anywhere in this process since the last
+ * call, on any stream and geometry; clears the process-wide flag and
+ * synchronises `stream`.  bem_geometry_status reports the same per geometry.
+ * No counterpart in the reference. */
 int bem_assembly_status(bem_stream_t stream);
 
 /* Launch-shape knobs of the assembly kernels, set by the autotuner

@@ -40,7 +40,7 @@ EXPORTED = (
     "bem_boundary2potential_noalloc_max", "bem_boundary2potential_noalloc",
     "bem_cmatmul_adjoint", "bem_conj_transpose", "bem_boundary2potential_adjoint", "bem_vertex_gradient",
     "bem_batch_workspace_bytes", "bem_batch_matrices_vk", "bem_set_tuning", "bem_assembly_status", "bem_get_tuning",
-    "bem_boundary_matrices_bm", "bem_batch_matrices_bm",
+    "bem_boundary_matrices_bm", "bem_batch_matrices_bm", "bem_geometry_status", "bem_geometry_release",
 )
 
 
@@ -141,6 +141,8 @@ def lib():
         "bem_get_tuning": ([i], i),
         "bem_boundary_matrices_bm": ([vp, i, f, vp, vp, vp], i),
         "bem_batch_matrices_bm": ([P(BmProblem), i, i, vp, sz, vp], i),
+        "bem_geometry_status": ([vp, vp], i),
+        "bem_geometry_release": ([vp], i),
     }
     for name, (argt, rest) in sigs.items():
         fn = getattr(L, name)

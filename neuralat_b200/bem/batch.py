@@ -100,6 +100,29 @@ def problem_bytes(nv: int, m: int, restart: int = 200) -> int:
 FORMULATIONS = ("cbie", "burton_miller")
 
 
+def plan_waves(sizes, budget: int, concurrency) -> list:
+    """Group jobs into waves: ``sizes`` is a list of (job, nv, bytes) in the
+    order the jobs should run; a wave holds jobs of one concurrency class
+    (``concurrency(nv)``) whose bytes fit ``budget`` together.  Returns
+    [(jobs, concurrency)].  Raises ``MemoryError`` (before anything is
+    allocated) when one job alone needs more than the budget."""
+    waves, wave, used, conc = [], [], 0, None
+    for job, nv, b in sizes:
+        if b > budget:
+            raise MemoryError(f"a problem of {nv} unknowns needs {b / 2**30:.2f} GiB of device memory, more than "
+                              f"the batch budget of {budget / 2**30:.2f} GiB")
+        c = concurrency(nv)
+        if wave and (used + b > budget or c != conc):
+            waves.append((wave, conc))
+            wave, used = [], 0
+        wave.append(job)
+        used += b
+        conc = c
+    if wave:
+        waves.append((wave, conc))
+    return waves
+
+
 class BatchRunner:
     """Run a list of meshes x wavenumbers x RHS through the GPU in waves.
 
@@ -114,7 +137,9 @@ class BatchRunner:
         if memory_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget_bytes = int(0.6 * free)
-        self.budget = memory_budget_bytes
+        if memory_budget_bytes <= 0:
+            raise ValueError("memory_budget_bytes must be positive")
+        self.budget = int(memory_budget_bytes)
         self.workers = max(1, workers)
         self.precision, self.rtol, self.restart = precision, rtol, restart
         self.formulation, self.max_iters = formulation, max_iters
@@ -198,21 +223,19 @@ class BatchRunner:
         # largest first: big problems start early and small ones fill the tail
         jobs.sort(key=lambda j: -solvers[j[0]].geometry.nv)
         res = BatchResult()
-        # waves: one size class (same concurrency) and within the memory budget
-        wave, used, conc = [], 0, None
-        waves = []
-        for j in jobs:
-            nv = solvers[j[0]].geometry.nv
-            b = problem_bytes(nv, neumann(*j).shape[1], self.restart)
-            c = self.concurrency(nv)
-            if wave and (used + b > self.budget or c != conc):
-                waves.append((wave, conc))
-                wave, used = [], 0
-            wave.append(j)
-            used += b
-            conc = c
-        if wave:
-            waves.append((wave, conc))
+        # waves: one size class (same concurrency) and within the memory budget,
+        # which must itself fit the device: a budget above the free memory is
+        # an error here, not an out-of-memory failure in the middle of a wave
+        free, _ = torch.cuda.mem_get_info(dev)
+        budget = self.budget
+        sizes = [(j, solvers[j[0]].geometry.nv,
+                  problem_bytes(solvers[j[0]].geometry.nv, neumann(*j).shape[1], self.restart)) for j in jobs]
+        waves = plan_waves(sizes, budget, self.concurrency)
+        bytes_of = {j: b for j, _, b in sizes}
+        peak = max(sum(bytes_of[j] for j in w) for w, _ in waves)
+        if peak > free:
+            raise MemoryError(f"a wave needs {peak / 2**30:.2f} GiB of device memory but only {free / 2**30:.2f} GiB "
+                              f"are free: lower memory_budget_bytes (now {budget / 2**30:.2f} GiB)")
         for wave, conc in waves:
             t0 = time.perf_counter()
             ss = [solvers[mi] for mi, _ in wave]
@@ -238,6 +261,8 @@ class BatchRunner:
             for lane, f in zip([ln for ln in lanes if ln], futs):
                 for i, r in zip(lane, f.result()):
                     out[i] = r
+            for sv in {id(x): x for x in ss}.values():  # a bounded wait of the wave's assembly expired?
+                sv.geometry.check_status()
             for (mi, ki), (u, p, info) in zip(wave, out):
                 res.dirichlet.append(u)
                 res.pressure.append(p)

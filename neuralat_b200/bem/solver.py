@@ -81,6 +81,23 @@ class Geometry:
     def ptr(self) -> ctypes.c_void_p:
         return _vp(self.buffer)
 
+    def check_status(self) -> None:
+        """Raise ``BEMError`` (BEM_ERR_CUDA) if a bounded wait of an assembly
+        kernel expired on this geometry since the last check (the matrices
+        assembled meanwhile may be wrong); synchronises the current stream."""
+        with torch.cuda.device(self.device):
+            L.check(L.lib().bem_geometry_status(self.ptr, _stream(self.device)), "assembly on this geometry")
+
+    def __del__(self):
+        # the library caches the header per workspace address: forget it
+        # before the allocator can hand the address to another buffer
+        try:
+            buf = self.__dict__.get("buffer")
+            if buf is not None:
+                L.lib().bem_geometry_release(_vp(buf))
+        except Exception:
+            pass
+
     def normals_and_curls(self):
         normals = torch.empty((self.nt, 3), dtype=torch.float32, device=self.device)
         curls = torch.empty((self.nt, 3, 3), dtype=torch.float32, device=self.device)
@@ -206,24 +223,33 @@ class BEM_Solver:
                                                 _stream(self.device)), f"assemble {layer_type}")
         return out
 
-    def assemble_vk(self, wavenumber, single=True, lhs=True):
-        """Fused assembly: (V, 0.5 I - K); either may be skipped (None)."""
+    def assemble_vk(self, wavenumber, single=True, lhs=True, *, check=True):
+        """Fused assembly: (V, 0.5 I - K); either may be skipped (None).
+
+        With ``check`` (default) the call synchronises and raises
+        ``BEMError`` if a bounded wait of the assembly kernel expired;
+        ``check=False`` leaves that to a later ``self.geometry.check_status()``
+        (the solve paths check once after their solver has synchronised)."""
         V = self._new_matrix() if single else None
         A = self._new_matrix() if lhs else None
         with torch.cuda.device(self.device):
             L.check(L.lib().bem_boundary_matrices_vk(self.geometry.ptr, float(wavenumber), _vp(V), _vp(A), 0.5, -1.0,
                                                      _stream(self.device)), "bem_boundary_matrices_vk")
+        if check:
+            self.geometry.check_status()
         return V, A
 
-    def assemble_bm(self, wavenumber, approx=True):
+    def assemble_bm(self, wavenumber, approx=True, *, check=True):
         """Fused Burton-Miller matrices (bm_lhs + 1/2 I, bm_rhs - (i/(2k)) I),
         one pass; ``approx`` as in ``assemble_boundary_matrix`` (True: the
         <2,3> rules of ``neumann2dirichlet``; False: <4,6>, which is the
-        ``HBIE`` system)."""
+        ``HBIE`` system).  ``check`` as in ``assemble_vk``."""
         lhs, rhs = self._new_matrix(), self._new_matrix()
         with torch.cuda.device(self.device):
             L.check(L.lib().bem_boundary_matrices_bm(self.geometry.ptr, _order(approx), float(wavenumber), _vp(lhs),
                                                      _vp(rhs), _stream(self.device)), "bem_boundary_matrices_bm")
+        if check:
+            self.geometry.check_status()
         return lhs, rhs
 
     def identity_matrix(self):
@@ -237,30 +263,37 @@ class BEM_Solver:
     def CBIE(self, k, neumann, *, precision="fp32", solver="gmres", rtol=1e-5, restart=200, max_iters=1000,
              info: dict | None = None):
         """Exterior Neumann CBIE (solver.py:97-104): (0.5 I - K) u = -V g."""
-        V, lhs = self.assemble_vk(k)
+        V, lhs = self.assemble_vk(k, check=False)
         rhs = -cmatmul(V, neumann.to(torch.complex64))
         del V
         if solver == "bicgstab":
-            return solve_linear_equation(lhs, rhs, solver="bicgstab", tol=rtol * rtol)
-        return gmres(lhs, rhs, rtol=rtol, max_iters=max_iters, restart=restart, precision=precision, info=info)
+            u = solve_linear_equation(lhs, rhs, solver="bicgstab", tol=rtol * rtol)
+        else:
+            u = gmres(lhs, rhs, rtol=rtol, max_iters=max_iters, restart=restart, precision=precision, info=info)
+        self.geometry.check_status()  # the solver has synchronised: a cheap read
+        return u
 
     def HBIE(self, k, neumann, **kw):
         """Hypersingular BIE (solver.py:106-116): 1/2 I - K + (i/k) W and
         -V - (i/k)(K' + 1/2 I) are the Burton-Miller pair at the <4,6>
         rules, assembled in one fused pass."""
-        lhs, rhs_m = self.assemble_bm(k, approx=False)
+        lhs, rhs_m = self.assemble_bm(k, approx=False, check=False)
         rhs = cmatmul(rhs_m, neumann.to(torch.complex64))
         del rhs_m
-        return solve_linear_equation(lhs, rhs, **kw)
+        u = solve_linear_equation(lhs, rhs, **kw)
+        self.geometry.check_status()
+        return u
 
     def neumann2dirichlet(self, k, neumann, **kw):
         """Burton-Miller with the <2,3> rules (solver.py:118-126): the fused
         assembly of (bm_lhs + 1/2 I, bm_rhs - (i/(2k)) I), then
         ``solve_linear_equation`` (same options)."""
-        lhs, rhs_m = self.assemble_bm(k)
+        lhs, rhs_m = self.assemble_bm(k, check=False)
         rhs = cmatmul(rhs_m, neumann.to(torch.complex64))
         del rhs_m
-        return solve_linear_equation(lhs, rhs, **kw)
+        u = solve_linear_equation(lhs, rhs, **kw)
+        self.geometry.check_status()
+        return u
 
     # ---- listeners ----------------------------------------------------------
     def potential_matrix(self, k, points, layer_type="single"):

@@ -288,7 +288,10 @@ struct SymSmem {
   uint64_t tile_full[2];                   // bulk-copy completion of each trial buffer
 };
 
-// A bounded wait of the assembly kernels expired (read by bem_assembly_status).
+// A bounded wait of the assembly kernels expired somewhere in this process
+// (read and cleared by bem_assembly_status).  The waits themselves check the
+// status word of the geometry they assemble (GeomView::err), so an expiry on
+// one geometry does not affect assemblies of other geometries.
 __device__ int g_asm_err;
 
 // Thread 0: bulk-copy trial tile jt (records and vertex table) into buffer b.
@@ -392,8 +395,10 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     const int bf = uses & 1;
     __syncthreads();  // the previous tile's gather is done with the slots and with buffer bf ^ 1
     if (tid == 0 && jt + 1 < jt_end) sym_fetch_tile(sm, g, jt + 1, bf ^ 1);
-    if (!mbar_wait(&sm.tile_full[bf], (uses >> 1) & 1u, &g_asm_err)) {
-      // expired (flag raised): let the copy land before the buffer is reused
+    if (!mbar_wait(&sm.tile_full[bf], (uses >> 1) & 1u, g.err)) {
+      // expired (this geometry's status word raised): record it process-wide
+      // too, and let the copy land before the buffer is reused
+      if (tid == 0) atomicExch(&g_asm_err, 1);
       mbar_wait_drain(&sm.tile_full[bf], (uses >> 1) & 1u);
     }
     const TriRec* trial = sm.trial[bf];

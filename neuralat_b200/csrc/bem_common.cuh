@@ -85,7 +85,7 @@ struct GeomHeader {
   int nv, nt, ntiles;
   int n_edge, n_vert;  // ordered singular pairs sharing 2 / 1 vertices
   int max_valence;
-  int pad;
+  int err;  // status word: set to 1 by an assembly kernel whose bounded wait expired on this geometry
   uint64_t off_vertices;   // float[nv*3] (copy of the input)
   uint64_t off_triangles;  // int[nt*3] (copy of the input)
   uint64_t off_perm;       // int[nt]  sorted position -> triangle id
@@ -115,6 +115,7 @@ struct GeomView {
   const float* normals;
   const float* curls;
   const BmRec* bm;         // sorted order
+  int* err;                // the header's status word (GeomHeader::err)
 };
 
 // Symmetric regular-pair work units (test tile g, trial tile jt >= g) in

@@ -202,8 +202,10 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
     const int bf = uses & 1;
     __syncthreads();  // the previous tile's gather is done with the slots and with buffer bf ^ 1
     if (tid == 0 && jt + 1 < jt_end) bm_fetch_tile(sm, g, jt + 1, bf ^ 1);
-    if (!mbar_wait(&sm.tile_full[bf], (uses >> 1) & 1u, &g_bm_err)) {
-      // expired (flag raised): let the copy land before the buffer is reused
+    if (!mbar_wait(&sm.tile_full[bf], (uses >> 1) & 1u, g.err)) {
+      // expired (this geometry's status word raised): record it process-wide
+      // too, and let the copy land before the buffer is reused
+      if (threadIdx.x == 0) atomicExch(&g_bm_err, 1);
       mbar_wait_drain(&sm.tile_full[bf], (uses >> 1) & 1u);
     }
     const TileRec& tileJ = sm.tileJ[bf];

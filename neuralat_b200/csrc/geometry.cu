@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 #include <unordered_map>
@@ -302,6 +303,11 @@ static void cache_put(const void* geom, const GeomHeader& h) {
   g_cache[geom] = h;
 }
 
+static void cache_drop(const void* geom) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  g_cache.erase(geom);
+}
+
 // Reads the header of a built geometry into a device view (host side).  A
 // geometry built elsewhere (copied buffer) is read back with a blocking copy.
 int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr) {
@@ -338,6 +344,7 @@ int geom_view(const void* geom, GeomView* v, GeomHeader* out_hdr) {
   v->normals = (const float*)(b + h.off_normals);
   v->curls = (const float*)(b + h.off_curls);
   v->bm = (const BmRec*)(b + h.off_bmrec);
+  v->err = (int*)((char*)geom + offsetof(GeomHeader, err));
   if (out_hdr) *out_hdr = h;
   return BEM_OK;
 }
@@ -382,6 +389,25 @@ extern "C" int bem_geometry_build(const float* vertices, int nv, const int* tria
   BEM_CUDA_TRY(cudaGetLastError());
   BEM_CUDA_TRY(cudaStreamSynchronize(s));  // staging buffer is pageable host memory
   cache_put(geom, h);
+  return BEM_OK;
+}
+
+extern "C" int bem_geometry_status(const void* geom, bem_stream_t stream) {
+  GeomView v;
+  int rc = geom_view(geom, &v, nullptr);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  int err = 0;
+  const int zero = 0;
+  BEM_CUDA_TRY(cudaMemcpyAsync(&err, v.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaMemcpyAsync(v.err, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  return err ? BEM_ERR_CUDA : BEM_OK;
+}
+
+extern "C" int bem_geometry_release(const void* geom) {
+  if (!geom) return BEM_ERR_INVALID_ARGUMENT;
+  cache_drop(geom);
   return BEM_OK;
 }
 

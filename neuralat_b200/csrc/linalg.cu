@@ -1763,7 +1763,14 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     BEM_CUDA_TRY(cudaGetLastError());
     return BEM_OK;
   };
-  cudaGraphExec_t step_exec = nullptr;
+  // the captured step is destroyed on every return path (early error returns included)
+  struct ExecGuard {
+    cudaGraphExec_t e = nullptr;
+    ~ExecGuard() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } step_guard;
+  cudaGraphExec_t& step_exec = step_guard.e;
   unsigned long long step_kernels = 0;
   bool step_direct_done = false;  // the first step runs uncaptured (sets kernel attributes)
   HostRing* ring;
@@ -1902,7 +1909,6 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int tc_err = 0;
     if (tc_error(tcws, &tc_err, s) != BEM_OK || tc_err) status = BEM_ERR_CUDA;
   }
-  if (step_exec) cudaGraphExecDestroy(step_exec);
   GmState fin;
   BEM_CUDA_TRY(cudaMemcpyAsync(&fin, P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));
   BEM_CUDA_TRY(cudaStreamSynchronize(s));

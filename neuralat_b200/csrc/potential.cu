@@ -204,21 +204,17 @@ extern "C" size_t bem_boundary2potential_scratch_bytes(int nt, int nrhs) {
   return 2 * sizeof(float2) * (size_t)nt * 6 * (size_t)nrhs;
 }
 
-extern "C" int bem_boundary2potential(const void* geom, const float* points, int np, float k, const void* neumann,
-                                      const void* dirichlet, int nrhs, void* out, void* scratch, size_t scratch_bytes,
-                                      bem_stream_t stream) {
-  GeomView g;
-  int rc = geom_view(geom, &g, nullptr);
-  if (rc) return rc;
-  if (np < 0 || nrhs <= 0 || (np > 0 && (!points || !out))) return BEM_ERR_INVALID_ARGUMENT;
-  if (np == 0) return BEM_OK;
-  if (!scratch || scratch_bytes < bem_boundary2potential_scratch_bytes(g.nt, nrhs)) return BEM_ERR_WORKSPACE;
-  cudaStream_t s = (cudaStream_t)stream;
-  float2* dn = (float2*)scratch;
-  float2* dd = dn + (size_t)g.nt * 6 * nrhs;
+namespace bemb {
+// The densities of both layers at every quadrature point (into dn, dd: 6 nt
+// nrhs complex64 each), then the listener sums: the work of
+// bem_boundary2potential and bem_boundary2potential_noalloc, which differ
+// only in where dn and dd live.
+int b2p_enqueue(const GeomView& g, const float* points, int np, float k, const void* neumann, const void* dirichlet,
+                int nrhs, void* out, float2* dn, float2* dd, cudaStream_t s) {
   const long long total = (long long)g.nt * 6 * nrhs;
   (b2p_density_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, (const float2*)neumann,
-                                                                      (const float2*)dirichlet, nrhs, dn, dd), count_launch());
+                                                                      (const float2*)dirichlet, nrhs, dn, dd),
+   count_launch());
   BEM_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)np * nrhs, s));
   const int nq = 6 * g.nt;
   const int ptiles = (np + 31) / 32;
@@ -236,6 +232,21 @@ extern "C" int bem_boundary2potential(const void* geom, const float* points, int
   }
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
+}
+}  // namespace bemb
+
+extern "C" int bem_boundary2potential(const void* geom, const float* points, int np, float k, const void* neumann,
+                                      const void* dirichlet, int nrhs, void* out, void* scratch, size_t scratch_bytes,
+                                      bem_stream_t stream) {
+  GeomView g;
+  int rc = geom_view(geom, &g, nullptr);
+  if (rc) return rc;
+  if (np < 0 || nrhs <= 0 || (np > 0 && (!points || !out))) return BEM_ERR_INVALID_ARGUMENT;
+  if (np == 0) return BEM_OK;
+  if (!scratch || scratch_bytes < bem_boundary2potential_scratch_bytes(g.nt, nrhs)) return BEM_ERR_WORKSPACE;
+  float2* dn = (float2*)scratch;
+  float2* dd = dn + (size_t)g.nt * 6 * nrhs;
+  return b2p_enqueue(g, points, np, k, neumann, dirichlet, nrhs, out, dn, dd, (cudaStream_t)stream);
 }
 
 extern "C" int bem_triangle2vertex(const void* geom, const void* tri_values, void* out, int* counts,
@@ -322,28 +333,6 @@ extern "C" int bem_boundary2potential_noalloc(const void* geom, const float* poi
   if (np == 0) return BEM_OK;
   float2* base = nullptr;
   if ((rc = noalloc_density(&base))) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
-  float2* dn = base;
-  float2* dd = base + kNoAllocQuadRhs;
-  const long long total = (long long)g.nt * 6 * nrhs;
-  (b2p_density_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, (const float2*)neumann,
-                                                                       (const float2*)dirichlet, nrhs, dn, dd),
-   count_launch());
-  BEM_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)np * nrhs, s));
-  const int nq = 6 * g.nt;
-  const int ptiles = (np + 31) / 32;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int nchunks = (4 * sms * 4 + ptiles - 1) / ptiles;
-  int chunk = (nq + nchunks - 1) / nchunks;
-  chunk = chunk < 256 ? 256 : chunk;
-  nchunks = (nq + chunk - 1) / chunk;
-  for (int r0 = 0; r0 < nrhs; r0 += kB2PRhs) {
-    (b2p_eval_kernel<<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, r0, chunk,
-                                                                    (float2*)out),
-     count_launch());
-  }
-  BEM_CUDA_TRY(cudaGetLastError());
-  return BEM_OK;
+  return b2p_enqueue(g, points, np, k, neumann, dirichlet, nrhs, out, base, base + kNoAllocQuadRhs,
+                     (cudaStream_t)stream);
 }

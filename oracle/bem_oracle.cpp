@@ -406,6 +406,60 @@ int oracle_boundary_matrix(int layer, int line_n, int tri_n, const double* verti
   return 0;
 }
 
+// Selected COLUMNS of the same matrix: output complex128 interleaved, nv x
+// ncols, column c = vertex cols[c] (the trial-vertex side, bind.cu:144-151).
+// Only trial triangles touching a selected vertex contribute, so a few
+// columns cost a few rows' worth of work (used by the finite-difference
+// checker of the vertex gradient, which updates the rows and columns a
+// moved vertex touches).
+int oracle_boundary_matrix_cols(int layer, int line_n, int tri_n, const double* vertices, int nv,
+                                const int* triangles, int nt, double k, const int* cols, int ncols, double* out) {
+  double tmp[12];
+  if (!line_rule(line_n, tmp, tmp + 6) || !tri_rule(tri_n, tmp, tmp + 6)) return 1;
+  if (!cols || ncols <= 0) return 2;
+  Mesh m{vertices, triangles, nv, nt};
+  std::vector<int> slot(nv, -1);
+  for (int c = 0; c < ncols; c++) slot[cols[c]] = c;
+  std::memset(out, 0, sizeof(double) * 2 * (size_t)nv * ncols);
+  std::vector<double> curls(9 * (size_t)nt);
+  std::vector<int> trial;
+  for (int j = 0; j < nt; j++) {
+    int id[3];
+    V3 p[3];
+    m.tri(j, id, p);
+    surface_curls(p, &curls[9 * (size_t)j]);
+    if (slot[id[0]] >= 0 || slot[id[1]] >= 0 || slot[id[2]] >= 0) trial.push_back(j);
+  }
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < nt; i++) {
+    int si[3];
+    V3 ti[3];
+    m.tri(i, si, ti);
+    V3 ni = tri_normal(ti);
+    for (int j : trial) {
+      int sj[3];
+      V3 tj[3];
+      m.tri(j, sj, tj);
+      cplx res[10];
+      if (common_vertices(si, sj) == 0)
+        regular_block(layer, tri_n, ti, tj, k, res);
+      else
+        singular_block(layer, line_n, si, ti, sj, tj, k, res);
+      combine_curls(layer, res, &curls[9 * (size_t)i], &curls[9 * (size_t)j], dot(ni, tri_normal(tj)), k);
+      for (int b = 0; b < 3; b++) {
+        const int c = slot[sj[b]];
+        if (c < 0) continue;
+        for (int a = 0; a < 3; a++) {
+          double* o = out + 2 * ((size_t)si[a] * ncols + c);
+          atomic_add(o, res[3 * a + b].real());
+          atomic_add(o + 1, res[3 * a + b].imag());
+        }
+      }
+    }
+  }
+  return 0;
+}
+
 // One 3x3 pair block (plus the unweighted slot 9), for unit tests of the
 // quadrature itself.  Triangles i and j of the mesh; output 10 complex.
 int oracle_pair_block(int layer, int line_n, int tri_n, const double* vertices, int nv,

@@ -25,7 +25,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 MODULE_NAME = "neuralat_ref_bem"
-DEFAULT_REFERENCE = "/root/reference"
+# The reference checkout: $NEURALAT_REFERENCE, else a directory named
+# "reference" beside this repository.
+DEFAULT_REFERENCE = os.environ.get(
+    "NEURALAT_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 def so_path() -> str:
@@ -79,4 +82,4 @@ def load_prebuilt():
 
 
 if __name__ == "__main__":
-    print(build(verbose=True))
+    print(build(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_REFERENCE, verbose=True))

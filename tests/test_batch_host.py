@@ -29,3 +29,24 @@ def test_problem_bytes_counts_matrices_and_krylov_basis():
     ratio = problem_bytes(2 * n, m, R) / b  # dense matrices quadratic, basis linear in n
     assert 2.0 < ratio <= 4.0
     assert problem_bytes(n, 2 * m, R) > b
+
+
+def test_plan_waves_groups_by_class_and_budget():
+    from neuralat_b200.bem.batch import plan_waves
+
+    def conc(nv):
+        return 2 if nv >= 4096 else 4
+
+    sizes = [("a", 10242, 40), ("b", 10242, 40), ("c", 10242, 40), ("d", 642, 5), ("e", 642, 5)]
+    waves = plan_waves(sizes, budget=100, concurrency=conc)
+    assert waves == [(["a", "b"], 2), (["c"], 2), (["d", "e"], 4)]
+    assert all(sum(b for j, _, b in sizes if j in w) <= 100 for w, _ in waves)
+
+
+def test_plan_waves_refuses_a_problem_above_the_budget():
+    from neuralat_b200.bem.batch import plan_waves
+
+    with pytest.raises(MemoryError):
+        plan_waves([("a", 642, 5), ("b", 10242, 101)], budget=100, concurrency=lambda nv: 1)
+    with pytest.raises(ValueError):
+        BatchRunner(memory_budget_bytes=0)

@@ -91,3 +91,49 @@ def test_recompute_matches_stored():
     _, gx2, gg2 = _adjoint_grads(v, t, k, g, pts, store=False)
     assert np.linalg.norm(gx1 - gx2) / np.linalg.norm(gx1) < 1e-5
     assert np.linalg.norm(gg1 - gg2) / np.linalg.norm(gg1) < 1e-5
+
+
+# ---- the differentiation workload itself: icosphere s4 (N = 2562), 2 kHz, 128 listeners ----
+import os  # noqa: E402
+
+CFG4_FD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cfg4_fd.npz")
+
+
+def _cfg4():
+    w = M.differentiation()
+    return (w["vertices"].astype(np.float32).astype(np.float64), w["triangles"].astype(np.int32), float(w["k"]),
+            w["neumann"].astype(np.complex64).astype(np.complex128), w["points"].astype(np.float32).astype(np.float64))
+
+
+@pytest.fixture(scope="module")
+def cfg4_grads():
+    v, t, k, g, pts = _cfg4()
+    return _adjoint_grads(v, t, k, g, pts)
+
+
+def test_cfg4_gradients_vs_committed_finite_differences(cfg4_grads):
+    """Adjoint gradient at all 64 seeded vertex coordinates and 16 Neumann
+    entries of the s4 workload against FP64 central differences of the
+    oracle (tests/golden/make_cfg4_fd.py): relative error <= 1e-3."""
+    f = np.load(CFG4_FD)
+    loss, gx, gg = cfg4_grads
+    assert abs(loss - float(f["loss"])) / float(f["loss"]) < 1e-4
+    adj_v = np.array([gx[a, c] for a, c in f["coords"]])
+    err_v = np.linalg.norm(adj_v - f["fd_vertices"]) / np.linalg.norm(f["fd_vertices"])
+    assert err_v <= 1e-3, err_v
+    adj_g = np.stack([gg[f["neumann_index"]].real, gg[f["neumann_index"]].imag], axis=1)
+    err_g = np.linalg.norm(adj_g - f["fd_neumann"]) / np.linalg.norm(f["fd_neumann"])
+    assert err_g <= 1e-3, err_g
+
+
+def test_cfg4_vertex_gradient_vs_live_finite_differences(cfg4_grads):
+    """Eight of those coordinates, differenced live on the oracle (base LU
+    plus an exact low-rank update per moved vertex)."""
+    v, t, k, g, pts = _cfg4()
+    F = O.ListenerLoss(v, t, k, g, pts)
+    _, gx, _ = cfg4_grads
+    coords = np.load(CFG4_FD)["coords"][:8]
+    h = 1e-4 * 0.1
+    fd = np.array([(F.vertex_loss(a, c, h) - F.vertex_loss(a, c, -h)) / (2 * h) for a, c in coords])
+    adj = np.array([gx[a, c] for a, c in coords])
+    assert np.linalg.norm(fd - adj) / np.linalg.norm(fd) <= 1e-3

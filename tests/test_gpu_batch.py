@@ -101,6 +101,27 @@ def test_batch_runner_matches_per_problem(solvers):
         assert relfro(p.cpu(), p1.cpu()) <= 1e-4
 
 
+def test_batch_runner_vs_oracle_on_mixed_sizes():
+    """The runner's own output (both formulations' CBIE path, two meshes of
+    different size, two wavenumbers on one of them, tensor-core precision)
+    against the FP64 oracle's dense CBIE solve and listener evaluation."""
+    ms = [_meshes()[0], _meshes()[2]]  # 42 and 162 vertices
+    ks = [[18.3, 90.0], [55.0]]
+    gs = [M.smoothed_gaussian_field(v.shape[0], t, 2, seed=20 + i) for i, (v, t) in enumerate(ms)]
+    pts = M.sphere_points(48, 1.0, seed=7)
+    with BatchRunner(workers=2, precision="fp16x3", rtol=1e-7) as runner:
+        res = runner.run(ms, ks, gs, pts, return_dirichlet=True)
+    for (mi, ki), p, u in zip(res.index, res.pressure, res.dirichlet):
+        v, t = ms[mi]
+        vd = v.astype(np.float32).astype(np.float64)
+        k = float(np.float32(ks[mi][ki]))
+        g = gs[mi].astype(np.complex64)
+        u_ref = O.cbie_solve(vd, t, k, g)
+        p_ref = O.boundary2potential(vd, t, k, g, u_ref, pts.astype(np.float32))
+        assert relfro(u.cpu(), u_ref) <= 1e-4, (mi, ki)
+        assert relfro(p.cpu(), p_ref) <= 1e-4, (mi, ki)
+
+
 def test_autotune_installs_and_caches(solvers, tmp_path, monkeypatch):
     monkeypatch.setenv("NEURALAT_B200_CACHE", str(tmp_path))
     ss = [solvers[1], solvers[2], solvers[3]]

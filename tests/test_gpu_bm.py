@@ -167,6 +167,30 @@ def test_solve_modes_matches_per_mode_loop(precision):
         assert relfro(p[i], p1) <= 1e-5, (i, k)
 
 
+def test_solve_modes_vs_oracle():
+    """EditableModalSound.solve's loop (src/scene.py:384-397) through
+    solve_modes against the FP64 oracle: per mode the <2,3> Burton-Miller
+    system (bm_lhs + 1/2 M) u = (bm_rhs - (i/2k) M) g solved densely
+    (solver.py:118-126), then the listener pressures (solver.py:140-147)."""
+    v, t = ellipsoid(2, (1.0, 0.8, 1.2))
+    vd = v.astype(np.float32).astype(np.float64)
+    s = BEM_Solver(v, t)
+    ks = [M.wavenumber(f) for f in (400.0, 2500.0, 6000.0)]
+    neu = M.smoothed_gaussian_field(v.shape[0], t, 3, seed=8).T.astype(np.complex64)
+    pts = M.sphere_points(40, 1.0, seed=6).astype(np.float32)
+    p = solve_modes(s, ks, torch.from_numpy(neu).cuda(), torch.from_numpy(pts).cuda(), precision="fp32", rtol=1e-7,
+                    workers=2)
+    I = O.identity_matrix(vd, t)
+    for i, k in enumerate(ks):
+        k32 = float(np.float32(k))
+        lhs = O.boundary_matrix("bm_lhs", vd, t, k32, approx="_approx") + 0.5 * I
+        rhs = O.boundary_matrix("bm_rhs", vd, t, k32, approx="_approx") - (0.5j / k32) * I
+        g = neu[i].astype(np.complex128)
+        u = np.linalg.solve(lhs, rhs @ g)
+        p_ref = O.boundary2potential(vd, t, k32, g, u, pts)
+        assert relfro(p[i].cpu().numpy(), p_ref) <= 1e-4, (i, k)
+
+
 def test_high_frequency_assembly_accuracy():
     """10 kHz on an r = 0.3 m ellipsoid (k r up to ~130): the fused V/K and
     Burton-Miller kernels (fast sincos of k r) stay within 1e-5 of the FP64

@@ -1,0 +1,73 @@
+"""The large multi-RHS configuration at full size: icosphere s6 (N = 40 962,
+T = 81 920) with 5 % radial noise, r = 0.2 m, 8 kHz.
+
+Its operators (13.4 GB each in complex64) are beyond the FP64 oracle's reach
+as whole matrices, so the checks are size-independent:
+  * 64 seeded rows of V and of 1/2 M - K against the FP64 oracle's rows,
+    through 16 random projections per row (tests/golden/cfg5_rows.npz, made
+    by tests/golden/make_cfg5_rows.py): relative error <= 1e-5;
+  * an analytic monopole at the centre (exact for any closed surface around
+    the source, scripts/unit_test.py:27-39 of the reference): the listener
+    pressures of the CBIE solve against e^{ikr}/(4 pi r) within the P1
+    discretisation error (<= 2e-2), with the FP64 residual of the solve
+    <= 1e-6.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
+from neuralat_b200.bem import meshes as M
+
+pytestmark = pytest.mark.gpu
+
+ROWS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cfg5_rows.npz")
+
+
+@pytest.fixture(scope="module")
+def large():
+    w = M.large_multi_rhs(m=1)
+    v = w["vertices"].astype(np.float32)
+    t = w["triangles"].astype(np.int32)
+    k = float(w["k"])
+    s = BEM_Solver(v, t)
+    V, A = s.assemble_vk(k)
+    yield w, s, k, V, A
+    del V, A
+    torch.cuda.empty_cache()
+
+
+def test_sampled_rows_match_fp64_oracle(large):
+    w, s, k, V, A = large
+    f = np.load(ROWS)
+    assert int(f["nv"]) == s.geometry.nv and int(f["nt"]) == s.geometry.nt
+    assert abs(float(f["vertex_checksum"]) - float(np.abs(w["vertices"].astype(np.float32).astype(np.float64)).sum())) \
+        <= 1e-9 * float(f["vertex_checksum"])
+    rows = torch.from_numpy(f["rows"].astype(np.int64)).cuda()
+    rng = np.random.default_rng(66)
+    nv = s.geometry.nv
+    Z = (rng.standard_normal((nv, 16)) + 1j * rng.standard_normal((nv, 16))) / np.sqrt(2.0)
+    pv = V[rows].cpu().numpy().astype(np.complex128) @ Z
+    pa = A[rows].cpu().numpy().astype(np.complex128) @ Z
+    assert np.linalg.norm(pv - f["V_proj"]) / np.linalg.norm(f["V_proj"]) <= 1e-5
+    assert np.linalg.norm(pa - f["A_proj"]) / np.linalg.norm(f["A_proj"]) <= 1e-5
+
+
+def test_monopole_known_answer_at_s6(large):
+    w, s, k, V, A = large
+    vd = w["vertices"].astype(np.float32).astype(np.float64)
+    nrm = M.vertex_normals(vd, w["triangles"])
+    r = np.linalg.norm(vd, axis=1)
+    ikr = 1j * k * r
+    g = (-np.exp(ikr) / (4 * np.pi * r ** 3) * (1 - ikr) * np.sum(vd * nrm, axis=1)).astype(np.complex64)
+    gd = torch.from_numpy(g).cuda()
+    info = {}
+    u = gmres(A, -cmatmul(V, gd), rtol=1e-6, precision="fp16x3", info=info)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-6
+    pts = M.sphere_points(256, 1.0, seed=8).astype(np.float32)
+    p = s.boundary2potential(k, gd, u, torch.from_numpy(pts).cuda()).cpu().numpy()
+    rp = np.linalg.norm(pts.astype(np.float64), axis=1)
+    exact = np.exp(1j * k * rp) / (4 * np.pi * rp)
+    assert np.linalg.norm(p - exact) / np.linalg.norm(exact) <= 2e-2

@@ -57,13 +57,30 @@ def test_triangle2vertex(golden):
     assert relfro(out, golden["t2v_out"]) <= 1e-6
 
 
-def test_curls_match_reference_preprocess(golden):
-    """Surface curls used by hypersingular / Burton-Miller (solver.py:40-58)."""
-    v, t = golden["vertices"].astype(np.float64), golden["triangles"]
+def fp64_normals_and_curls(v, t):
+    """Unit normals and surface curls n x grad(phi_b) of the P1 hat functions
+    in FP64: grad phi_b from the inverse metric (J^T J)^-1 of the edge
+    vectors, the quantities of the reference's preprocess (solver.py:40-58)."""
+    v = v.astype(np.float64)
     p0, p1, p2 = v[t[:, 0]], v[t[:, 1]], v[t[:, 2]]
-    n = np.cross(p1 - p0, p2 - p0)
+    e1, e2 = p1 - p0, p2 - p0
+    n = np.cross(e1, e2)
     n /= np.linalg.norm(n, axis=1, keepdims=True)
+    J = np.stack([e1, e2], axis=2)                       # (T, 3, 2)
+    G = np.linalg.inv(np.einsum("tia,tib->tab", J, J))  # (T, 2, 2)
+    d = np.einsum("tia,tab->tib", J, G)                  # columns: grad of the 2nd and 3rd barycentric
+    grads = np.stack([-(d[:, :, 0] + d[:, :, 1]), d[:, :, 0], d[:, :, 1]], axis=1)  # (T, 3 functions, 3)
+    curls = np.cross(n[:, None, :], grads)
+    return n, curls
+
+
+def test_normals_and_curls_match_reference_preprocess(golden):
+    """Unit normals and surface curls (used by the hypersingular and
+    Burton-Miller operators) against the reference's own preprocess output."""
+    n, curls = fp64_normals_and_curls(golden["vertices"], golden["triangles"])
     assert np.abs(n - golden["normals"]).max() < 1e-6
+    scale = np.abs(golden["curls"]).max()
+    assert np.abs(curls - golden["curls"]).max() <= 1e-5 * scale
 
 
 @pytest.mark.parametrize("suffix", SUFFIXES)
