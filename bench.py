@@ -335,7 +335,7 @@ def reference_gpu(v, t, k, g, pts, steps=1):
         e.record()
         return e
 
-    def problem():
+    def problem(tol=1e-10, atol=1e-16):
         e = [ev()]
         normals, curls = reference_preprocess(torch, vt, tt)
         e.append(ev())
@@ -352,7 +352,7 @@ def reference_gpu(v, t, k, g, pts, steps=1):
         us = []
         for j in range(gt.shape[1]):
             solver = BiCGSTAB(lambda x: A @ x)
-            us.append(solver.solve(b[:, j].contiguous(), nsteps=500, tol=1e-10, atol=1e-16))
+            us.append(solver.solve(b[:, j].contiguous(), nsteps=500, tol=tol, atol=atol))
             iters.append(solver.iterations)
         u = torch.stack(us, dim=1)
         del A
@@ -364,18 +364,27 @@ def reference_gpu(v, t, k, g, pts, steps=1):
         torch.cuda.synchronize()
         return e, p, iters
 
-    problem()
-    times, p, iters = [], None, None
-    for _ in range(max(1, steps)):
-        e, p, iters = problem()
-        times.append([e[i].elapsed_time(e[i + 1]) for i in range(len(e) - 1)])
     names = ["preprocess", "assemble", "rhs", "solve", "eval"]
-    stage_ms = {n: float(np.mean([tm[i] for tm in times])) for i, n in enumerate(names)}
-    return {"s_per_problem": sum(stage_ms.values()) / 1e3, "stages_ms": stage_ms, "steps": len(times),
-            "bicgstab_iterations": iters,
-            "listener_err_vs_fp64": listener_error_vs_fixture(v, t, k, g, p, None).get("mixed"),
-            "what": "reference src/bem kernels (bind.cu, unmodified, oracle/_ref) + torch/cuBLAS + the reference's "
-                    "BiCGSTAB per RHS with its defaults; FP32; one B200"}
+
+    def timed(**kw):
+        problem(**kw)
+        times, p, iters = [], None, None
+        for _ in range(max(1, steps)):
+            e, p, iters = problem(**kw)
+            times.append([e[i].elapsed_time(e[i + 1]) for i in range(len(e) - 1)])
+        stage_ms = {n: float(np.mean([tm[i] for tm in times])) for i, n in enumerate(names)}
+        return {"s_per_problem": sum(stage_ms.values()) / 1e3, "stages_ms": stage_ms, "steps": len(times),
+                "bicgstab_iterations": iters,
+                "listener_err_vs_fp64": listener_error_vs_fixture(v, t, k, g, p, None).get("mixed")}
+
+    out = timed()
+    out["what"] = ("reference src/bem kernels (bind.cu, unmodified, oracle/_ref) + torch/cuBLAS + the reference's "
+                   "BiCGSTAB per RHS with its defaults (tol 1e-10 on ||r||^2/||b||^2, atol 1e-16 on ||r||^2: on this "
+                   "workload's scale the absolute test stops it near relative residual 1e-3); FP32; one B200")
+    # the same path with the absolute test off, so that only the relative one
+    # (1e-5 in ||r||) stops it: the reference's own kernels at their best accuracy
+    out["relative_tol_only"] = timed(atol=0.0)
+    return out
 
 
 def run_reference(args):
@@ -536,7 +545,7 @@ def run_ours(args):
             del A
             S = s.potential_matrix(k, p_d, "single")
             D = s.potential_matrix(k, p_d, "double")
-            return -cmatmul(S, g_d) + cmatmul(D, u)
+            return -(S @ g_d) + D @ u  # (P x N) products as the reference forms them (solver.py:147)
 
         plain_step()
         torch.cuda.synchronize()
@@ -869,8 +878,12 @@ def validate_large(w, v, t, g, pts, k, u, precision):
         made by tests/golden/make_cfg5_rows.py);
       * per right-hand side, the FP64 residual ||b - A x|| / ||b|| of the
         timed solution against the FP32-stored operator;
-      * an analytic monopole at the centre as one more right-hand side: the
-        listener pressures against e^{ikr}/(4 pi r) (P1 discretisation error)."""
+      * an analytic monopole at the centre of the same-size sphere without the
+        radial noise (icosphere s6, r = 0.2 m, same k): the listener pressures
+        against e^{ikr}/(4 pi r) (P1 discretisation error).  On the noisy
+        surface itself neighbouring vertices differ in radius by up to 2 cm,
+        k x 2 cm ~ 3 rad, so the monopole's surface field is not resolved
+        there and its error says nothing about the solver."""
     import torch
 
     from neuralat_b200.bem import BEM_Solver, cmatmul, gmres
@@ -902,14 +915,18 @@ def validate_large(w, v, t, g, pts, k, u, precision):
         del blk
     rel = (r2.sqrt() / b.to(torch.complex128).abs().pow(2).sum(dim=0).sqrt()).cpu().numpy()
     out["fp64_residual_per_rhs"] = {"max": float(rel.max()), "median": float(np.median(rel)), "all": rel.tolist()}
+    del V, A, s, b, u64
+    torch.cuda.empty_cache()
     # analytic monopole (exact for any closed surface around the source)
-    vd = w["vertices"].astype(np.float32).astype(np.float64)
-    nrm = M.vertex_normals(vd, w["triangles"])
-    d = vd
-    rr = np.linalg.norm(d, axis=1)
+    vs, ts = M.icosphere(6, 0.2)
+    vd = vs.astype(np.float32).astype(np.float64)
+    nrm = M.vertex_normals(vd, ts)
+    rr = np.linalg.norm(vd, axis=1)
     ikr = 1j * k * rr
-    gm = (-np.exp(ikr) / (4 * np.pi * rr ** 3) * (1 - ikr) * np.sum(d * nrm, axis=1)).astype(np.complex64)
+    gm = (-np.exp(ikr) / (4 * np.pi * rr ** 3) * (1 - ikr) * np.sum(vd * nrm, axis=1)).astype(np.complex64)
     gm_d = torch.from_numpy(gm).cuda()
+    s = BEM_Solver(vs.astype(np.float32), ts)
+    V, A = s.assemble_vk(k)
     um = gmres(A, -cmatmul(V, gm_d), rtol=1e-6, precision=precision)
     pm = s.boundary2potential(k, gm_d, um, pts).cpu().numpy()
     pp = pts.cpu().numpy().astype(np.float64)

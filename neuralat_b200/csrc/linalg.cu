@@ -1808,7 +1808,9 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     max_rel = 0.0;
     for (int c = 0; c < m; c++) {
       const double bn = std::sqrt(hb[c]), rn = std::sqrt(hres[c]);
-      const double rel = bn > 0.0 ? rn / bn : (rn > 0.0 ? INFINITY : 0.0);
+      // a NaN or Inf anywhere in b or in the residual makes its norm non-finite
+      const double rel = !(std::isfinite(bn) && std::isfinite(rn)) ? NAN
+                                                                     : (bn > 0.0 ? rn / bn : (rn > 0.0 ? INFINITY : 0.0));
       if (!std::isfinite(rel)) {
         status = BEM_ERR_NONFINITE;
         done = true;

