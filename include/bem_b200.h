@@ -188,8 +188,16 @@ enum {
   BEM_TUNE_GMRES_REORTH = 4,         /* Arnoldi Gram-Schmidt passes: 0 automatic (one), 1 one, 2 two */
   BEM_TUNE_ARNOLDI_CLUSTER = 5,      /* largest thread-block cluster (<= 16 CTAs) per Krylov column in
                                         the Arnoldi kernel (0: automatic) */
-  BEM_TUNE_ARNOLDI_MODE = 6          /* Arnoldi step: 0 automatic, 1 one cluster kernel per step,
-                                        2 three streamed kernels over all SMs (large n) */
+  BEM_TUNE_ARNOLDI_MODE = 6,         /* Arnoldi step: 0 automatic (3 when its grid fits, else 1),
+                                        1 one cluster kernel per step, 2 streamed kernels over all SMs,
+                                        3 one cooperative kernel over all SMs (two grid barriers) */
+  BEM_TUNE_TC_WAIT_US = 7,           /* limit of each bounded wait in the tensor-core matvec, microseconds
+                                        (0: 2 s) */
+  BEM_TUNE_TC_TEST_SKIP_FILL = 8     /* test hook for the bounded waits, one launch: value v > 0 makes CTA 0
+                                        of the next tensor-core matvec leave its (v-1)-th pipeline fill
+                                        unissued, so the consumer's wait expires, the kernel drains its
+                                        copies and returns, and bem_tc_status reports BEM_ERR_CUDA
+                                        (no fault, no hang); 0 = off */
 };
 int bem_set_tuning(int key, int value);
 int bem_get_tuning(int key);
@@ -304,7 +312,8 @@ int bem_tc_operator_prepare(const void* A, int n, int precision, void* workspace
 int bem_tc_matmul(const void* workspace, size_t workspace_bytes, int n, int precision, const void* X, int m,
                   void* Y, bem_stream_t stream);
 /* BEM_OK, or BEM_ERR_CUDA if a tensor-core kernel on this workspace gave up
- * a bounded wait (synchronises `stream`). */
+ * a bounded wait since the last call (its output is then not usable);
+ * clears the flag and synchronises `stream`. */
 int bem_tc_status(const void* workspace, bem_stream_t stream);
 
 /* Workspace bytes for bem_gmres_solve (n unknowns, m right-hand sides). */

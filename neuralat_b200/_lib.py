@@ -53,6 +53,8 @@ class BEMError(RuntimeError):
 
 TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE, TUNE_GMRES_REORTH, TUNE_ARNOLDI_CLUSTER = 1, 2, 3, 4, 5
 TUNE_ARNOLDI_MODE = 6
+TUNE_TC_WAIT_US = 7
+TUNE_TC_TEST_SKIP_FILL = 8
 
 
 class BatchProblem(ctypes.Structure):

@@ -44,6 +44,8 @@ extern int g_tc_promote;    // tensor-core matvec accumulator segment (tc_matvec
 extern int g_gmres_reorth;  // Gram-Schmidt passes of the Arnoldi step (linalg.cu)
 extern int g_arn_max_cluster;  // largest Arnoldi cluster size (linalg.cu)
 extern int g_arn_mode;         // Arnoldi step variant (linalg.cu)
+extern int g_tc_wait_us;       // bounded-wait limit of the tensor-core kernels (tc_matvec.cu)
+extern std::atomic<int> g_tc_skip_fill;  // test hook of the tensor-core kernel (tc_matvec.cu)
 
 namespace {
 extern int g_tune_chunk;
@@ -1039,8 +1041,14 @@ int set_tuning(int key, int value) {
       g_arn_max_cluster = value;
       return BEM_OK;
     case BEM_TUNE_ARNOLDI_MODE:
-      if (value > 2) return BEM_ERR_INVALID_ARGUMENT;
+      if (value > 3) return BEM_ERR_INVALID_ARGUMENT;
       g_arn_mode = value;
+      return BEM_OK;
+    case BEM_TUNE_TC_WAIT_US:
+      g_tc_wait_us = value;
+      return BEM_OK;
+    case BEM_TUNE_TC_TEST_SKIP_FILL:
+      g_tc_skip_fill.store(value);
       return BEM_OK;
   }
   return BEM_ERR_INVALID_ARGUMENT;
@@ -1054,6 +1062,8 @@ int get_tuning(int key) {
     case BEM_TUNE_GMRES_REORTH: return g_gmres_reorth;
     case BEM_TUNE_ARNOLDI_CLUSTER: return g_arn_max_cluster;
     case BEM_TUNE_ARNOLDI_MODE: return g_arn_mode;
+    case BEM_TUNE_TC_WAIT_US: return g_tc_wait_us;
+    case BEM_TUNE_TC_TEST_SKIP_FILL: return g_tc_skip_fill.load();
   }
   return -1;
 }

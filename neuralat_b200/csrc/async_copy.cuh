@@ -37,15 +37,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait: false (and *err raised) if the phase did not complete within
-// kWaitLimitNs; returns false at once once *err is set by anyone.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// limit_ns; returns false at once once *err is set by anyone.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   for (uint32_t it = 0;; it++) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255u) == 0u) {
       if (*(volatile int*)err) return false;
-      if (globaltimer() - t0 > kWaitLimitNs) {
+      if (globaltimer() - t0 > limit_ns) {
         atomicExch(err, 1);
         return false;
       }
@@ -54,11 +55,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
 }
 
 // Bounded wait that ignores the error flag (draining copies before exit).
-__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity,
+                                                unsigned long long limit_ns = kWaitLimitNs) {
   const unsigned long long t0 = globaltimer();
   for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (globaltimer() - t0 > kWaitLimitNs) return false;
+    if (globaltimer() - t0 > limit_ns) return false;
   }
 }
 

@@ -36,13 +36,14 @@ namespace cg = cooperative_groups;
 
 int g_gmres_reorth = 0;     // Gram-Schmidt passes: 0 automatic, 1 one pass (CGS), 2 two passes (CGS2); a tuning knob
 int g_arn_max_cluster = 0;  // largest Arnoldi cluster size tried (0: 16); a tuning knob
-int g_arn_mode = 0;         // Arnoldi step: 0 automatic, 1 cluster kernel, 2 streamed kernels; a tuning knob
+int g_arn_mode = 0;         // Arnoldi step: 0 automatic, 1 cluster kernel, 2 streamed kernels, 3 cooperative
+                            // kernel; a tuning knob
 
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
 int tc_matvec(const void* ws, int n, int precision, const float2* X, int m, float2* Y, const int* active,
               cudaStream_t s);
-int tc_error(const void* ws, int* err_host, cudaStream_t s);
+int tc_error(const void* ws, int* err_host, cudaStream_t s, bool clear);
 size_t tc_workspace_bytes(int n, int m, int precision);
 int tc_b_planes(void* ws, int n, int m, int precision, __nv_bfloat16** bh, __nv_bfloat16** bl, int* ldb, int* nb,
                 float** cinv);
@@ -497,8 +498,10 @@ int launch_cgemv(const float2* A, int n, const float2* X, int m, float2* Y, cons
 // GMRES state and kernels
 // ---------------------------------------------------------------------------
 struct GmState {
-  int err;  // a bounded wait of gm_arnoldi_kernel expired
-  int pad[3];
+  int err;             // a bounded wait of an Arnoldi kernel expired
+  unsigned bar_count;  // grid barrier of the cooperative step: arrivals
+  unsigned bar_gen;    // and generation
+  int pad;
 };
 
 // Host-mapped ring of per-step column activity (kSnapRing steps x m ints),
@@ -1242,6 +1245,452 @@ __global__ void __launch_bounds__(32) gm_st_givens_kernel(GmPtrs P) {
   if (lane == 0) column_done(P, s, k + 1, still);
 }
 
+// ---------------------------------------------------------------------------
+// Cooperative Arnoldi step (one classical Gram-Schmidt pass): ONE launch of a
+// cooperative grid over all SMs, every CTA resident and owning a contiguous
+// range of unknowns for every column, with two grid-wide barriers:
+//   load    w = Y over the CTA's unknowns (FP64, shared memory); Y = 0 for
+//           the next accumulating matvec
+//   dots    h = V^H w.  Work items are (column, 4 basis rows); each compute
+//           warp takes every 8th item and streams its rows of the CTA's
+//           unknowns through its own ring of shared-memory slots with 1-D
+//           bulk async copies (mbarrier completion, bounded waits), its lane
+//           0 issuing ahead, so a whole ring of copies is in flight per warp.
+//           Lanes own unknown pairs: FP64 products (exact for the FP32
+//           basis), a warp reduce-scatter, FP64 atomics into the column's h
+//           (P.hacc, by the column's step parity).
+//   == grid barrier ==  (the ring already holds the first rows of the next pass)
+//   update  w' = w - V h, the same items and ring (h read from L2, every
+//           lane the same address), contributions subtracted from w in
+//           shared memory with FP64 shared atomics; |w'|^2 per column, FP64
+//           atomics (P.nacc).  Meanwhile the Givens warp of the CTA that owns
+//           the column (CTA c: columns c, c + G, ...) applies its previous
+//           rotations to h, which is inherently sequential.
+//   == grid barrier ==
+//   finish  v_{k+1} = w' / |w'| -> basis and the next matvec operand; the
+//           Givens warp adds the new rotation, the residual estimate and the
+//           step record (k + 1, activity, host-mapped snapshot)
+// Every CTA streams the same number of basis bytes; a step costs one launch
+// and two barriers.  Barrier and copy waits are bounded (P.st->err on expiry;
+// copies still in flight are drained before the CTA exits).
+// ---------------------------------------------------------------------------
+constexpr int kCoComputeWarps = 8;
+constexpr int kCoCompute = 32 * kCoComputeWarps;  // 256 compute threads
+constexpr int kCoThreads = kCoCompute + 32;       // + the Givens warp
+constexpr int kCoRows = 4;                        // basis rows per work item
+constexpr int kCoMaxColsPerCta = 4;               // columns whose rotations one CTA applies
+constexpr unsigned long long kCoWaitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier of the cooperative step (all CTAs resident).  Thread 0
+// of each CTA arrives; the last one resets the count and advances the
+// generation.  The wait is bounded: on expiry (or once anyone raised the
+// error flag) the CTA goes on and P.st->err is set, so the solve reports
+// BEM_ERR_CUDA instead of hanging.
+__device__ __forceinline__ void co_grid_sync(GmState* st) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned gen = ld_acquire_u32(&st->bar_gen);
+    __threadfence();  // this CTA's writes and atomics before the arrival
+    const unsigned arrived = atomicAdd(&st->bar_count, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      const unsigned long long t0 = globaltimer();
+      for (unsigned it = 0;; it++) {
+        if (ld_acquire_u32(&st->bar_gen) != gen) break;
+        if ((it & 31u) == 0u) {
+          if (*(volatile int*)&st->err) break;
+          if (globaltimer() - t0 > kCoWaitNs) {
+            atomicExch(&st->err, 1);
+            break;
+          }
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();  // the other CTAs' writes are visible after the barrier
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void co_compute_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCoCompute) : "memory"); }
+
+// Dynamic shared memory: ks[m] act[m] | wsm[m][2 npc] | nsm[m] | full[8][slots]
+// | ring[8][slots][kCoRows][2 npc] | per owned column: hc[R+1], snv[R]
+// (double2), csv[R], misc[2] (double2, 16-byte aligned).
+struct CoLayout {
+  size_t ks, act, wsm, nsm, full, ring, giv, total;
+  int giv_stride;  // bytes of one column's Givens scratch
+  int slot_floats;  // float2 entries of one ring slot
+};
+__host__ __device__ inline CoLayout co_layout(int m, int npc, int R, int cpc, int slots) {
+  CoLayout L;
+  size_t o = 0;
+  auto take = [&](size_t b) {
+    const size_t r = o;
+    o = (o + b + 15) / 16 * 16;
+    return r;
+  };
+  L.ks = take(sizeof(int) * m);
+  L.act = take(sizeof(int) * m);
+  L.wsm = take(sizeof(double2) * (size_t)m * 2 * npc);
+  L.nsm = take(sizeof(double) * m);
+  L.full = take(sizeof(uint64_t) * kCoComputeWarps * slots);
+  L.slot_floats = kCoRows * 2 * npc;
+  L.ring = take(sizeof(float2) * (size_t)L.slot_floats * kCoComputeWarps * slots);
+  L.giv_stride = (int)((sizeof(double2) * (R + 1) + sizeof(double2) * R + sizeof(double) * R + 16 +
+                        2 * sizeof(double2) + 15) / 16 * 16);
+  L.giv = take((size_t)L.giv_stride * cpc);
+  L.total = o;
+  return L;
+}
+
+__device__ __forceinline__ double2* co_misc(double* csv, int R) {
+  return reinterpret_cast<double2*>(((uintptr_t)(csv + R) + 15) & ~(uintptr_t)15);
+}
+
+// The work items of a pass: (column s, rows 4c .. 4c+3), it = s nch + c,
+// present when the column is active and 4c <= k_s.
+struct CoItems {
+  const int* ks;
+  const int* act;
+  int nch, total;
+  __device__ bool valid(int it) const {
+    const int s = it / nch, c = it - s * nch;
+    return act[s] && kCoRows * c <= ks[s];
+  }
+  // the first valid item at or after `it` in this warp's sequence (stride 8)
+  __device__ int next(int it) const {
+    while (it < total && !valid(it)) it += kCoComputeWarps;
+    return it;
+  }
+};
+
+__global__ void __launch_bounds__(kCoThreads, 1)
+    gm_arnoldi_coop_kernel(GmPtrs P, int npc, int cpc, int slots) {
+  extern __shared__ __align__(16) unsigned char co_raw[];
+  const int m = P.m, R = P.R;
+  const CoLayout Lo = co_layout(m, npc, R, cpc, slots);
+  int* ks = reinterpret_cast<int*>(co_raw + Lo.ks);
+  int* act = reinterpret_cast<int*>(co_raw + Lo.act);
+  double2* wsm = reinterpret_cast<double2*>(co_raw + Lo.wsm);
+  double* nsm = reinterpret_cast<double*>(co_raw + Lo.nsm);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool giv_warp = warp == kCoComputeWarps;
+  const int npairs_all = (P.n + 1) / 2;
+  const int p_begin = blockIdx.x * npc;
+  const int nvp = max(0, min(npc, npairs_all - p_begin));  // valid pairs of this CTA
+  const int i0 = 2 * p_begin;
+  const int rows = 2 * npc;  // wsm row stride and ring row stride (float2)
+
+  for (int s = tid; s < m; s += kCoThreads) {
+    ks[s] = P.kcol[s];
+    act[s] = P.active[s];
+  }
+  if (tid < kCoComputeWarps * slots) mbar_init(reinterpret_cast<uint64_t*>(co_raw + Lo.full) + tid, 1);
+  mbar_init_fence();
+  __syncthreads();
+  int kmax = -1;
+  for (int s = 0; s < m; s++)
+    if (act[s]) kmax = max(kmax, ks[s]);
+  CoItems items;
+  items.ks = ks;
+  items.act = act;
+  items.nch = kmax >= 0 ? kmax / kCoRows + 1 : 1;
+  items.total = (kmax >= 0 && nvp > 0) ? m * items.nch : 0;
+
+  // this warp's ring: slot q holds kCoRows rows of 2 nvp unknowns (row stride 2 npc)
+  uint64_t* full = reinterpret_cast<uint64_t*>(co_raw + Lo.full) + (giv_warp ? 0 : warp) * slots;
+  float2* ring = reinterpret_cast<float2*>(co_raw + Lo.ring) + (size_t)(giv_warp ? 0 : warp) * slots * Lo.slot_floats;
+  const uint64_t pol = l2_evict_last_policy();
+  const uint32_t row_bytes = (uint32_t)nvp * 16u;
+  // the warp's sequence: its items of the dots pass, then the same items again for the update pass
+  int iss = giv_warp ? items.total : items.next(warp), iss_pass = 0;  // next item to issue, and its pass
+  unsigned nissued = 0, nconsumed = 0;
+  auto issue = [&]() {  // lane 0: bulk-copy the next item of the sequence into its slot
+    if (iss_pass > 1) return;
+    if (lane == 0) {
+      const int s = iss / items.nch, c = iss - s * items.nch;
+      const int l0 = kCoRows * c, nl = min(kCoRows, ks[s] + 1 - l0);
+      uint64_t* bar = &full[nissued % slots];
+      float2* dst = ring + (size_t)(nissued % slots) * Lo.slot_floats;
+      mbar_expect_tx(bar, row_bytes * (uint32_t)nl);
+      for (int li = 0; li < nl; li++) bulk_load_hint(dst + (size_t)li * rows, vrow(P, s, l0 + li) + i0, row_bytes, bar, pol);
+    }
+    nissued++;
+    iss = items.next(iss + kCoComputeWarps);
+    if (iss >= items.total && iss_pass == 0) {
+      iss_pass = 1;
+      iss = items.next(warp);
+    } else if (iss >= items.total) {
+      iss_pass = 2;
+    }
+  };
+  // consumer: wait for the next slot.  If the bounded wait expires (the error
+  // flag is raised) it still lets the copy land, so the slot accounting stays
+  // in step and no copy is left in flight; false only if that drain expires too.
+  auto acquire = [&](const float2** rowsp) -> bool {
+    const unsigned q = nconsumed % slots;
+    const uint32_t par = (nconsumed / slots) & 1u;
+    bool ok = mbar_wait(&full[q], par, &P.st->err);
+    if (!ok) ok = mbar_wait_drain(&full[q], par);
+    *rowsp = ring + (size_t)q * Lo.slot_floats;
+    return ok;
+  };
+
+  // ---- load w = Y (all columns; Y cleared), clear the next step's sums ----
+  if (!giv_warp) {
+    for (int d = 0; d < slots && iss_pass < 2 && items.total > 0; d++) issue();  // rows start landing now
+    for (int t = tid; t < 2 * npc * m; t += kCoCompute) {
+      const int il = t / m, s = t - il * m;
+      const int i = i0 + il;
+      double2 w = make_double2(0.0, 0.0);
+      if (il < 2 * nvp && i < P.n) {
+        float2* y = P.Y + (size_t)i * m + s;
+        const float2 yv = *y;
+        w = make_double2(yv.x, yv.y);
+        *y = make_float2(0.f, 0.f);
+      }
+      wsm[(size_t)s * rows + il] = w;
+    }
+    // the sums of the next step (other parity) start from zero; nobody reads them now
+    const size_t per = 2 * (size_t)(R + 1);
+    for (size_t t = (size_t)blockIdx.x * kCoCompute + tid; t < (size_t)m * (per + 1);
+         t += (size_t)gridDim.x * kCoCompute) {
+      const int s = (int)(t / (per + 1));
+      const size_t j = t - (size_t)s * (per + 1);
+      const int nb = (ks[s] & 1) ^ 1;
+      if (j < per)
+        st_hacc(P, nb, s, 0)[j] = 0.0;
+      else
+        *st_nacc(P, nb, s, 1) = 0.0;
+    }
+  }
+  __syncthreads();
+
+  // ---- dots: h += V^H w over this CTA's unknowns ----
+  if (!giv_warp) {
+    for (int it = items.next(warp); it < items.total; it = items.next(it + kCoComputeWarps)) {
+      const int s = it / items.nch, c = it - s * items.nch;
+      const int l0 = kCoRows * c, nl = min(kCoRows, ks[s] + 1 - l0);
+      const float2* rw;
+      const bool ok = acquire(&rw);
+      double v[2 * kCoRows];
+#pragma unroll
+      for (int q = 0; q < 2 * kCoRows; q++) v[q] = 0.0;
+      if (ok) {
+        const double2* ws = wsm + (size_t)s * rows;
+        for (int p = lane; p < nvp; p += 32) {
+          const bool pad = i0 + 2 * p + 1 >= P.n;
+          const double2 w0 = ws[2 * p], w1 = ws[2 * p + 1];
+#pragma unroll
+          for (int li = 0; li < kCoRows; li++) {
+            if (li < nl) {
+              float4 a = *reinterpret_cast<const float4*>(rw + (size_t)li * rows + 2 * p);
+              if (pad) {
+                a.z = 0.f;
+                a.w = 0.f;
+              }
+              const double ax = a.x, ay = a.y, az = a.z, aw = a.w;
+              v[2 * li] = fma(ax, w0.x, fma(ay, w0.y, fma(az, w1.x, fma(aw, w1.y, v[2 * li]))));
+              v[2 * li + 1] = fma(ax, w0.y, fma(-ay, w0.x, fma(az, w1.y, fma(-aw, w1.x, v[2 * li + 1]))));
+            }
+          }
+        }
+      }
+      __syncwarp();  // every lane is done with the slot
+      nconsumed++;
+      issue();
+      const double tsum = warp_reduce_scatter<2 * kCoRows>(v, lane);
+      if ((lane & 3) == 0 && (lane >> 2) < 2 * nl && tsum != 0.0)
+        atomicAdd(st_hacc(P, ks[s] & 1, s, 0) + 2 * l0 + (lane >> 2), tsum);
+    }
+  }
+  co_grid_sync(P.st);
+
+  // ---- update (compute warps) and the previous rotations (Givens warp) ----
+  if (!giv_warp) {
+    for (int it = items.next(warp); it < items.total; it = items.next(it + kCoComputeWarps)) {
+      const int s = it / items.nch, c = it - s * items.nch;
+      const int l0 = kCoRows * c, nl = min(kCoRows, ks[s] + 1 - l0);
+      const double* hp = st_hacc(P, ks[s] & 1, s, 0) + 2 * l0;
+      double2 h[kCoRows];
+#pragma unroll
+      for (int li = 0; li < kCoRows; li++)
+        h[li] = li < nl ? make_double2(__ldcg(hp + 2 * li), __ldcg(hp + 2 * li + 1)) : make_double2(0.0, 0.0);
+      const float2* rw;
+      const bool ok = acquire(&rw);
+      if (ok) {
+        double2* ws = wsm + (size_t)s * rows;
+        for (int p = lane; p < nvp; p += 32) {
+          const bool pad = i0 + 2 * p + 1 >= P.n;
+          double2 d0 = make_double2(0.0, 0.0), d1 = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int li = 0; li < kCoRows; li++) {
+            if (li < nl) {
+              float4 v = *reinterpret_cast<const float4*>(rw + (size_t)li * rows + 2 * p);
+              if (pad) {
+                v.z = 0.f;
+                v.w = 0.f;
+              }
+              const double2 cc = h[li];
+              d0.x = fma((double)v.x, cc.x, fma(-(double)v.y, cc.y, d0.x));
+              d0.y = fma((double)v.x, cc.y, fma((double)v.y, cc.x, d0.y));
+              d1.x = fma((double)v.z, cc.x, fma(-(double)v.w, cc.y, d1.x));
+              d1.y = fma((double)v.z, cc.y, fma((double)v.w, cc.x, d1.y));
+            }
+          }
+          atomicAdd(&ws[2 * p].x, -d0.x);
+          atomicAdd(&ws[2 * p].y, -d0.y);
+          atomicAdd(&ws[2 * p + 1].x, -d1.x);
+          atomicAdd(&ws[2 * p + 1].y, -d1.y);
+        }
+      }
+      __syncwarp();
+      nconsumed++;
+      issue();
+    }
+    for (int s = tid; s < m; s += kCoCompute) nsm[s] = 0.0;
+    co_compute_sync();  // every update of wsm is done
+    for (int u = tid; u < m * npc; u += kCoCompute) {
+      const int s = u / npc, p = u - s * npc;
+      if (!act[s] || p >= nvp) continue;
+      const double2 a0 = wsm[(size_t)s * rows + 2 * p], a1 = wsm[(size_t)s * rows + 2 * p + 1];
+      atomicAdd(&nsm[s], a0.x * a0.x + a0.y * a0.y + a1.x * a1.x + a1.y * a1.y);
+    }
+    co_compute_sync();
+    for (int s = tid; s < m; s += kCoCompute)
+      if (act[s] && nsm[s] != 0.0) atomicAdd(st_nacc(P, ks[s] & 1, s, 1), nsm[s]);
+    if (lane == 0) {  // every issued copy was consumed; make sure the last use of each slot has landed
+      for (unsigned q = nissued > (unsigned)slots ? nissued - slots : 0u; q < nissued; q++)
+        mbar_wait_drain(&full[q % slots], (q / slots) & 1u);
+    }
+  } else {
+    // Givens warp: columns s = blockIdx.x + q gridDim.x
+    for (int q = 0; q < cpc; q++) {
+      const int s = blockIdx.x + q * gridDim.x;
+      if (s >= m || !act[s]) continue;
+      unsigned char* gv = co_raw + Lo.giv + (size_t)q * Lo.giv_stride;
+      double2* hc = reinterpret_cast<double2*>(gv);
+      double2* snv = hc + (R + 1);
+      double* csv = reinterpret_cast<double*>(snv + R);
+      double2* misc = co_misc(csv, R);  // [0] = g_k, [1].x = tol
+      const int k = ks[s];
+      const double* h = st_hacc(P, k & 1, s, 0);
+      for (int l = lane; l <= k; l += 32) hc[l] = make_double2(__ldcg(h + 2 * l), __ldcg(h + 2 * l + 1));
+      for (int l = lane; l < k; l += 32) {
+        csv[l] = P.cs[s * R + l];
+        snv[l] = P.sn[s * R + l];
+      }
+      if (lane == 0) {
+        misc[0] = P.g[(size_t)s * (R + 1) + k];
+        misc[1] = make_double2(P.tol[s], 0.0);
+      }
+      __syncwarp();
+      if (lane == 0) {
+        // previous rotations, sequential: hc[l], hc[l+1] <- (c a + sn b, -conj(sn) a + c b)
+        double2 a = hc[0];
+        for (int l = 0; l < k; l++) {
+          const double c = csv[l];
+          const double2 sn = snv[l];
+          const double2 b = hc[l + 1];
+          const double2 sb = cmul(sn, b);
+          const double2 t = cmul(make_double2(-sn.x, sn.y), a);
+          hc[l] = make_double2(c * a.x + sb.x, c * a.y + sb.y);
+          a = make_double2(t.x + c * b.x, t.y + c * b.y);
+        }
+        hc[k] = a;
+      }
+      __syncwarp();
+    }
+  }
+  co_grid_sync(P.st);
+
+  // ---- finish: v_{k+1} = w' / |w'| and the next operand ----
+  if (!giv_warp) {
+    for (int u = tid; u < m * npc; u += kCoCompute) {
+      const int s = u / npc, p = u - s * npc;
+      if (!act[s] || p >= nvp) continue;
+      const int k = ks[s];
+      const double hn = sqrt(__ldcg(st_nacc(P, k & 1, s, 1)));
+      const double inv = hn > 0.0 ? 1.0 / hn : 0.0;
+      const int i = i0 + 2 * p;
+      const double2 a0 = wsm[(size_t)s * rows + 2 * p], a1 = wsm[(size_t)s * rows + 2 * p + 1];
+      const float2 f0 = make_float2((float)(a0.x * inv), (float)(a0.y * inv));
+      const float2 f1 = i + 1 < P.n ? make_float2((float)(a1.x * inv), (float)(a1.y * inv)) : make_float2(0.f, 0.f);
+      *reinterpret_cast<float4*>(P.Vb + ((size_t)s * (R + 1) + k + 1) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+      store_operand(P, i, s, f0, f1);
+    }
+  } else {
+    for (int q = 0; q < cpc; q++) {
+      const int s = blockIdx.x + q * gridDim.x;
+      if (s >= m) continue;
+      const int k = ks[s];
+      if (!act[s]) {
+        if (lane == 0) column_done(P, s, k, false);
+        continue;
+      }
+      unsigned char* gv = co_raw + Lo.giv + (size_t)q * Lo.giv_stride;
+      double2* hc = reinterpret_cast<double2*>(gv);
+      double2* snv = hc + (R + 1);
+      double* csv = reinterpret_cast<double*>(snv + R);
+      double2* misc = co_misc(csv, R);
+      const double hn = sqrt(__ldcg(st_nacc(P, k & 1, s, 1)));
+      int still = 0;
+      if (lane == 0) {
+        const double2 a = hc[k];
+        const double na = sqrt(a.x * a.x + a.y * a.y), nb = hn;
+        const double rho = sqrt(na * na + nb * nb);
+        double c;
+        double2 sn;
+        if (rho == 0.0) {
+          c = 1.0;
+          sn = make_double2(0.0, 0.0);
+        } else if (na == 0.0) {
+          c = 0.0;
+          sn = make_double2(1.0, 0.0);  // conj(hn)/|hn|, hn real and positive
+          hc[k] = make_double2(nb, 0.0);
+        } else {
+          c = na / rho;
+          const double2 ph = make_double2(a.x / na, a.y / na);
+          sn = make_double2(ph.x * nb / rho, ph.y * nb / rho);  // ph conj(b)/rho, b = hn real
+          hc[k] = make_double2(ph.x * rho, ph.y * rho);
+        }
+        hc[k + 1] = make_double2(0.0, 0.0);
+        P.cs[s * R + k] = c;
+        P.sn[s * R + k] = sn;
+        double2* gs = P.g + (size_t)s * (R + 1);
+        const double2 gk = misc[0];
+        const double2 gk1 = cmul(make_double2(-sn.x, sn.y), gk);
+        gs[k + 1] = gk1;
+        gs[k] = make_double2(c * gk.x, c * gk.y);
+        const double res = sqrt(gk1.x * gk1.x + gk1.y * gk1.y);
+        P.resid[s] = res;
+        P.kend[s] = k + 1;
+        const bool breakdown = !(hn > 1e-300) || !(hn > 1e-14 * rho);
+        if (res <= misc[1].x || breakdown || k + 1 >= R)
+          P.active[s] = 0;
+        else
+          still = 1;
+      }
+      __syncwarp();
+      double2* Hk = P.H + ((size_t)s * R + k) * (R + 1);
+      for (int l = lane; l <= k + 1; l += 32) Hk[l] = hc[l];
+      still = __shfl_sync(0xffffffffu, still, 0);
+      if (lane == 0) column_done(P, s, k + 1, still != 0);
+      __syncwarp();
+    }
+  }
+}
+
 // Back substitution H y = g on the Givens-reduced Hessenberg matrix, one
 // warp per column, column-oriented: y_j = g_j / H_jj, then the lanes update
 // g_0..g_{j-1} -= y_j H_{0..j-1, j} (column j of H is contiguous).
@@ -1600,6 +2049,49 @@ int arnoldi_shape(int n, int m, ArnShape* out) {
   return best_cost < 0 ? BEM_ERR_UNSUPPORTED : BEM_OK;
 }
 
+// Launch shape of gm_arnoldi_coop_kernel: npc unknown pairs per CTA (at
+// least 16, enough CTAs to cover every SM once), one CTA per SM at most, all
+// resident (cooperative launch); every column's rotations owned by one CTA.
+struct CoShape {
+  int npc = 0, grid = 0, cpc = 0, slots = 0;
+  size_t smem = 0;
+};
+
+int coop_shape(int n, int m, int R, CoShape* out) {
+  static std::atomic<bool> attr{false};
+  int dev = 0, coop_ok = 0, smem_optin = 0;
+  BEM_CUDA_TRY(cudaGetDevice(&dev));
+  BEM_CUDA_TRY(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
+  BEM_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (!coop_ok) return BEM_ERR_UNSUPPORTED;
+  const int sms = sm_count_linalg();
+  const int npairs = (n + 1) / 2;
+  int npc = std::max(16, (npairs + sms - 1) / sms);
+  const int grid = (npairs + npc - 1) / npc;
+  const int cpc = (m + grid - 1) / grid;  // columns whose rotations one CTA applies
+  if (cpc > kCoMaxColsPerCta) return BEM_ERR_UNSUPPORTED;
+  // ring slots per warp: 4, fewer when shared memory is short (half the
+  // opt-in maximum, leaving room for a concurrent solve's kernels)
+  int slots = 4;
+  while (slots > 2 && co_layout(m, npc, R, cpc, slots).total > (size_t)smem_optin / 2) slots--;
+  const size_t smem = co_layout(m, npc, R, cpc, slots).total;
+  if (smem > (size_t)smem_optin / 2) return BEM_ERR_UNSUPPORTED;
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_arnoldi_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem_optin / 2));
+    attr.store(true, std::memory_order_release);
+  }
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_arnoldi_coop_kernel, kCoThreads, smem));
+  if (occ < 1 || grid > occ * sms) return BEM_ERR_UNSUPPORTED;
+  out->npc = npc;
+  out->grid = grid;
+  out->cpc = cpc;
+  out->slots = slots;
+  out->smem = smem;
+  return BEM_OK;
+}
+
 }  // namespace
 
 int cmatmul(const float2* A, int n, const float2* X, int m, float2* Y, cudaStream_t s) {
@@ -1709,6 +2201,10 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   // The streamed step (launches over all SMs, selective second pass) when
   // the mode key asks for it; the cluster kernel is faster at s5 and s6.
   const bool streamed = reorth == 0 && g_arn_mode == 2;
+  // The cooperative step (one launch over all SMs, two grid barriers): the
+  // default for one Gram-Schmidt pass whenever its grid fits on the device.
+  CoShape co;
+  const bool coop = reorth == 0 && (g_arn_mode == 0 || g_arn_mode == 3) && coop_shape(n, m, R, &co) == BEM_OK;
   const int npairs_all = (n + 1) / 2;
   // about 8 work items per SM over all columns, each of 128 to 4096 pairs
   // (w of an item in FP64: at most 128 KB of shared memory)
@@ -1734,6 +2230,22 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
                  ? launch_cgemv((const float2*)A, n, P.X, m, P.Y, P.active, st, &P.st->err)
                  : tc_gemm(tcws, n, prec, m, P.Y, P.active, st);
     if (r2) return r2;
+    if (coop) {
+      cudaLaunchConfig_t ccfg = {};
+      ccfg.gridDim = dim3((unsigned)co.grid, 1, 1);
+      ccfg.blockDim = dim3(kCoThreads, 1, 1);
+      ccfg.dynamicSmemBytes = co.smem;
+      ccfg.stream = st;
+      cudaLaunchAttribute cat[1];
+      cat[0].id = cudaLaunchAttributeCooperative;
+      cat[0].val.cooperative = 1;
+      ccfg.attrs = cat;
+      ccfg.numAttrs = 1;
+      BEM_CUDA_TRY(cudaLaunchKernelEx(&ccfg, gm_arnoldi_coop_kernel, P, co.npc, co.cpc, co.slots));
+      count_launch();
+      BEM_CUDA_TRY(cudaGetLastError());
+      return BEM_OK;
+    }
     if (streamed) {
       (gm_st_dots_kernel<0><<<st_grid, kStThreads, sizeof(double4) * st_span, st>>>(P, st_span, st_nb),
        count_launch());
@@ -1835,7 +2347,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     bool first_cycle = true;
     while (total_iters < params->max_iters) {
       BEM_CUDA_TRY(cudaMemsetAsync(P.norm2, 0, sizeof(double) * m, s));
-      if (streamed) {  // both parity buffers of the streamed step's sums
+      if (streamed || coop) {  // both parity buffers of the step's sums
         BEM_CUDA_TRY(cudaMemsetAsync(P.hacc, 0, sizeof(double) * 2 * (size_t)m * 4 * (R + 1), s));
         BEM_CUDA_TRY(cudaMemsetAsync(P.nacc, 0, sizeof(double) * 2 * (size_t)m * 3, s));
       }
@@ -1909,7 +2421,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   BEM_CUDA_TRY(cudaStreamSynchronize(s));
   if (prec != BEM_PREC_FP32) {
     int tc_err = 0;
-    if (tc_error(tcws, &tc_err, s) != BEM_OK || tc_err) status = BEM_ERR_CUDA;
+    if (tc_error(tcws, &tc_err, s, false) != BEM_OK || tc_err) status = BEM_ERR_CUDA;
   }
   GmState fin;
   BEM_CUDA_TRY(cudaMemcpyAsync(&fin, P.st, sizeof(GmState), cudaMemcpyDeviceToHost, s));

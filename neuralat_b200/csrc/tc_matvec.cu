@@ -49,6 +49,8 @@
 namespace bemb {
 
 int g_tc_promote = 0;  // accumulator segment length in K blocks (0: automatic); a tuning knob
+int g_tc_wait_us = 0;  // limit of the bounded waits of the tensor-core kernels in microseconds (0: 2 s)
+std::atomic<int> g_tc_skip_fill{0};  // test hook, one launch: fill (value - 1) of CTA 0 is not issued
 
 namespace {
 
@@ -69,6 +71,9 @@ struct TcArgs {
   const float* rinv;  // FP16X3: per-row and per-right-hand-side inverse scales
   const float* cinv;
   long long promote;  // K blocks per accumulator segment
+  unsigned long long wait_ns;  // limit of every bounded wait
+  int skip_fill;  // test hook: CTA 0's producer leaves its fill number skip_fill (>= 0) unissued, so the
+                  // consumer's bounded wait on that stage expires; -1 = off
 };
 
 // Shared-memory matrix descriptor: K-major tile with 128-byte swizzle, rows
@@ -134,6 +139,7 @@ struct TcSmem {
                                    : (kAccBufs * NB <= 256) ? 256
                                                             : 512;
   static constexpr int kBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+  static_assert((2 * kStages + 2 * kAccBufs) * 8 + 8 + 8 <= 256, "barriers, TMEM slot and done barrier fit");
 };
 
 // End of the accumulator segment that starts at unit u: the row block's end,
@@ -163,7 +169,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   uint64_t* empty = bars + S::kStages;
   uint64_t* accf = bars + 2 * S::kStages;
   uint64_t* acce = accf + S::kAccBufs;
-  uint32_t* tmem_slot = (uint32_t*)(acce + S::kAccBufs);
+  uint64_t* mma_done = acce + S::kAccBufs;  // all MMAs of this CTA complete (checked before TMEM is released)
+  uint32_t* tmem_slot = (uint32_t*)(mma_done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // this CTA's contiguous range of (row block, K block) units
@@ -179,6 +186,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 4 * 32);
     }
+    mbar_init(mma_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -195,21 +203,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---------------- TMA producer ----------------
     int stage = 0;
     uint32_t phase = 0;
+    int armed[S::kStages];  // phase of each stage's last issued fill, -1: none
+#pragma unroll
+    for (int q = 0; q < S::kStages; q++) armed[q] = -1;
     const uint64_t stream_policy = l2_evict_first_policy();
-    for (long long u = u0; u < u1; u++) {
+    long long fill = 0;
+    for (long long u = u0; u < u1; u++, fill++) {
       const int rb = (int)(u / p.n_kb), kb = (int)(u % p.n_kb);
-      if (!mbar_wait(&empty[stage], phase ^ 1u, p.err)) break;
-      unsigned char* st = base + stage * S::kStageBytes;
-      mbar_expect_tx(&full[stage], S::kStageBytes);
-      tma_load_2d_hint(st, &tmAh, kb * kBK, rb * kBM, &full[stage], stream_policy);
-      if (X3) tma_load_2d_hint(st + S::kABytes, &tmAl, kb * kBK, rb * kBM, &full[stage], stream_policy);
-      unsigned char* bst = st + (X3 ? 2 : 1) * S::kABytes;
-      tma_load_2d(bst, &tmBh, kb * kBK, 0, &full[stage]);
-      tma_load_2d(bst + S::kBBytes, &tmBl, kb * kBK, 0, &full[stage]);
+      if (!mbar_wait(&empty[stage], phase ^ 1u, p.err, p.wait_ns)) break;
+      if (!(blockIdx.x == 0 && fill == p.skip_fill)) {
+        unsigned char* st = base + stage * S::kStageBytes;
+        mbar_expect_tx(&full[stage], S::kStageBytes);
+        tma_load_2d_hint(st, &tmAh, kb * kBK, rb * kBM, &full[stage], stream_policy);
+        if (X3) tma_load_2d_hint(st + S::kABytes, &tmAl, kb * kBK, rb * kBM, &full[stage], stream_policy);
+        unsigned char* bst = st + (X3 ? 2 : 1) * S::kABytes;
+        tma_load_2d(bst, &tmBh, kb * kBK, 0, &full[stage]);
+        tma_load_2d(bst + S::kBBytes, &tmBl, kb * kBK, 0, &full[stage]);
+        armed[stage] = (int)phase;
+      }
       if (++stage == S::kStages) {
         stage = 0;
         phase ^= 1u;
       }
+    }
+    if (*(volatile int*)p.err) {
+      // a wait expired: the consumer may have stopped; let every issued copy
+      // land before the CTA exits (the last fill of each stage is the newest)
+#pragma unroll 1
+      for (int q = 0; q < S::kStages; q++)
+        if (armed[q] >= 0) mbar_wait_drain(&full[q], (uint32_t)armed[q], p.wait_ns);
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
@@ -222,12 +244,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     long long u = u0;
     while (u < u1 && ok) {
       const long long seg_end = segment_end(u, u1, p);
-      if (!mbar_wait(&acce[buf], acc_phase ^ 1u, p.err)) break;
+      if (!mbar_wait(&acce[buf], acc_phase ^ 1u, p.err, p.wait_ns)) break;
       tc_fence_after();
       const uint32_t dt = tmem_base + (uint32_t)(buf * NB);
       bool first = true;
       for (; u < seg_end; u++) {
-        if (!mbar_wait(&full[stage], phase, p.err)) {
+        if (!mbar_wait(&full[stage], phase, p.err, p.wait_ns)) {
           ok = false;
           break;
         }
@@ -257,6 +279,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         acc_phase ^= 1u;
       }
     }
+    // every MMA issued here has finished reading shared memory and writing
+    // tensor memory before the CTA releases either (the epilogue may have
+    // stopped waiting after an expired wait)
+    umma_commit(mma_done);
+    mbar_wait_drain(mma_done, 0u, p.wait_ns);
   } else if (warp >= 2) {
     // ---------------- epilogue: TMEM -> registers -> atomics into Y ----------------
     // Each lane owns one row.  With NB <= 128 the segment sums are added in
@@ -276,7 +303,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const long long seg_end = segment_end(u, u1, p);
       u = seg_end;
       const bool row_done = u == u1 || u % p.n_kb == 0;
-      if (!mbar_wait(&accf[buf], acc_phase, p.err)) break;
+      if (!mbar_wait(&accf[buf], acc_phase, p.err, p.wait_ns)) break;
       tc_fence_after();
       const int row = rb * kBM + quarter * 32 + lane;
       float* yr = p.Y + (size_t)row * p.m2;
@@ -575,6 +602,8 @@ int launch_tc(const TcLayout& L, char* ws, int n, const int* active, int nact, f
   // two K blocks per segment: fp16x3 error 6e-7 on the BEM matrix (one block:
   // 4e-7 but 18% slower; 16 blocks: 4e-6; a whole row block: 3e-5)
   a.promote = g_tc_promote > 0 ? g_tc_promote : (NB <= 128 ? 2 : (1ll << 40));
+  a.wait_ns = g_tc_wait_us > 0 ? 1000ull * (unsigned long long)g_tc_wait_us : kWaitLimitNs;
+  a.skip_fill = g_tc_skip_fill.exchange(0) - 1;  // consumed by this launch
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -674,9 +703,11 @@ int tc_gemm(const void* ws_, int n, int precision, int m, float2* Y, const int* 
   return BEM_ERR_UNSUPPORTED;
 }
 
-// Error flag of the tensor-core kernels that used this workspace (syncs).
-int tc_error(const void* ws_, int* err_host, cudaStream_t s) {
+// Error flag of the tensor-core kernels that used this workspace (syncs);
+// with `clear` it is reset for the next launches.
+int tc_error(const void* ws_, int* err_host, cudaStream_t s, bool clear) {
   BEM_CUDA_TRY(cudaMemcpyAsync(err_host, ws_, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (clear) BEM_CUDA_TRY(cudaMemsetAsync(const_cast<void*>(ws_), 0, sizeof(int), s));
   BEM_CUDA_TRY(cudaStreamSynchronize(s));
   return BEM_OK;
 }
@@ -707,7 +738,7 @@ extern "C" int bem_tc_matmul(const void* ws, size_t ws_bytes, int n, int precisi
 extern "C" int bem_tc_status(const void* ws, bem_stream_t stream) {
   if (!ws) return BEM_ERR_INVALID_ARGUMENT;
   int err = 0;
-  int rc = tc_error(ws, &err, (cudaStream_t)stream);
+  int rc = tc_error(ws, &err, (cudaStream_t)stream, true);
   if (rc) return rc;
   return err ? BEM_ERR_CUDA : BEM_OK;
 }

@@ -1,12 +1,14 @@
 """The Arnoldi step variants of the device GMRES give the same solves.
 
-The default is the cluster kernel (one launch per step, a thread-block
-cluster per right-hand side) with one classical Gram-Schmidt pass whose
-projections are formed with FP64 products; two passes (CGS2) are the stable
-reference.  The streamed step (launches over all SMs, a second pass where the
-first one cancels most of w) is selected with BEM_TUNE_ARNOLDI_MODE.  The
-odd-sized 3 kHz case here is one where single-pass Gram-Schmidt with FP32
-products needed up to 1.7 times the steps."""
+The default is the cooperative kernel (one launch over all SMs per step, two
+grid barriers) with one classical Gram-Schmidt pass whose projections are
+formed with FP64 products; two passes (CGS2, on the cluster kernel: a
+thread-block cluster per right-hand side) are the stable reference.  The
+cluster kernel with one pass and the streamed step (launches over all SMs, a
+second pass where the first one cancels most of w) are selected with
+BEM_TUNE_ARNOLDI_MODE.  The odd-sized 3 kHz case here is one where
+single-pass Gram-Schmidt with FP32 products needed up to 1.7 times the steps;
+it also exercises the padding entry of an odd number of unknowns."""
 import numpy as np
 import pytest
 import torch
@@ -46,7 +48,8 @@ def test_arnoldi_variants_match_two_pass_reference(system, m, precision):
     lib = L.lib()
     out = {}
     try:
-        for name, mode, reorth in (("cgs2", 1, 2), ("default", 0, 0), ("streamed", 2, 0)):
+        for name, mode, reorth in (("cgs2", 1, 2), ("default", 0, 0), ("cluster", 1, 0), ("streamed", 2, 0),
+                                   ("cooperative", 3, 0)):
             L.check(lib.bem_set_tuning(L.TUNE_ARNOLDI_MODE, mode))
             L.check(lib.bem_set_tuning(L.TUNE_GMRES_REORTH, reorth))
             info = {}
@@ -56,7 +59,7 @@ def test_arnoldi_variants_match_two_pass_reference(system, m, precision):
         L.check(lib.bem_set_tuning(L.TUNE_GMRES_REORTH, 0))
     u_ref, i_ref = out["cgs2"]
     assert i_ref["status"] == 0
-    for name in ("default", "streamed"):
+    for name in ("default", "cluster", "streamed", "cooperative"):
         u, info = out[name]
         assert info["status"] == 0, name
         assert info["iterations"] <= 1.1 * i_ref["iterations"] + 2, (name, info["iterations"], i_ref["iterations"])
@@ -69,4 +72,4 @@ def test_arnoldi_variants_match_two_pass_reference(system, m, precision):
 def test_arnoldi_mode_key():
     lib = L.lib()
     assert lib.bem_get_tuning(L.TUNE_ARNOLDI_MODE) == 0
-    assert lib.bem_set_tuning(L.TUNE_ARNOLDI_MODE, 3) == L.BEM_ERR_INVALID_ARGUMENT
+    assert lib.bem_set_tuning(L.TUNE_ARNOLDI_MODE, 4) == L.BEM_ERR_INVALID_ARGUMENT

@@ -106,3 +106,38 @@ def test_mixed_precision_cbie_matches_fp32(precision):
     for x in (x32, xmx):
         xx = x.cpu().numpy()
         assert np.linalg.norm(xx - ref) / np.linalg.norm(ref) <= 1e-4  # residual 1e-6 times the conditioning
+
+
+@pytest.mark.parametrize("fill", [1, 4])
+def test_expired_bounded_wait_is_reported_and_the_next_call_is_clean(fill):
+    """A bounded wait that runs out, made on the host: the test hook leaves one
+    pipeline fill of CTA 0 unissued, so its tensor-core consumer waits on a
+    stage that never fills.  With a 1 ms limit the wait expires, the kernel
+    lets its other copies land, releases tensor memory and returns (no fault,
+    no hang); bem_tc_status reports BEM_ERR_CUDA once, and the next call on the
+    same workspace is exact again."""
+    lib = L.lib()
+    rng = np.random.default_rng(3)
+    n, m = 4000, 8  # 32 row blocks x 125 K blocks: ~27 pipeline fills per CTA
+    A = torch.from_numpy((rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)).cuda()
+    X = torch.from_numpy((rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))).astype(np.complex64)).cuda()
+    ref = A.cpu().numpy().astype(np.complex128) @ X.cpu().numpy().astype(np.complex128)
+    prec = L.PREC_FP16X3
+    nbytes = int(lib.bem_tc_operator_bytes(n, m, prec))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    L.check(lib.bem_tc_operator_prepare(_vp(A), n, prec, _vp(ws), nbytes, _stream()))
+    Y = torch.empty_like(X)
+    try:
+        L.check(lib.bem_set_tuning(L.TUNE_TC_WAIT_US, 1000))
+        L.check(lib.bem_set_tuning(L.TUNE_TC_TEST_SKIP_FILL, fill))
+        L.check(lib.bem_tc_matmul(_vp(ws), nbytes, n, prec, _vp(X), m, _vp(Y), _stream()))
+        assert lib.bem_get_tuning(L.TUNE_TC_TEST_SKIP_FILL) == 0  # one launch only
+        assert lib.bem_tc_status(_vp(ws), _stream()) == L.BEM_ERR_CUDA
+        assert lib.bem_tc_status(_vp(ws), _stream()) == L.BEM_OK  # read once, then clear
+    finally:
+        lib.bem_set_tuning(L.TUNE_TC_TEST_SKIP_FILL, 0)
+        lib.bem_set_tuning(L.TUNE_TC_WAIT_US, 0)
+    L.check(lib.bem_tc_matmul(_vp(ws), nbytes, n, prec, _vp(X), m, _vp(Y), _stream()))
+    assert lib.bem_tc_status(_vp(ws), _stream()) == L.BEM_OK
+    err = np.linalg.norm(Y.cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err <= 3e-6, err
