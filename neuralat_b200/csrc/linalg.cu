@@ -1413,7 +1413,10 @@ __global__ void __launch_bounds__(kCoThreads, 1)
   const uint64_t pol = l2_evict_last_policy();
   const uint32_t row_bytes = (uint32_t)nvp * 16u;
   // the warp's sequence: its items of the dots pass, then the same items again for the update pass
-  int iss = giv_warp ? items.total : items.next(warp), iss_pass = 0;  // next item to issue, and its pass
+  // next item to issue and its pass (2: nothing left); a warp without items
+  // in the dots pass has none in the update pass either
+  int iss = giv_warp ? items.total : items.next(warp);
+  int iss_pass = iss < items.total ? 0 : 2;
   unsigned nissued = 0, nconsumed = 0;
   auto issue = [&]() {  // lane 0: bulk-copy the next item of the sequence into its slot
     if (iss_pass > 1) return;
