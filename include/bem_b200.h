@@ -188,9 +188,10 @@ enum {
   BEM_TUNE_GMRES_REORTH = 4,         /* Arnoldi Gram-Schmidt passes: 0 automatic (one), 1 one, 2 two */
   BEM_TUNE_ARNOLDI_CLUSTER = 5,      /* largest thread-block cluster (<= 16 CTAs) per Krylov column in
                                         the Arnoldi kernel (0: automatic) */
-  BEM_TUNE_ARNOLDI_MODE = 6,         /* Arnoldi step: 0 automatic (3 when its grid fits, else 1),
-                                        1 one cluster kernel per step, 2 streamed kernels over all SMs,
-                                        3 one cooperative kernel over all SMs (two grid barriers) */
+  BEM_TUNE_ARNOLDI_MODE = 6,         /* Arnoldi step: 0 automatic (1), 1 one cluster kernel per step,
+                                        2 streamed kernels over all SMs, 3 one cooperative kernel over
+                                        all SMs (two grid barriers; falls back to 1 when its grid does
+                                        not fit) */
   BEM_TUNE_TC_WAIT_US = 7,           /* limit of each bounded wait in the tensor-core matvec, microseconds
                                         (0: 2 s) */
   BEM_TUNE_TC_TEST_SKIP_FILL = 8     /* test hook for the bounded waits, one launch: value v > 0 makes CTA 0

@@ -36,8 +36,8 @@ namespace cg = cooperative_groups;
 
 int g_gmres_reorth = 0;     // Gram-Schmidt passes: 0 automatic, 1 one pass (CGS), 2 two passes (CGS2); a tuning knob
 int g_arn_max_cluster = 0;  // largest Arnoldi cluster size tried (0: 16); a tuning knob
-int g_arn_mode = 0;         // Arnoldi step: 0 automatic, 1 cluster kernel, 2 streamed kernels, 3 cooperative
-                            // kernel; a tuning knob
+int g_arn_mode = 0;         // Arnoldi step: 0 automatic (the cluster kernel), 1 cluster kernel, 2 streamed
+                            // kernels, 3 cooperative kernel; a tuning knob
 
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
@@ -2204,10 +2204,14 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   // The streamed step (launches over all SMs, selective second pass) when
   // the mode key asks for it; the cluster kernel is faster at s5 and s6.
   const bool streamed = reorth == 0 && g_arn_mode == 2;
-  // The cooperative step (one launch over all SMs, two grid barriers): the
-  // default for one Gram-Schmidt pass whenever its grid fits on the device.
+  // The cooperative step (one launch over all SMs, two grid barriers) when the
+  // mode key asks for it.  Measured on the s5 workload (8 right-hand sides)
+  // it is slower than the cluster kernel (solve 28.6 ms against 25.2 ms):
+  // both are bound by FP64 work per basis element (two float->double
+  // conversions and two complex FP64 multiply-adds per element and step), and
+  // with ~70 unknowns per CTA its lanes diverge and its bulk copies are small.
   CoShape co;
-  const bool coop = reorth == 0 && (g_arn_mode == 0 || g_arn_mode == 3) && coop_shape(n, m, R, &co) == BEM_OK;
+  const bool coop = reorth == 0 && g_arn_mode == 3 && coop_shape(n, m, R, &co) == BEM_OK;
   const int npairs_all = (n + 1) / 2;
   // about 8 work items per SM over all columns, each of 128 to 4096 pairs
   // (w of an item in FP64: at most 128 KB of shared memory)

@@ -1,12 +1,11 @@
 """The Arnoldi step variants of the device GMRES give the same solves.
 
-The default is the cooperative kernel (one launch over all SMs per step, two
-grid barriers) with one classical Gram-Schmidt pass whose projections are
-formed with FP64 products; two passes (CGS2, on the cluster kernel: a
-thread-block cluster per right-hand side) are the stable reference.  The
-cluster kernel with one pass and the streamed step (launches over all SMs, a
-second pass where the first one cancels most of w) are selected with
-BEM_TUNE_ARNOLDI_MODE.  The odd-sized 3 kHz case here is one where
+The default is the cluster kernel (one launch per step, a thread-block
+cluster per right-hand side) with one classical Gram-Schmidt pass whose
+projections are formed with FP64 products; two passes (CGS2) are the stable
+reference.  The streamed step (launches over all SMs, a second pass where the
+first one cancels most of w) and the cooperative kernel (one launch over all
+SMs, two grid barriers) are selected with BEM_TUNE_ARNOLDI_MODE.  The odd-sized 3 kHz case here is one where
 single-pass Gram-Schmidt with FP32 products needed up to 1.7 times the steps;
 it also exercises the padding entry of an odd number of unknowns."""
 import numpy as np
