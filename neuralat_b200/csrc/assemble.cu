@@ -306,6 +306,10 @@ __device__ __forceinline__ void sym_fetch_tile(SymSmem& sm, const GeomView& g, i
 }
 
 // aV, aK as pair_block; aM[3a+b] = sum_pq C_ap C_bq dn_i(q) Gk(r_pq) = K_ji[b][a].
+// The arithmetic runs on packed FP32 pairs: the complex accumulations as
+// (re, im) pairs and the distance computation for two trial points at once,
+// with the same operations and rounding as the scalar form (bit-identical),
+// in about half the issued instructions; rsqrt and sin/cos stay scalar.
 __device__ __forceinline__ void pair_block_sym(const float (*xs)[kSymTest], int tl, const float (&yq)[18],
                                                const float (&dq)[6], float njx, float njy, float njz, float cjx,
                                                float cjy, float cjz, float k, float2 (&aV)[9], float2 (&aK)[9],
@@ -316,6 +320,15 @@ __device__ __forceinline__ void pair_block_sym(const float (*xs)[kSymTest], int 
     aK[e] = make_float2(0.f, 0.f);
     aM[e] = make_float2(0.f, 0.f);
   }
+  // trial points in pairs (2h, 2h + 1), one float2 per coordinate
+  float2 Yx[3], Yy[3], Yz[3];
+#pragma unroll
+  for (int h = 0; h < 3; h++) {
+    Yx[h] = make_float2(yq[6 * h], yq[6 * h + 3]);
+    Yy[h] = make_float2(yq[6 * h + 1], yq[6 * h + 4]);
+    Yz[h] = make_float2(yq[6 * h + 2], yq[6 * h + 5]);
+  }
+  const float2 kk = make_float2(k, -k);
 #pragma unroll
   for (int p = 0; p < 6; p++) {
     const float px = xs[3 * p][tl], py = xs[3 * p + 1][tl], pz = xs[3 * p + 2][tl];
@@ -328,41 +341,43 @@ __device__ __forceinline__ void pair_block_sym(const float (*xs)[kSymTest], int 
       uK[b] = make_float2(0.f, 0.f);
     }
 #pragma unroll
-    for (int q = 0; q < 6; q++) {
-      const float dx = yq[3 * q] - px, dy = yq[3 * q + 1] - py, dz = yq[3 * q + 2] - pz;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const float rinv = fminf(rsqrtf(r2), 1.0f / kEps);
-      const float r = fmaxf(r2 * rinv, kEps);
-      float s, c;
-      __sincosf(k * r, &s, &c);
-      const float gvr = c * rinv, gvi = s * rinv;
-      const float rinv2 = rinv * rinv;
-      const float gkr = fmaf(k, s, gvr) * rinv2;   // (c + kr s) / r^3
-      const float gki = fmaf(-k, c, gvi) * rinv2;  // (s - kr c) / r^3
-      const float mkr = dq[q] * gkr, mki = dq[q] * gki;
+    for (int h = 0; h < 3; h++) {
+      const float2 dx = f2_sub(Yx[h], f2(px)), dy = f2_sub(Yy[h], f2(py)), dz = f2_sub(Yz[h], f2(pz));
+      const float2 r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
+      const float2 rinv = make_float2(fminf(rsqrtf(r2.x), 1.0f / kEps), fminf(rsqrtf(r2.y), 1.0f / kEps));
+      float2 r = f2_mul(r2, rinv);
+      r.x = fmaxf(r.x, kEps);
+      r.y = fmaxf(r.y, kEps);
+      const float2 kr = f2_mul(f2(k), r);
+      const float2 rinv2 = f2_mul(rinv, rinv);
+      float sc[2][2];  // [point][sin, cos]
+      __sincosf(kr.x, &sc[0][0], &sc[0][1]);
+      __sincosf(kr.y, &sc[1][0], &sc[1][1]);
 #pragma unroll
-      for (int b = 0; b < 3; b++) {
-        const float w = (float)(tri6_w(q) * tri6_phi(q, b));
-        tV[b].x = fmaf(w, gvr, tV[b].x);
-        tV[b].y = fmaf(w, gvi, tV[b].y);
-        tK[b].x = fmaf(w, gkr, tK[b].x);
-        tK[b].y = fmaf(w, gki, tK[b].y);
-        uK[b].x = fmaf(w, mkr, uK[b].x);
-        uK[b].y = fmaf(w, mki, uK[b].y);
+      for (int j = 0; j < 2; j++) {
+        const int q = 2 * h + j;
+        const float ri = j == 0 ? rinv.x : rinv.y, ri2 = j == 0 ? rinv2.x : rinv2.y;
+        const float2 gv = f2_mul(make_float2(sc[j][1], sc[j][0]), f2(ri));                  // (c, s) / r
+        const float2 gk = f2_mul(f2_fma(kk, make_float2(sc[j][0], sc[j][1]), gv), f2(ri2));  // (c + kr s, s - kr c) / r^3
+        const float2 mk = f2_mul(f2(dq[q]), gk);
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          const float2 w = f2((float)(tri6_w(q) * tri6_phi(q, b)));
+          tV[b] = f2_fma(w, gv, tV[b]);
+          tK[b] = f2_fma(w, gk, tK[b]);
+          uK[b] = f2_fma(w, mk, uK[b]);
+        }
       }
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const float wa = (float)(tri6_w(p) * tri6_phi(p, a));
-      const float wk = wa * dn;
+      const float2 wa2 = f2(wa), wk2 = f2(wa * dn);
 #pragma unroll
       for (int b = 0; b < 3; b++) {
-        aV[3 * a + b].x = fmaf(wa, tV[b].x, aV[3 * a + b].x);
-        aV[3 * a + b].y = fmaf(wa, tV[b].y, aV[3 * a + b].y);
-        aK[3 * a + b].x = fmaf(wk, tK[b].x, aK[3 * a + b].x);
-        aK[3 * a + b].y = fmaf(wk, tK[b].y, aK[3 * a + b].y);
-        aM[3 * a + b].x = fmaf(wa, uK[b].x, aM[3 * a + b].x);
-        aM[3 * a + b].y = fmaf(wa, uK[b].y, aM[3 * a + b].y);
+        aV[3 * a + b] = f2_fma(wa2, tV[b], aV[3 * a + b]);
+        aK[3 * a + b] = f2_fma(wk2, tK[b], aK[3 * a + b]);
+        aM[3 * a + b] = f2_fma(wa2, uK[b], aM[3 * a + b]);
       }
     }
   }
