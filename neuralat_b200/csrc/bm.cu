@@ -104,6 +104,8 @@ __device__ __forceinline__ void bm_fetch_tile(BmSmem& sm, const GeomView& g, int
 
 // S, T, U blocks of one unordered pair under the TN x TN point rule (test
 // triangle tl, points in xs; trial points yq, dq[q] = n_i . (c_i - y_q)).
+// Packed FP32 pairs (f32x2): complex sums as (re, im) pairs, distances for two
+// trial points at once; same operations and rounding as the scalar form.
 template <int TN>
 __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl, const float (&yq)[3 * TN],
                                               const float (&dq)[TN], float njx, float njy, float njz, float cjx,
@@ -115,6 +117,7 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
     aT[e] = make_float2(0.f, 0.f);
     aU[e] = make_float2(0.f, 0.f);
   }
+  const float2 kk = make_float2(k, -k);
 #pragma unroll
   for (int p = 0; p < TN; p++) {
     const float px = xs[3 * p][tl], py = xs[3 * p + 1][tl], pz = xs[3 * p + 2][tl];
@@ -127,41 +130,49 @@ __device__ __forceinline__ void bm_pair_block(const float (*xs)[kBmTest], int tl
       tU[b] = make_float2(0.f, 0.f);
     }
 #pragma unroll
-    for (int q = 0; q < TN; q++) {
-      const float dx = yq[3 * q] - px, dy = yq[3 * q + 1] - py, dz = yq[3 * q + 2] - pz;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const float rinv = fminf(rsqrtf(r2), 1.0f / kEps);
-      const float r = fmaxf(r2 * rinv, kEps);
-      float s, c;
-      __sincosf(k * r, &s, &c);
-      const float gr = c * rinv, gi = s * rinv;
-      const float rinv2 = rinv * rinv;
-      const float hr = fmaf(k, s, gr) * rinv2;   // (c + kr s) / r^3
-      const float hi = fmaf(-k, c, gi) * rinv2;  // (s - kr c) / r^3
-      const float ur = dq[q] * hr, ui = dq[q] * hi;
+    for (int q0 = 0; q0 < TN; q0 += 2) {
+      constexpr int kLast = TN - 1;
+      const int q1 = q0 + 1 < TN ? q0 + 1 : kLast;  // an odd rule repeats its last point in the idle lane
+      const float2 dx = f2_sub(make_float2(yq[3 * q0], yq[3 * q1]), f2(px));
+      const float2 dy = f2_sub(make_float2(yq[3 * q0 + 1], yq[3 * q1 + 1]), f2(py));
+      const float2 dz = f2_sub(make_float2(yq[3 * q0 + 2], yq[3 * q1 + 2]), f2(pz));
+      const float2 r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
+      const float2 rinv = make_float2(fminf(rsqrtf(r2.x), 1.0f / kEps), fminf(rsqrtf(r2.y), 1.0f / kEps));
+      float2 r = f2_mul(r2, rinv);
+      r.x = fmaxf(r.x, kEps);
+      r.y = fmaxf(r.y, kEps);
+      const float2 kr = f2_mul(f2(k), r);
+      const float2 rinv2 = f2_mul(rinv, rinv);
+      float sc[2][2];  // [point][sin, cos]
+      __sincosf(kr.x, &sc[0][0], &sc[0][1]);
+      if (q0 + 1 < TN) __sincosf(kr.y, &sc[1][0], &sc[1][1]);
 #pragma unroll
-      for (int b = 0; b < 3; b++) {
-        const float w = bm_c<TN>(q, b);
-        tS[b].x = fmaf(w, gr, tS[b].x);
-        tS[b].y = fmaf(w, gi, tS[b].y);
-        tT[b].x = fmaf(w, hr, tT[b].x);
-        tT[b].y = fmaf(w, hi, tT[b].y);
-        tU[b].x = fmaf(w, ur, tU[b].x);
-        tU[b].y = fmaf(w, ui, tU[b].y);
+      for (int j = 0; j < 2; j++) {
+        if (q0 + j < TN) {
+          const int q = q0 + j;
+          const float ri = j == 0 ? rinv.x : rinv.y, ri2 = j == 0 ? rinv2.x : rinv2.y;
+          const float2 g = f2_mul(make_float2(sc[j][1], sc[j][0]), f2(ri));                  // (c, s) / r
+          const float2 h = f2_mul(f2_fma(kk, make_float2(sc[j][0], sc[j][1]), g), f2(ri2));  // (c + kr s, s - kr c) / r^3
+          const float2 u = f2_mul(f2(dq[q]), h);
+#pragma unroll
+          for (int b = 0; b < 3; b++) {
+            const float2 w = f2(bm_c<TN>(q, b));
+            tS[b] = f2_fma(w, g, tS[b]);
+            tT[b] = f2_fma(w, h, tT[b]);
+            tU[b] = f2_fma(w, u, tU[b]);
+          }
+        }
       }
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const float wa = bm_c<TN>(p, a);
-      const float wt = wa * dn;
+      const float2 wa2 = f2(wa), wt2 = f2(wa * dn);
 #pragma unroll
       for (int b = 0; b < 3; b++) {
-        aS[3 * a + b].x = fmaf(wa, tS[b].x, aS[3 * a + b].x);
-        aS[3 * a + b].y = fmaf(wa, tS[b].y, aS[3 * a + b].y);
-        aT[3 * a + b].x = fmaf(wt, tT[b].x, aT[3 * a + b].x);
-        aT[3 * a + b].y = fmaf(wt, tT[b].y, aT[3 * a + b].y);
-        aU[3 * a + b].x = fmaf(wa, tU[b].x, aU[3 * a + b].x);
-        aU[3 * a + b].y = fmaf(wa, tU[b].y, aU[3 * a + b].y);
+        aS[3 * a + b] = f2_fma(wa2, tS[b], aS[3 * a + b]);
+        aT[3 * a + b] = f2_fma(wt2, tT[b], aT[3 * a + b]);
+        aU[3 * a + b] = f2_fma(wa2, tU[b], aU[3 * a + b]);
       }
     }
   }
