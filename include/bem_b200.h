@@ -194,11 +194,13 @@ enum {
                                         not fit) */
   BEM_TUNE_TC_WAIT_US = 7,           /* limit of each bounded wait in the tensor-core matvec, microseconds
                                         (0: 2 s) */
-  BEM_TUNE_TC_TEST_SKIP_FILL = 8     /* test hook for the bounded waits, one launch: value v > 0 makes CTA 0
+  BEM_TUNE_TC_TEST_SKIP_FILL = 8,    /* test hook for the bounded waits, one launch: value v > 0 makes CTA 0
                                         of the next tensor-core matvec leave its (v-1)-th pipeline fill
                                         unissued, so the consumer's wait expires, the kernel drains its
                                         copies and returns, and bem_tc_status reports BEM_ERR_CUDA
                                         (no fault, no hang); 0 = off */
+  BEM_TUNE_GMRES_BLOCK = 9           /* bem_gmres_solve with 2..16 right-hand sides: 0 one block Krylov space
+                                        for all of them (block GMRES, the default), 1 one space per column */
 };
 int bem_set_tuning(int key, int value);
 int bem_get_tuning(int key);

@@ -55,6 +55,7 @@ TUNE_ASSEMBLY_CHUNK, TUNE_ASSEMBLY_CTAS_PER_SM, TUNE_TC_PROMOTE, TUNE_GMRES_REOR
 TUNE_ARNOLDI_MODE = 6
 TUNE_TC_WAIT_US = 7
 TUNE_TC_TEST_SKIP_FILL = 8
+TUNE_GMRES_BLOCK = 9
 
 
 class BatchProblem(ctypes.Structure):

@@ -44,6 +44,7 @@ extern int g_tc_promote;    // tensor-core matvec accumulator segment (tc_matvec
 extern int g_gmres_reorth;  // Gram-Schmidt passes of the Arnoldi step (linalg.cu)
 extern int g_arn_max_cluster;  // largest Arnoldi cluster size (linalg.cu)
 extern int g_arn_mode;         // Arnoldi step variant (linalg.cu)
+extern int g_gmres_block;      // block Krylov space for several right-hand sides (linalg.cu)
 extern int g_tc_wait_us;       // bounded-wait limit of the tensor-core kernels (tc_matvec.cu)
 extern std::atomic<int> g_tc_skip_fill;  // test hook of the tensor-core kernel (tc_matvec.cu)
 
@@ -1065,6 +1066,10 @@ int set_tuning(int key, int value) {
     case BEM_TUNE_TC_TEST_SKIP_FILL:
       g_tc_skip_fill.store(value);
       return BEM_OK;
+    case BEM_TUNE_GMRES_BLOCK:
+      if (value > 1) return BEM_ERR_INVALID_ARGUMENT;
+      g_gmres_block = value;
+      return BEM_OK;
   }
   return BEM_ERR_INVALID_ARGUMENT;
 }
@@ -1079,6 +1084,7 @@ int get_tuning(int key) {
     case BEM_TUNE_ARNOLDI_MODE: return g_arn_mode;
     case BEM_TUNE_TC_WAIT_US: return g_tc_wait_us;
     case BEM_TUNE_TC_TEST_SKIP_FILL: return g_tc_skip_fill.load();
+    case BEM_TUNE_GMRES_BLOCK: return g_gmres_block;
   }
   return -1;
 }

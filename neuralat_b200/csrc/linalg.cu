@@ -19,6 +19,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -38,6 +39,7 @@ int g_gmres_reorth = 0;     // Gram-Schmidt passes: 0 automatic, 1 one pass (CGS
 int g_arn_max_cluster = 0;  // largest Arnoldi cluster size tried (0: 16); a tuning knob
 int g_arn_mode = 0;         // Arnoldi step: 0 automatic (the cluster kernel), 1 cluster kernel, 2 streamed
                             // kernels, 3 cooperative kernel; a tuning knob
+int g_gmres_block = 0;      // 0: one block Krylov space for 2..16 right-hand sides, 1: separate spaces; a tuning knob
 
 // tensor-core operator (tc_matvec.cu)
 int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStream_t s);
@@ -1694,6 +1696,331 @@ __global__ void __launch_bounds__(kCoThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Block GMRES step (2 <= m <= kBkMaxP right-hand sides sharing ONE block
+// Krylov space).  On the BEM operators the block space converges in about a
+// quarter of the operator applications of m separate Krylov spaces (30
+// against 118 at s4 with 8 right-hand sides), because each application
+// extends the space by m directions.  Per step, one cooperative launch over
+// all SMs (CTAs own nr unknowns of every column):
+//   W = Y (this step's matvec output, FP64 in shared memory; Y cleared)
+//   H = Q^H W   basis staged 32 vectors at a time (converted to FP64 once),
+//               thread (vector, column) dots over the CTA's unknowns, FP64
+//               atomics into the step's H block column (by step parity)
+//   == grid barrier ==
+//   W' = W - Q H (same tiles, H staged beside them), Gram G = W'^H W'
+//               (FP64 atomics)
+//   == grid barrier ==
+//   CholQR: G = L L^H (every CTA, identically), Q_{j+1} = W' L^{-H} ->
+//               basis (complex64) and the next matvec operand; CTA 0 writes
+//               H and R_{j+1} = L^H to host-mapped memory
+// The small block least-squares problem (incremental Householder QR of the
+// block Hessenberg matrix and the residual estimate per right-hand side)
+// runs on the host, a few steps behind the GPU, so it never stalls the step.
+// A column that is dependent on the earlier ones (Cholesky pivot <= 1e-10 of
+// its own squared norm) or vanishes is reported as a breakdown: the cycle
+// ends with the steps before it (at the start block: per-column spaces).
+// ---------------------------------------------------------------------------
+constexpr int kBkThreads = 256;
+constexpr int kBkTile = 32;  // basis vectors staged per tile
+constexpr int kBkMaxP = 16;
+constexpr int kBkVectors = 384;  // basis vectors per cycle: kBkVectors / m block steps (at most the restart length)
+
+// Block steps per cycle for m right-hand sides and restart length R.
+__host__ __device__ inline int bk_steps(int m, int R) {
+  const int nb = kBkVectors / m;
+  return nb < R ? nb : R;
+}
+
+struct BkPtrs {
+  int p;           // block size (= number of right-hand sides)
+  int nb;          // block steps per cycle (bk_steps)
+  int nr;          // unknowns per CTA (even)
+  double* hacc;    // [2][(nb + 1) p][p][re, im]: H column block of the step, by step parity
+  double* gacc;    // [2][p][p][re, im]: Gram matrix of the step (parity 1 also serves the cycle start)
+  double2* Yb;     // [nb p][p]: least-squares solution uploaded by the host
+  int* step;       // block step j of the cycle (device)
+  double2* hostH;  // host-mapped [nb][(nb + 1) p][p]: H column block j incl. R_{j+1}
+  double2* hostR0; // host-mapped [p][p]: R_0 of the cycle's start block
+  int* hostS;      // host-mapped [nb + 1]: 1 step done, 2 breakdown (index nb: the start)
+};
+
+__device__ __forceinline__ double* bk_hacc(const BkPtrs& K, int par) {
+  return K.hacc + (size_t)par * (K.nb + 1) * K.p * K.p * 2;
+}
+__device__ __forceinline__ double* bk_gacc(const BkPtrs& K, int par) { return K.gacc + (size_t)par * K.p * K.p * 2; }
+
+// Dynamic shared memory of gm_block_kernel.
+struct BkLayout {
+  size_t W, Qt, Ht, G, total;
+  int qstride;  // double2 per staged basis vector (nr + 1: odd, conflict-free 16-byte reads)
+};
+__host__ __device__ inline BkLayout bk_layout(int p, int nr) {
+  BkLayout L;
+  size_t o = 0;
+  auto take = [&](size_t b) {
+    const size_t r = o;
+    o = (o + b + 15) / 16 * 16;
+    return r;
+  };
+  L.qstride = nr + 1;
+  L.W = take(sizeof(double2) * (size_t)p * nr);
+  L.Qt = take(sizeof(double2) * (size_t)kBkTile * L.qstride);
+  L.Ht = take(sizeof(double2) * (size_t)kBkTile * p);
+  L.G = take(sizeof(double2) * 2 * (size_t)p * p);  // G, then R = L^H
+  L.total = o;
+  return L;
+}
+
+// Basis vectors [a0, a0 + kBkTile) over this CTA's rows, converted to FP64.
+__device__ __forceinline__ void bk_stage_tile(const GmPtrs& P, int a0, int na, int i0, int nvr, int nr,
+                                              double2* Qt, int qs) {
+  for (int t = threadIdx.x; t < kBkTile * nr; t += kBkThreads) {
+    const int al = t / nr, i = t - al * nr;
+    double2 q = make_double2(0.0, 0.0);
+    if (al < na && i < nvr) {
+      const float2 f = P.Vb[(size_t)(a0 + al) * P.ldv + i0 + i];
+      q = make_double2(f.x, f.y);
+    }
+    Qt[al * qs + i] = q;
+  }
+}
+
+// mode 0: cycle start (W = r_in from P.w, CholQR -> Q_0, R_0); mode 1: step j.
+__global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtrs K, int mode) {
+  extern __shared__ __align__(16) unsigned char bk_raw[];
+  const int p = K.p, nr = K.nr, n = P.n;
+  const BkLayout Lo = bk_layout(p, nr);
+  double2* W = reinterpret_cast<double2*>(bk_raw + Lo.W);    // [p][nr]
+  double2* Qt = reinterpret_cast<double2*>(bk_raw + Lo.Qt);  // [kBkTile][qs]
+  double2* Ht = reinterpret_cast<double2*>(bk_raw + Lo.Ht);  // [kBkTile][p]
+  double2* G = reinterpret_cast<double2*>(bk_raw + Lo.G);    // [p][p], then R at G + p p
+  const int qs = Lo.qstride;
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * nr;
+  const int nvr = max(0, min(nr, n - i0));  // valid unknowns of this CTA
+  const int j = mode == 0 ? -1 : *K.step;   // read before any CTA can pass the second barrier
+  const int par = j & 1;                    // this step's sums (the start uses parity 1)
+  const int na_all = (j + 1) * p;           // basis vectors 0 .. na_all - 1 exist
+
+  // ---- load W, clear the next step's sums ----
+  if (mode == 0) {
+    if (P.f16 && blockIdx.x == 0 && tid < p) P.cinv[tid] = 1.f / kF16VecScale;  // operand scale of Q_0, Q_1, ...
+    for (int t = tid; t < p * nr; t += kBkThreads) {
+      const int b = t / nr, i = t - b * nr;
+      W[t] = i < nvr ? P.w[(size_t)b * n + i0 + i] : make_double2(0.0, 0.0);
+    }
+  } else {
+    for (int t = tid; t < p * nr; t += kBkThreads) {
+      const int i = t / p, b = t - i * p;
+      double2 w = make_double2(0.0, 0.0);
+      if (i < nvr) {
+        float2* y = P.Y + (size_t)(i0 + i) * P.m + b;
+        const float2 yv = *y;
+        w = make_double2(yv.x, yv.y);
+        *y = make_float2(0.f, 0.f);
+      }
+      W[b * nr + i] = w;
+    }
+  }
+  {
+    const int np = par ^ 1;
+    const size_t nh = (size_t)(K.nb + 1) * p * p * 2, ng = (size_t)p * p * 2;
+    double* hn = bk_hacc(K, np);
+    double* gn = bk_gacc(K, np);
+    for (size_t t = (size_t)blockIdx.x * kBkThreads + tid; t < nh + ng; t += (size_t)gridDim.x * kBkThreads) {
+      if (t < nh)
+        hn[t] = 0.0;
+      else
+        gn[t - nh] = 0.0;
+    }
+  }
+  __syncthreads();
+
+  double* hacc = bk_hacc(K, par);
+  if (mode == 1) {
+    // ---- H = Q^H W over this CTA's unknowns ----
+    for (int a0 = 0; a0 < na_all; a0 += kBkTile) {
+      const int na = min(kBkTile, na_all - a0);
+      bk_stage_tile(P, a0, na, i0, nvr, nr, Qt, qs);
+      __syncthreads();
+      for (int u = tid; u < kBkTile * p; u += kBkThreads) {
+        const int al = u & (kBkTile - 1), b = u / kBkTile;
+        if (al < na) {
+          const double2* q = Qt + al * qs;
+          const double2* w = W + b * nr;
+          double re = 0.0, im = 0.0;
+          for (int i = 0; i < nvr; i++) {  // conj(q) w
+            const double2 qq = q[i], ww = w[i];
+            re = fma(qq.x, ww.x, fma(qq.y, ww.y, re));
+            im = fma(qq.x, ww.y, fma(-qq.y, ww.x, im));
+          }
+          double* h = hacc + ((size_t)(a0 + al) * p + b) * 2;
+          if (re != 0.0) atomicAdd(h, re);
+          if (im != 0.0) atomicAdd(h + 1, im);
+        }
+      }
+      __syncthreads();
+    }
+    co_grid_sync(P.st);
+
+    // ---- W' = W - Q H ----
+    for (int a0 = 0; a0 < na_all; a0 += kBkTile) {
+      const int na = min(kBkTile, na_all - a0);
+      bk_stage_tile(P, a0, na, i0, nvr, nr, Qt, qs);
+      for (int t = tid; t < kBkTile * p; t += kBkThreads) {
+        const int al = t / p, b = t - al * p;
+        const double* h = hacc + ((size_t)(a0 + al) * p + b) * 2;
+        Ht[t] = al < na ? make_double2(__ldcg(h), __ldcg(h + 1)) : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+      for (int u = tid; u < p * nr; u += kBkThreads) {
+        const int b = u / nr, i = u - b * nr;
+        if (i < nvr) {
+          double2 w = W[u];
+          for (int al = 0; al < na; al++) {
+            const double2 qq = Qt[al * qs + i], hh = Ht[al * p + b];
+            w.x -= qq.x * hh.x - qq.y * hh.y;
+            w.y -= qq.x * hh.y + qq.y * hh.x;
+          }
+          W[u] = w;
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  // ---- Gram G = W^H W (FP64 atomics) ----
+  {
+    double* gacc = bk_gacc(K, par);
+    for (int u = tid; u < p * p; u += kBkThreads) {
+      const int b1 = u / p, b2 = u - b1 * p;
+      if (b2 < b1) continue;  // Hermitian: the upper triangle
+      const double2* w1 = W + b1 * nr;
+      const double2* w2 = W + b2 * nr;
+      double re = 0.0, im = 0.0;
+      for (int i = 0; i < nvr; i++) {  // conj(w1) w2
+        const double2 x = w1[i], y = w2[i];
+        re = fma(x.x, y.x, fma(x.y, y.y, re));
+        im = fma(x.x, y.y, fma(-x.y, y.x, im));
+      }
+      if (re != 0.0) atomicAdd(gacc + 2 * u, re);
+      if (im != 0.0) atomicAdd(gacc + 2 * u + 1, im);
+    }
+  }
+  co_grid_sync(P.st);
+
+  // ---- CholQR: G = L L^H, R = L^H (every CTA computes the same) ----
+  __shared__ int s_breakdown;
+  double2* R = G + p * p;  // R[c][b], upper triangular
+  if (tid == 0) {
+    const double* gacc = bk_gacc(K, par);
+    for (int u = 0; u < p * p; u++) {
+      const int b1 = u / p, b2 = u - b1 * p;
+      const int v = b2 >= b1 ? u : b2 * p + b1;  // lower triangle from the upper one
+      double2 g = make_double2(__ldcg(gacc + 2 * v), __ldcg(gacc + 2 * v + 1));
+      if (b2 < b1) g.y = -g.y;
+      G[u] = g;
+    }
+    double dmax = 0.0;
+    for (int b = 0; b < p; b++) dmax = fmax(dmax, G[b * p + b].x);
+    int bd = !(dmax > 0.0);
+    for (int u = 0; u < p * p; u++) R[u] = make_double2(0.0, 0.0);
+    // G = R^H R with R upper triangular (row-oriented Cholesky)
+    for (int c = 0; c < p && !bd; c++) {
+      double d = G[c * p + c].x;
+      for (int k = 0; k < c; k++) d -= R[k * p + c].x * R[k * p + c].x + R[k * p + c].y * R[k * p + c].y;
+      // a column dependent on the earlier ones to within 1e-5 in angle (the
+      // pivot relative to the column's own norm), or a vanishing column: CholQR
+      // would lose orthogonality (its error grows like the square of that ratio)
+      const double gcc = G[c * p + c].x;
+      if (!(gcc > 1e-30 * dmax) || !(d > 1e-10 * gcc)) {
+        bd = 1;
+        break;
+      }
+      const double rc = sqrt(d);
+      R[c * p + c] = make_double2(rc, 0.0);
+      for (int b = c + 1; b < p; b++) {
+        double2 x = G[c * p + b];
+        for (int k = 0; k < c; k++) {  // x -= conj(R[k][c]) R[k][b]
+          const double2 a = R[k * p + c], bb = R[k * p + b];
+          x.x -= a.x * bb.x + a.y * bb.y;
+          x.y -= a.x * bb.y - a.y * bb.x;
+        }
+        R[c * p + b] = make_double2(x.x / rc, x.y / rc);
+      }
+    }
+    s_breakdown = bd;
+  }
+  __syncthreads();
+  const bool breakdown = s_breakdown != 0;
+
+  // ---- Q_{j+1} = W R^{-1}: per unknown, forward substitution over the columns ----
+  if (!breakdown) {
+    const int qa0 = (j + 1) * p;  // first basis vector of the new block
+    for (int pr = tid; pr < nr / 2; pr += kBkThreads) {
+      const int il = 2 * pr;
+      if (il >= nvr) continue;
+      const int i = i0 + il;
+      double2 q0[kBkMaxP], q1[kBkMaxP];
+#pragma unroll
+      for (int b = 0; b < kBkMaxP; b++) {
+        if (b < p) {
+          double2 x0 = W[b * nr + il], x1 = W[b * nr + il + 1];
+          for (int c = 0; c < b; c++) {
+            const double2 r = R[c * p + b];
+            x0.x -= q0[c].x * r.x - q0[c].y * r.y;
+            x0.y -= q0[c].x * r.y + q0[c].y * r.x;
+            x1.x -= q1[c].x * r.x - q1[c].y * r.y;
+            x1.y -= q1[c].x * r.y + q1[c].y * r.x;
+          }
+          const double inv = 1.0 / R[b * p + b].x;
+          q0[b] = make_double2(x0.x * inv, x0.y * inv);
+          q1[b] = make_double2(x1.x * inv, x1.y * inv);
+          const float2 f0 = make_float2((float)q0[b].x, (float)q0[b].y);
+          const float2 f1 = i + 1 < n ? make_float2((float)q1[b].x, (float)q1[b].y) : make_float2(0.f, 0.f);
+          *reinterpret_cast<float4*>(P.Vb + (size_t)(qa0 + b) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+          store_operand(P, i, b, f0, f1);
+        }
+      }
+    }
+  }
+
+  // ---- CTA 0: H column block and R to the host, step record ----
+  if (blockIdx.x == 0) {
+    if (mode == 0) {
+      for (int u = tid; u < p * p; u += kBkThreads) K.hostR0[u] = R[u];
+    } else {
+      double2* hj = K.hostH + (size_t)j * (K.nb + 1) * p * p;
+      for (int u = tid; u < (na_all + p) * p; u += kBkThreads) {
+        const int a = u / p;
+        hj[u] = a < na_all ? make_double2(__ldcg(hacc + 2 * u), __ldcg(hacc + 2 * u + 1)) : R[u - na_all * p];
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence_system();
+      reinterpret_cast<volatile int*>(K.hostS)[mode == 0 ? K.nb : j] = breakdown ? 2 : 1;
+      *K.step = j + 1;
+    }
+  }
+}
+
+// D(:, s) += sum_{a < na} Q_a Y[a][s] for the block solution of the cycle.
+__global__ void gm_block_xupdate_kernel(GmPtrs P, BkPtrs K, int na) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (i >= P.n) return;
+  double2 acc = P.d[(size_t)s * P.n + i];
+  for (int a = 0; a < na; a++) {
+    const float2 v = P.Vb[(size_t)a * P.ldv + i];
+    const double2 t = cmul(make_double2(v.x, v.y), K.Yb[(size_t)a * K.p + s]);
+    acc.x += t.x;
+    acc.y += t.y;
+  }
+  P.d[(size_t)s * P.n + i] = acc;
+}
+
 // Back substitution H y = g on the Givens-reduced Hessenberg matrix, one
 // warp per column, column-oriented: y_j = g_j / H_jj, then the lanes update
 // g_0..g_{j-1} -= y_j H_{0..j-1, j} (column j of H is contiguous).
@@ -1871,7 +2198,7 @@ inline size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
 struct Layout {
   size_t Vb, H, cs, sn, g, w, d, x, r, X, Y, norm2, rnorm2, beta, tol, resid, active, kend, kcol, colstep, y, st,
-      bnorm2, hacc, nacc, tc, total;
+      bnorm2, hacc, nacc, bk_hacc, bk_gacc, bk_y, bk_step, tc, total;
 };
 
 Layout layout(int n, int m, int R, int precision) {
@@ -1907,6 +2234,13 @@ Layout layout(int n, int m, int R, int precision) {
   L.bnorm2 = take(sizeof(double) * m);
   L.hacc = take(sizeof(double) * 2 * (size_t)m * 4 * (R + 1));
   L.nacc = take(sizeof(double) * 2 * (size_t)m * 3);
+  // block solver state (used when 2 <= m <= kBkMaxP)
+  const bool bk = m >= 2 && m <= kBkMaxP;
+  const int nb = bk_steps(m, R);
+  L.bk_hacc = take(bk ? sizeof(double) * 2 * (size_t)(nb + 1) * m * m * 2 : 0);
+  L.bk_gacc = take(bk ? sizeof(double) * 2 * (size_t)m * m * 2 : 0);
+  L.bk_y = take(bk ? sizeof(double2) * (size_t)nb * m * m : 0);
+  L.bk_step = take(bk ? sizeof(int) : 0);
   L.tc = take(precision == BEM_PREC_FP32 ? 0 : tc_workspace_bytes(n, m, precision));
   L.total = o;
   return L;
@@ -1962,6 +2296,132 @@ int capture_graph(const std::function<int(cudaStream_t)>& body, cudaGraphExec_t*
   *nkern = launch_count() - l0;
   return BEM_OK;
 }
+
+// Host-mapped buffers of the block solver (H column blocks, R_0, step
+// status), one set per host thread, grown on demand.
+struct BlockHost {
+  double2* H = nullptr;  // host view [nb][(nb + 1) p][p]
+  double2* dH = nullptr;  // device view
+  double2* R0 = nullptr;
+  double2* dR0 = nullptr;
+  int* S = nullptr;
+  int* dS = nullptr;
+  size_t cap = 0;  // H entries the buffers hold
+  ~BlockHost() {
+    if (H) cudaFreeHost(H);
+    if (R0) cudaFreeHost(R0);
+    if (S) cudaFreeHost(S);
+  }
+};
+thread_local BlockHost t_block;
+
+int block_host(int p, int nb, BlockHost** out) {
+  const size_t need = (size_t)nb * (nb + 1) * p * p;
+  if (t_block.cap < need) {
+    if (t_block.H) cudaFreeHost(t_block.H);
+    if (t_block.R0) cudaFreeHost(t_block.R0);
+    if (t_block.S) cudaFreeHost(t_block.S);
+    t_block.H = t_block.R0 = nullptr;
+    t_block.S = nullptr;
+    t_block.cap = 0;
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.H, sizeof(double2) * need, cudaHostAllocMapped));
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.R0, sizeof(double2) * kBkMaxP * kBkMaxP, cudaHostAllocMapped));
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.S, sizeof(int) * (kBkVectors + 1), cudaHostAllocMapped));
+    BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_block.dH, t_block.H, 0));
+    BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_block.dR0, t_block.R0, 0));
+    BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_block.dS, t_block.S, 0));
+    t_block.cap = need;
+  }
+  *out = &t_block;
+  return BEM_OK;
+}
+
+// The block least-squares problem min || E1 R_0 - H_k Y || of block GMRES,
+// solved incrementally on the host: Householder reflections triangularise
+// the block Hessenberg matrix one block column at a time (column c has
+// nonzeros down to row c + p, so each reflection acts on p + 1 rows) and are
+// applied to the right-hand side Z = E1 R_0; the residual of right-hand side
+// b is the norm of Z's rows (k+1)p .. (k+2)p-1 below the triangle.
+struct BlockLS {
+  typedef std::complex<double> cd;
+  int p = 0, ld = 0, ncols = 0;
+  std::vector<cd> T, Z, U;   // T: ld x (nb p), Z: ld x p (column-major); U: reflections (p + 1 each)
+  std::vector<double> fac;   // 2 / (u^H u) of each reflection (0: identity)
+  void init(int p_, int nb, const double2* R0) {
+    p = p_;
+    ld = (nb + 1) * p;
+    ncols = 0;
+    T.assign((size_t)ld * nb * p, cd(0.0, 0.0));
+    Z.assign((size_t)ld * p, cd(0.0, 0.0));
+    U.assign((size_t)nb * p * (p + 1), cd(0.0, 0.0));
+    fac.assign((size_t)nb * p, 0.0);
+    for (int c = 0; c < p; c++)
+      for (int b = 0; b < p; b++) Z[(size_t)b * ld + c] = cd(R0[c * p + b].x, R0[c * p + b].y);
+  }
+  // y[r .. r+p] -= fac_r u_r (u_r^H y[r .. r+p])
+  void reflect(int r, cd* y) const {
+    const cd* u = &U[(size_t)r * (p + 1)];
+    cd d(0.0, 0.0);
+    for (int e = 0; e <= p; e++) d += std::conj(u[e]) * y[r + e];
+    d *= fac[r];
+    for (int e = 0; e <= p; e++) y[r + e] -= u[e] * d;
+  }
+  // block column j: hj[a][b], rows a < (j + 2) p; residual estimate per right-hand side.
+  // Returns false if the triangular factor is singular (a lost direction).
+  bool add(int j, const double2* hj, double* resid) {
+    const int c0 = j * p;
+    for (int t = 0; t < p; t++) {
+      cd* x = &T[(size_t)(c0 + t) * ld];
+      for (int a = 0; a < (j + 2) * p; a++) x[a] = cd(hj[a * p + t].x, hj[a * p + t].y);
+      for (int a = (j + 2) * p; a < ld; a++) x[a] = cd(0.0, 0.0);
+    }
+    for (int t = 0; t < p; t++) {
+      const int cc = c0 + t;
+      cd* x = &T[(size_t)cc * ld];
+      for (int r = 0; r < cc; r++)
+        if (fac[r] != 0.0) reflect(r, x);
+      // reflection for rows cc .. cc + p of column cc
+      double nrm2 = 0.0;
+      for (int e = 0; e <= p; e++) nrm2 += std::norm(x[cc + e]);
+      const double nrm = std::sqrt(nrm2);
+      if (!(nrm > 0.0)) return false;
+      const cd alpha = x[cc];
+      const cd ph = std::abs(alpha) > 0.0 ? alpha / std::abs(alpha) : cd(1.0, 0.0);
+      cd* u = &U[(size_t)cc * (p + 1)];
+      for (int e = 0; e <= p; e++) u[e] = x[cc + e];
+      u[0] += ph * nrm;
+      double uu = 0.0;
+      for (int e = 0; e <= p; e++) uu += std::norm(u[e]);
+      fac[cc] = uu > 0.0 ? 2.0 / uu : 0.0;
+      x[cc] = -ph * nrm;
+      for (int e = 1; e <= p; e++) x[cc + e] = cd(0.0, 0.0);
+      for (int b = 0; b < p; b++) reflect(cc, &Z[(size_t)b * ld]);
+    }
+    ncols = c0 + p;
+    for (int b = 0; b < p; b++) {
+      double r2 = 0.0;
+      for (int a = (j + 1) * p; a < (j + 2) * p; a++) r2 += std::norm(Z[(size_t)b * ld + a]);
+      resid[b] = std::sqrt(r2);
+    }
+    return true;
+  }
+  // Y (kk p x p, row a col b -> Y[a p + b]) solving T[0:kk p, 0:kk p] Y = Z[0:kk p, :]
+  void solve(int kk, std::vector<double2>& Y) const {
+    const int nc = kk * p;
+    Y.assign((size_t)nc * p, make_double2(0.0, 0.0));
+    std::vector<cd> y(nc);
+    for (int b = 0; b < p; b++) {
+      for (int a = 0; a < nc; a++) y[a] = Z[(size_t)b * ld + a];
+      for (int c = nc - 1; c >= 0; c--) {
+        const cd v = y[c] / T[(size_t)c * ld + c];
+        y[c] = v;
+        const cd* col = &T[(size_t)c * ld];
+        for (int a = 0; a < c; a++) y[a] -= col[a] * v;
+      }
+      for (int a = 0; a < nc; a++) Y[(size_t)a * p + b] = make_double2(y[a].real(), y[a].imag());
+    }
+  }
+};
 
 int host_ring(int m, HostRing** r) {
   if (!t_ring.ev[0])
@@ -2095,6 +2555,56 @@ int coop_shape(int n, int m, int R, CoShape* out) {
   return BEM_OK;
 }
 
+// Launch shape of gm_block_kernel: nr unknowns per CTA (even), one CTA per
+// SM at most, all resident (cooperative launch).
+struct BkShape {
+  int nr = 0, grid = 0;
+  size_t smem = 0;
+};
+
+int block_shape(int n, int p, BkShape* out) {
+  static std::atomic<bool> attr{false};
+  int dev = 0, coop_ok = 0, smem_optin = 0;
+  BEM_CUDA_TRY(cudaGetDevice(&dev));
+  BEM_CUDA_TRY(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
+  BEM_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (!coop_ok) return BEM_ERR_UNSUPPORTED;
+  const int sms = sm_count_linalg();
+  int nr = (n + sms - 1) / sms;
+  nr = std::max(16, (nr + 1) & ~1);
+  const int grid = (n + nr - 1) / nr;
+  const size_t smem = bk_layout(p, nr).total;
+  if (smem > (size_t)smem_optin / 2) return BEM_ERR_UNSUPPORTED;
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin / 2));
+    attr.store(true, std::memory_order_release);
+  }
+  int occ = 0;
+  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel, kBkThreads, smem));
+  if (occ < 1 || grid > occ * sms) return BEM_ERR_UNSUPPORTED;
+  out->nr = nr;
+  out->grid = grid;
+  out->smem = smem;
+  return BEM_OK;
+}
+
+int launch_block(const GmPtrs& P, const BkPtrs& K, const BkShape& sh, int mode, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)sh.grid, 1, 1);
+  cfg.blockDim = dim3(kBkThreads, 1, 1);
+  cfg.dynamicSmemBytes = sh.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel, P, K, mode));
+  count_launch();
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
 }  // namespace
 
 int cmatmul(const float2* A, int n, const float2* X, int m, float2* Y, cudaStream_t s) {
@@ -2166,6 +2676,26 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   double* rnorm2 = (double*)(w + L.rnorm2);
   void* tcws = w + L.tc;
   const int prec = params->precision;
+  // one block Krylov space for all right-hand sides (see gm_block_kernel)
+  BkPtrs K = {};
+  BkShape bshape;
+  BlockHost* bh = nullptr;
+  bool block = g_gmres_block == 0 && m >= 2 && m <= kBkMaxP && block_shape(n, m, &bshape) == BEM_OK;
+  const int nbk = bk_steps(m, R);
+  if (block) {
+    int rcb = block_host(m, nbk, &bh);
+    if (rcb) return rcb;
+    K.p = m;
+    K.nb = nbk;
+    K.nr = bshape.nr;
+    K.hacc = (double*)(w + L.bk_hacc);
+    K.gacc = (double*)(w + L.bk_gacc);
+    K.Yb = (double2*)(w + L.bk_y);
+    K.step = (int*)(w + L.bk_step);
+    K.hostH = bh->dH;
+    K.hostR0 = bh->dR0;
+    K.hostS = bh->dS;
+  }
   if (prec != BEM_PREC_FP32) {
     int rc = tc_operator_prepare((const float2*)A, n, prec, tcws, s);
     if (rc) return rc;
@@ -2292,6 +2822,21 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   cudaGraphExec_t& step_exec = step_guard.e;
   unsigned long long step_kernels = 0;
   bool step_direct_done = false;  // the first step runs uncaptured (sets kernel attributes)
+  // block step: the matvec of the block Q_j, then gm_block_kernel
+  auto block_step = [&](cudaStream_t st) -> int {
+    int r2 = prec == BEM_PREC_FP32 ? launch_cgemv((const float2*)A, n, P.X, m, P.Y, nullptr, st, &P.st->err)
+                                   : tc_gemm(tcws, n, prec, m, P.Y, nullptr, st);
+    if (r2) return r2;
+    return launch_block(P, K, bshape, 1, st);
+  };
+  ExecGuard block_guard;
+  cudaGraphExec_t& block_exec = block_guard.e;
+  unsigned long long block_kernels = 0;
+  bool block_direct_done = false;
+  BlockLS ls;
+  std::vector<double> bres(m), btol(m);
+  std::vector<double2> bY;
+  constexpr int kBkLookahead = 2;
   HostRing* ring;
   int rc = host_ring(m, &ring);
   if (rc) return rc;
@@ -2367,6 +2912,72 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       // absolute inner target: inner_rtol * ||r_out|| but never below rtol * ||b|| / 2
       (gm_start_scalar_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P, rnorm2, inner_rtol, 0.5 * params->rtol), count_launch());
       BEM_CUDA_TRY(cudaMemsetAsync(P.Y, 0, sizeof(float2) * (size_t)n * m, s));
+      if (block) {
+        // ---- one block Krylov space: start block Q_0 R_0 = r_in (CholQR) ----
+        first_cycle = false;
+        BEM_CUDA_TRY(cudaMemsetAsync(K.hacc, 0, sizeof(double) * 2 * (size_t)(nbk + 1) * m * m * 2, s));
+        BEM_CUDA_TRY(cudaMemsetAsync(K.gacc, 0, sizeof(double) * 2 * (size_t)m * m * 2, s));
+        for (int q = 0; q <= nbk; q++) bh->S[q] = 0;  // no step of this solve is in flight here
+        if ((rc = launch_block(P, K, bshape, 0, s))) return rc;
+        BEM_CUDA_TRY(cudaMemcpyAsync(btol.data(), P.tol, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+        BEM_CUDA_TRY(cudaStreamSynchronize(s));
+        if (reinterpret_cast<volatile int*>(bh->S)[nbk] != 1) {
+          // the residual block has lost rank (e.g. equal or zero columns):
+          // separate Krylov spaces for the rest of this solve
+          block = false;
+        } else {
+          ls.init(m, nbk, bh->R0);
+          int kk = 0, launched_c = 0, checked_c = 0;
+          bool conv = false, stop = false;
+          const long long bbase = launched;
+          auto process = [&](int jj) -> int {
+            BEM_CUDA_TRY(cudaEventSynchronize(ring->ev[(bbase + jj) % kSnapRing]));
+            if (stop) return BEM_OK;
+            if (reinterpret_cast<volatile int*>(bh->S)[jj] != 1 ||
+                !ls.add(jj, bh->H + (size_t)jj * (nbk + 1) * m * m, bres.data())) {
+              stop = true;  // breakdown: keep the steps before this one
+              return BEM_OK;
+            }
+            iters_done++;
+            kk = jj + 1;
+            bool all = true;
+            for (int c = 0; c < m; c++)
+              if (!(bres[c] <= btol[c])) all = false;
+            if (all) conv = stop = true;
+            return BEM_OK;
+          };
+          while (launched_c < nbk && total_iters < params->max_iters && !stop) {
+            if (!block_direct_done || !block_exec) {
+              if ((rc = block_step(s))) return rc;
+              if (!block_direct_done) {
+                block_direct_done = true;
+                if (capture_graph(block_step, &block_exec, &block_kernels) != BEM_OK) block_exec = nullptr;
+              }
+            } else {
+              BEM_CUDA_TRY(cudaGraphLaunch(block_exec, s));
+              count_launches(block_kernels);
+            }
+            BEM_CUDA_TRY(cudaEventRecord(ring->ev[launched % kSnapRing], s));
+            launched++;
+            launched_c++;
+            total_iters++;
+            while (checked_c < launched_c - kBkLookahead)
+              if ((rc = process(checked_c++))) return rc;
+          }
+          while (checked_c < launched_c)  // every launched step has finished after this
+            if ((rc = process(checked_c++))) return rc;
+          if (kk > 0) {
+            ls.solve(kk, bY);
+            BEM_CUDA_TRY(cudaMemcpyAsync(K.Yb, bY.data(), sizeof(double2) * bY.size(), cudaMemcpyHostToDevice, s));
+            (gm_block_xupdate_kernel<<<gv, 256, 0, s>>>(P, K, kk * m), count_launch());
+          }
+          if (conv) break;
+          if (kk == 0 && stop) {  // broke down at its first step: separate Krylov spaces instead
+            block = false;
+          }
+          continue;
+        }
+      }
       (gm_start_norm_kernel<<<pair_grid, kPairThreads, 0, s>>>(P), count_launch());
       first_cycle = false;
       int it = 0, checked = 0;
