@@ -19,7 +19,6 @@
 
 #include <atomic>
 #include <cmath>
-#include <complex>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -1702,18 +1701,24 @@ __global__ void __launch_bounds__(kCoThreads, 1)
 // quarter of the operator applications of m separate Krylov spaces (30
 // against 118 at s4 with 8 right-hand sides), because each application
 // extends the space by m directions.  Per step, one cooperative launch over
-// all SMs (CTAs own nr unknowns of every column):
+// all SMs (CTAs own nr unknowns of every column; the block size p is padded
+// to PP = 4, 8 or 16 columns):
 //   W = Y (this step's matvec output, FP64 in shared memory; Y cleared)
-//   H = Q^H W   basis staged 32 vectors at a time (converted to FP64 once),
-//               thread (vector, column) dots over the CTA's unknowns, FP64
-//               atomics into the step's H block column (by step parity)
+//   H = Q^H W   the basis rows over this CTA's unknowns stream through a ring
+//               of 32-vector stages (1-D bulk copies of the complex64 rows,
+//               converted to FP64 on use); thread (vector, 4 columns,
+//               unknown slice), slices reduced by shuffles; FP64 atomics into
+//               one of kBkCopies copies of the step's H block column, the
+//               tiles taken in a CTA-dependent order so that the CTAs' atomics
+//               spread over many L2 lines
 //   == grid barrier ==
-//   W' = W - Q H (same tiles, H staged beside them), Gram G = W'^H W'
-//               (FP64 atomics)
+//   W' = W - Q H (second pass over the ring, H staged once; thread (unknown,
+//               4 columns, vector slice), slices summed at the end), Gram
+//               G = W'^H W' (FP64 atomics, copies as for H)
 //   == grid barrier ==
-//   CholQR: G = L L^H (every CTA, identically), Q_{j+1} = W' L^{-H} ->
-//               basis (complex64) and the next matvec operand; CTA 0 writes
-//               H and R_{j+1} = L^H to host-mapped memory
+//   CholQR: G = R^H R and R^{-1} (one warp, every CTA identically),
+//               Q_{j+1} = W' R^{-1} -> basis (complex64) and the next matvec
+//               operand; CTA 0 writes H and R_{j+1} to host-mapped memory
 // The small block least-squares problem (incremental Householder QR of the
 // block Hessenberg matrix and the residual estimate per right-hand side)
 // runs on the host, a few steps behind the GPU, so it never stalls the step.
@@ -1721,10 +1726,12 @@ __global__ void __launch_bounds__(kCoThreads, 1)
 // its own squared norm) or vanishes is reported as a breakdown: the cycle
 // ends with the steps before it (at the start block: per-column spaces).
 // ---------------------------------------------------------------------------
-constexpr int kBkThreads = 256;
-constexpr int kBkTile = 32;  // basis vectors staged per tile
+constexpr int kBkThreads = 512;
+constexpr int kBkTile = 32;  // basis vectors per ring stage
 constexpr int kBkMaxP = 16;
 constexpr int kBkVectors = 384;  // basis vectors per cycle: kBkVectors / m block steps (at most the restart length)
+constexpr int kBkCopies = 4;     // copies of the H and Gram sums (CTA c adds into copy c % kBkCopies)
+constexpr int kBkMaxStages = 4;
 
 // Block steps per cycle for m right-hand sides and restart length R.
 __host__ __device__ inline int bk_steps(int m, int R) {
@@ -1732,12 +1739,24 @@ __host__ __device__ inline int bk_steps(int m, int R) {
   return nb < R ? nb : R;
 }
 
+// Shape of the per-CTA work (host-computed, see bk_geom).
+struct BkGeom {
+  int pp;      // padded block size: 4, 8 or 16
+  int hs;      // unknown slices of the dots (16 / (pp / 4))
+  int L;       // unknowns per slice (odd)
+  int lw;      // L * hs >= nr: padded unknowns of a W row
+  int rs;      // ring row stride in complex64 (>= lw, == hs mod 16, even)
+  int as;      // vector slices of the update
+  int stages;  // ring stages
+};
+
 struct BkPtrs {
   int p;           // block size (= number of right-hand sides)
   int nb;          // block steps per cycle (bk_steps)
   int nr;          // unknowns per CTA (even)
-  double* hacc;    // [2][(nb + 1) p][p][re, im]: H column block of the step, by step parity
-  double* gacc;    // [2][p][p][re, im]: Gram matrix of the step (parity 1 also serves the cycle start)
+  BkGeom g;
+  double* hacc;    // [2][kBkCopies][(nb + 1) p][p][re, im]: H column block of the step, by step parity
+  double* gacc;    // [2][kBkCopies][p][p][re, im]: Gram matrix of the step (parity 1 also serves the cycle start)
   double2* Yb;     // [nb p][p]: least-squares solution uploaded by the host
   int* step;       // block step j of the cycle (device)
   double2* hostH;  // host-mapped [nb][(nb + 1) p][p]: H column block j incl. R_{j+1}
@@ -1745,17 +1764,36 @@ struct BkPtrs {
   int* hostS;      // host-mapped [nb + 1]: 1 step done, 2 breakdown (index nb: the start)
 };
 
-__device__ __forceinline__ double* bk_hacc(const BkPtrs& K, int par) {
-  return K.hacc + (size_t)par * (K.nb + 1) * K.p * K.p * 2;
+__device__ __forceinline__ double* bk_hacc(const BkPtrs& K, int par, int copy) {
+  return K.hacc + ((size_t)par * kBkCopies + copy) * (K.nb + 1) * K.p * K.p * 2;
 }
-__device__ __forceinline__ double* bk_gacc(const BkPtrs& K, int par) { return K.gacc + (size_t)par * K.p * K.p * 2; }
+__device__ __forceinline__ double* bk_gacc(const BkPtrs& K, int par, int copy) {
+  return K.gacc + ((size_t)par * kBkCopies + copy) * K.p * K.p * 2;
+}
+
+__host__ __device__ inline BkGeom bk_geom(int p, int nr) {
+  BkGeom g;
+  g.pp = p <= 4 ? 4 : (p <= 8 ? 8 : 16);
+  const int cg = g.pp / 4;
+  g.hs = 16 / cg;
+  g.L = ((nr + g.hs - 1) / g.hs) | 1;
+  g.lw = g.L * g.hs;
+  // rows rs apart with rs == hs (mod 16) and odd L: the dots' 8-byte loads
+  // (hs slices x 32 / hs vectors per warp) hit every bank pair exactly twice
+  const int r = g.hs & 15;
+  g.rs = g.lw + ((r - g.lw % 16) + 16) % 16;
+  g.as = kBkThreads / (nr * cg);
+  if (g.as < 1) g.as = 1;
+  if (g.as > 32) g.as = 32;
+  g.stages = 0;
+  return g;
+}
 
 // Dynamic shared memory of gm_block_kernel.
 struct BkLayout {
-  size_t W, Qt, Ht, G, total;
-  int qstride;  // double2 per staged basis vector (nr + 1: odd, conflict-free 16-byte reads)
+  size_t ring, W, Hs, G, bars, total;
 };
-__host__ __device__ inline BkLayout bk_layout(int p, int nr) {
+__host__ __device__ inline BkLayout bk_layout(int p, int nr, const BkGeom& g, int na_max) {
   BkLayout L;
   size_t o = 0;
   auto take = [&](size_t b) {
@@ -1763,238 +1801,400 @@ __host__ __device__ inline BkLayout bk_layout(int p, int nr) {
     o = (o + b + 15) / 16 * 16;
     return r;
   };
-  L.qstride = nr + 1;
-  L.W = take(sizeof(double2) * (size_t)p * nr);
-  L.Qt = take(sizeof(double2) * (size_t)kBkTile * L.qstride);
-  L.Ht = take(sizeof(double2) * (size_t)kBkTile * p);
-  L.G = take(sizeof(double2) * 2 * (size_t)p * p);  // G, then R = L^H
+  const size_t ring = sizeof(float2) * (size_t)g.stages * kBkTile * g.rs;
+  const size_t part = sizeof(double2) * (size_t)(g.as - 1) * g.pp * nr;  // update slices, after the ring is drained
+  L.ring = take(ring > part ? ring : part);
+  L.W = take(sizeof(double2) * (size_t)g.pp * g.lw);
+  L.Hs = take(sizeof(double2) * (size_t)na_max * g.pp);
+  L.G = take(sizeof(double2) * 2 * (size_t)p * p + sizeof(double) * p);  // G / R^{-1}, R, 1 / R_cc
+  L.bars = take(sizeof(uint64_t) * kBkMaxStages);
   L.total = o;
   return L;
 }
 
-// Basis vectors [a0, a0 + kBkTile) over this CTA's rows, converted to FP64.
-__device__ __forceinline__ void bk_stage_tile(const GmPtrs& P, int a0, int na, int i0, int nvr, int nr,
-                                              double2* Qt, int qs) {
-  for (int t = threadIdx.x; t < kBkTile * nr; t += kBkThreads) {
-    const int al = t / nr, i = t - al * nr;
-    double2 q = make_double2(0.0, 0.0);
-    if (al < na && i < nvr) {
-      const float2 f = P.Vb[(size_t)(a0 + al) * P.ldv + i0 + i];
-      q = make_double2(f.x, f.y);
+// Sum of 8 values over HS lanes (xor partners): afterwards lane h holds
+// value h & 7 (HS >= 8) or values 2h, 2h + 1 (HS == 4) in v[0] (and v[1]).
+template <int HS>
+__device__ __forceinline__ void bk_reduce8(double (&v)[8], int h) {
+  if constexpr (HS == 16) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 8);
+  }
+  constexpr int top = HS >= 8 ? 4 : HS / 2;
+#pragma unroll
+  for (int o = top, half = 4; o >= 1; o >>= 1, half >>= 1) {
+    const bool hi = (h & o) != 0;
+#pragma unroll
+    for (int k = 0; k < half; k++) {
+      const double send = hi ? v[k] : v[k + half];
+      const double keep = hi ? v[k + half] : v[k];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
     }
-    Qt[al * qs + i] = q;
   }
 }
 
+// Ring stage s: tile (rot + s) mod T of the basis rows over unknowns
+// [i0, i0 + nvc) (nvc even: 16-byte rows), issued by the lanes of warp 0.
+__device__ __forceinline__ void bk_issue(const GmPtrs& P, const BkPtrs& K, float2* ring, uint64_t* bars, int s, int T,
+                                         int rot, int na_all, int i0, int nvc) {
+  const BkGeom& g = K.g;
+  const int slot = s % g.stages;
+  const int tile = (rot + s) % T;
+  const int a0 = tile * kBkTile, na = min(kBkTile, na_all - a0);
+  const int lane = threadIdx.x & 31;
+  const uint32_t bytes = (uint32_t)nvc * sizeof(float2);
+  if (lane == 0) mbar_expect_tx(&bars[slot], bytes * (uint32_t)na);
+  __syncwarp();
+  if (lane < na)
+    bulk_load(ring + ((size_t)slot * kBkTile + lane) * g.rs, P.Vb + (size_t)(a0 + lane) * P.ldv + i0, bytes,
+              &bars[slot]);
+}
+
 // mode 0: cycle start (W = r_in from P.w, CholQR -> Q_0, R_0); mode 1: step j.
+template <int PP>
 __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtrs K, int mode) {
+  constexpr int CG = PP / 4, HS = 16 / CG;
   extern __shared__ __align__(16) unsigned char bk_raw[];
   const int p = K.p, nr = K.nr, n = P.n;
-  const BkLayout Lo = bk_layout(p, nr);
-  double2* W = reinterpret_cast<double2*>(bk_raw + Lo.W);    // [p][nr]
-  double2* Qt = reinterpret_cast<double2*>(bk_raw + Lo.Qt);  // [kBkTile][qs]
-  double2* Ht = reinterpret_cast<double2*>(bk_raw + Lo.Ht);  // [kBkTile][p]
-  double2* G = reinterpret_cast<double2*>(bk_raw + Lo.G);    // [p][p], then R at G + p p
-  const int qs = Lo.qstride;
-  const int tid = threadIdx.x;
+  const BkGeom& g = K.g;
+  const int j = mode == 0 ? -1 : *K.step;  // read before any CTA can pass the second barrier
+  const int na_all = (j + 1) * p;          // basis vectors 0 .. na_all - 1 exist
+  const BkLayout Lo = bk_layout(p, nr, g, K.nb * p);
+  float2* ring = reinterpret_cast<float2*>(bk_raw + Lo.ring);  // [stages][kBkTile][rs]
+  double2* W = reinterpret_cast<double2*>(bk_raw + Lo.W);      // [PP][lw]
+  double2* Hs = reinterpret_cast<double2*>(bk_raw + Lo.Hs);    // [na_all][PP]
+  double2* G = reinterpret_cast<double2*>(bk_raw + Lo.G);      // [p][p]: G, then R^{-1}
+  double2* Rm = G + p * p;                                      // [p][p]: R
+  double* rinv = reinterpret_cast<double*>(Rm + p * p);         // [p]: 1 / R_cc
+  uint64_t* bars = reinterpret_cast<uint64_t*>(bk_raw + Lo.bars);
+  const int tid = threadIdx.x, lane = tid & 31, wq = tid >> 5;
   const int i0 = blockIdx.x * nr;
   const int nvr = max(0, min(nr, n - i0));  // valid unknowns of this CTA
-  const int j = mode == 0 ? -1 : *K.step;   // read before any CTA can pass the second barrier
+  const int nvc = (nvr + 1) & ~1;           // copied unknowns (the basis rows are zero-padded to even)
   const int par = j & 1;                    // this step's sums (the start uses parity 1)
-  const int na_all = (j + 1) * p;           // basis vectors 0 .. na_all - 1 exist
+  const int copy = blockIdx.x % kBkCopies;
+  const int T = (na_all + kBkTile - 1) / kBkTile;  // basis tiles
+  const int rot = T > 0 ? (int)(blockIdx.x % T) : 0;
+  int* err = &P.st->err;
 
-  // ---- load W, clear the next step's sums ----
+  // ---- ring start, W, clear the next step's sums ----
+  if (mode == 1) {
+    if (tid == 0) {
+      for (int s = 0; s < g.stages; s++) mbar_init(&bars[s], 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+    if (wq == 0)
+      for (int s = 0; s < min(g.stages, 2 * T); s++) bk_issue(P, K, ring, bars, s, T, rot, na_all, i0, nvc);
+    // the unknowns [nvc, lw) of every ring row stay zero (never written by the copies)
+    const int padw = g.lw - nvc;
+    for (int t = tid; t < g.stages * kBkTile * padw; t += kBkThreads) {
+      const int row = t / padw;
+      ring[(size_t)row * g.rs + nvc + (t - row * padw)] = make_float2(0.f, 0.f);
+    }
+  }
   if (mode == 0) {
     if (P.f16 && blockIdx.x == 0 && tid < p) P.cinv[tid] = 1.f / kF16VecScale;  // operand scale of Q_0, Q_1, ...
-    for (int t = tid; t < p * nr; t += kBkThreads) {
-      const int b = t / nr, i = t - b * nr;
-      W[t] = i < nvr ? P.w[(size_t)b * n + i0 + i] : make_double2(0.0, 0.0);
+    for (int t = tid; t < PP * g.lw; t += kBkThreads) {
+      const int b = t / g.lw, i = t - b * g.lw;
+      W[t] = (b < p && i < nvr) ? P.w[(size_t)b * n + i0 + i] : make_double2(0.0, 0.0);
     }
   } else {
-    for (int t = tid; t < p * nr; t += kBkThreads) {
-      const int i = t / p, b = t - i * p;
+    for (int t = tid; t < PP * g.lw; t += kBkThreads) {
+      const int i = t / PP, b = t - i * PP;
       double2 w = make_double2(0.0, 0.0);
-      if (i < nvr) {
+      if (i < nvr && b < p) {
         float2* y = P.Y + (size_t)(i0 + i) * P.m + b;
         const float2 yv = *y;
         w = make_double2(yv.x, yv.y);
         *y = make_float2(0.f, 0.f);
       }
-      W[b * nr + i] = w;
+      W[b * g.lw + i] = w;
     }
   }
   {
     const int np = par ^ 1;
     const size_t nh = (size_t)(K.nb + 1) * p * p * 2, ng = (size_t)p * p * 2;
-    double* hn = bk_hacc(K, np);
-    double* gn = bk_gacc(K, np);
-    for (size_t t = (size_t)blockIdx.x * kBkThreads + tid; t < nh + ng; t += (size_t)gridDim.x * kBkThreads) {
-      if (t < nh)
-        hn[t] = 0.0;
+    for (size_t t = (size_t)blockIdx.x * kBkThreads + tid; t < kBkCopies * (nh + ng);
+         t += (size_t)gridDim.x * kBkThreads) {
+      const int c = (int)(t / (nh + ng));
+      const size_t u = t - (size_t)c * (nh + ng);
+      if (u < nh)
+        bk_hacc(K, np, c)[u] = 0.0;
       else
-        gn[t - nh] = 0.0;
+        bk_gacc(K, np, c)[u - nh] = 0.0;
     }
   }
   __syncthreads();
 
-  double* hacc = bk_hacc(K, par);
   if (mode == 1) {
-    // ---- H = Q^H W over this CTA's unknowns ----
-    for (int a0 = 0; a0 < na_all; a0 += kBkTile) {
-      const int na = min(kBkTile, na_all - a0);
-      bk_stage_tile(P, a0, na, i0, nvr, nr, Qt, qs);
-      __syncthreads();
-      for (int u = tid; u < kBkTile * p; u += kBkThreads) {
-        const int al = u & (kBkTile - 1), b = u / kBkTile;
-        if (al < na) {
-          const double2* q = Qt + al * qs;
-          const double2* w = W + b * nr;
-          double re = 0.0, im = 0.0;
-          for (int i = 0; i < nvr; i++) {  // conj(q) w
-            const double2 qq = q[i], ww = w[i];
-            re = fma(qq.x, ww.x, fma(qq.y, ww.y, re));
-            im = fma(qq.x, ww.y, fma(-qq.y, ww.x, im));
-          }
-          double* h = hacc + ((size_t)(a0 + al) * p + b) * 2;
-          if (re != 0.0) atomicAdd(h, re);
-          if (im != 0.0) atomicAdd(h + 1, im);
+    double* hacc = bk_hacc(K, par, copy);
+    // ---- H = Q^H W: thread (vector, 4 columns, unknown slice) ----
+    const int d_cg = wq % CG;
+    const int d_al = (wq / CG) * (32 / HS) + lane / HS;
+    const int d_hs = lane % HS;
+    for (int s = 0; s < T; s++) {
+      const int slot = s % g.stages;
+      const int a0 = ((rot + s) % T) * kBkTile, na = min(kBkTile, na_all - a0);
+      mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
+      const float2* q = ring + ((size_t)slot * kBkTile + d_al) * g.rs + d_hs * g.L;
+      const double2* w = W + (size_t)(d_cg * 4) * g.lw + d_hs * g.L;
+      double v[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = 0.0;
+      for (int e = 0; e < g.L; e++) {  // conj(q) w
+        const float2 qf = q[e];
+        const double qx = qf.x, qy = qf.y;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const double2 wv = w[(size_t)c * g.lw + e];
+          v[2 * c] = fma(qx, wv.x, fma(qy, wv.y, v[2 * c]));
+          v[2 * c + 1] = fma(qx, wv.y, fma(-qy, wv.x, v[2 * c + 1]));
         }
       }
-      __syncthreads();
+      bk_reduce8<HS>(v, d_hs);
+      if (d_al < na) {
+        if constexpr (HS >= 8) {
+          const int b = d_cg * 4 + ((d_hs & 7) >> 1);
+          if (d_hs < 8 && b < p && v[0] != 0.0) atomicAdd(hacc + ((size_t)(a0 + d_al) * p + b) * 2 + (d_hs & 1), v[0]);
+        } else {
+          const int b = d_cg * 4 + d_hs;
+          if (b < p) {
+            double* hp = hacc + ((size_t)(a0 + d_al) * p + b) * 2;
+            if (v[0] != 0.0) atomicAdd(hp, v[0]);
+            if (v[1] != 0.0) atomicAdd(hp + 1, v[1]);
+          }
+        }
+      }
+      __syncthreads();  // stage consumed by every warp
+      if (wq == 0 && s + g.stages < 2 * T) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
     }
     co_grid_sync(P.st);
 
-    // ---- W' = W - Q H ----
-    for (int a0 = 0; a0 < na_all; a0 += kBkTile) {
-      const int na = min(kBkTile, na_all - a0);
-      bk_stage_tile(P, a0, na, i0, nvr, nr, Qt, qs);
-      for (int t = tid; t < kBkTile * p; t += kBkThreads) {
-        const int al = t / p, b = t - al * p;
-        const double* h = hacc + ((size_t)(a0 + al) * p + b) * 2;
-        Ht[t] = al < na ? make_double2(__ldcg(h), __ldcg(h + 1)) : make_double2(0.0, 0.0);
+    // ---- stage H (sum of the copies) ----
+    for (int t = tid; t < na_all * PP; t += kBkThreads) {
+      const int a = t / PP, b = t - a * PP;
+      double2 h = make_double2(0.0, 0.0);
+      if (b < p) {
+#pragma unroll
+        for (int c = 0; c < kBkCopies; c++) {
+          const double* hp = bk_hacc(K, par, c) + ((size_t)a * p + b) * 2;
+          h.x += __ldcg(hp);
+          h.y += __ldcg(hp + 1);
+        }
       }
-      __syncthreads();
-      for (int u = tid; u < p * nr; u += kBkThreads) {
-        const int b = u / nr, i = u - b * nr;
-        if (i < nvr) {
-          double2 w = W[u];
-          for (int al = 0; al < na; al++) {
-            const double2 qq = Qt[al * qs + i], hh = Ht[al * p + b];
-            w.x -= qq.x * hh.x - qq.y * hh.y;
-            w.y -= qq.x * hh.y + qq.y * hh.x;
+      Hs[t] = h;
+    }
+    __syncthreads();
+
+    // ---- W' = W - Q H: thread (unknown, 4 columns, vector slice) ----
+    const int u_as = tid / (nr * CG);
+    const int u_cg = (tid / nr) % CG;
+    const int u_i = tid % nr;
+    const bool u_on = u_as < g.as && u_i < nvr;
+    double2 acc[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
+    for (int s = T; s < 2 * T; s++) {
+      const int slot = s % g.stages;
+      const int a0 = ((rot + s) % T) * kBkTile, na = min(kBkTile, na_all - a0);
+      mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
+      if (u_on) {
+        const float2* q = ring + (size_t)slot * kBkTile * g.rs + u_i;
+        const double2* h = Hs + (size_t)a0 * PP + u_cg * 4;
+        for (int al = u_as; al < na; al += g.as) {
+          const float2 qf = q[(size_t)al * g.rs];
+          const double qx = qf.x, qy = qf.y;
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            const double2 hv = h[(size_t)al * PP + c];
+            acc[c].x = fma(qx, hv.x, fma(-qy, hv.y, acc[c].x));
+            acc[c].y = fma(qx, hv.y, fma(qy, hv.x, acc[c].y));
           }
-          W[u] = w;
         }
       }
       __syncthreads();
+      if (wq == 0 && s + g.stages < 2 * T) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
     }
+    // every issued stage has been waited for (after an error, a wait may have
+    // given up: the last stage issued into each slot is drained before the
+    // ring is reused for the slice sums)
+    if (tid == 0)
+      for (int sl = 0; sl < min(g.stages, 2 * T); sl++) {
+        const int s_last = sl + ((2 * T - 1 - sl) / g.stages) * g.stages;
+        mbar_wait_drain(&bars[sl], (uint32_t)(s_last / g.stages) & 1u);
+      }
+    __syncthreads();
+    double2* part = reinterpret_cast<double2*>(ring);  // [as - 1][CG][nr][4]
+    if (u_on && u_as > 0) {
+      double2* dst = part + (((size_t)(u_as - 1) * CG + u_cg) * nr + u_i) * 4;
+#pragma unroll
+      for (int c = 0; c < 4; c++) dst[c] = acc[c];
+    }
+    __syncthreads();
+    if (u_on && u_as == 0) {
+      for (int a = 1; a < g.as; a++) {
+        const double2* src = part + (((size_t)(a - 1) * CG + u_cg) * nr + u_i) * 4;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          acc[c].x += src[c].x;
+          acc[c].y += src[c].y;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        double2* wp = W + (size_t)(u_cg * 4 + c) * g.lw + u_i;
+        wp->x -= acc[c].x;
+        wp->y -= acc[c].y;
+      }
+    }
+    __syncthreads();
   }
 
-  // ---- Gram G = W^H W (FP64 atomics) ----
+  // ---- Gram G = W^H W (FP64 atomics): 16 lanes per upper-triangle entry ----
   {
-    double* gacc = bk_gacc(K, par);
-    for (int u = tid; u < p * p; u += kBkThreads) {
-      const int b1 = u / p, b2 = u - b1 * p;
-      if (b2 < b1) continue;  // Hermitian: the upper triangle
-      const double2* w1 = W + b1 * nr;
-      const double2* w2 = W + b2 * nr;
+    double* gacc = bk_gacc(K, par, copy);
+    const int nent = p * (p + 1) / 2;
+    const int nu = (16 * nent + 31) & ~31;  // whole warps: every lane takes part in the shuffles
+    for (int u = tid; u < nu; u += kBkThreads) {
+      const int e = u >> 4, k = u & 15;  // entry, row slice
+      int b1 = 0, b2 = 0;
       double re = 0.0, im = 0.0;
-      for (int i = 0; i < nvr; i++) {  // conj(w1) w2
-        const double2 x = w1[i], y = w2[i];
-        re = fma(x.x, y.x, fma(x.y, y.y, re));
-        im = fma(x.x, y.y, fma(-x.y, y.x, im));
+      if (e < nent) {
+        int rem = e;
+        while (rem >= p - b1) {  // e -> (b1, b2), b2 >= b1
+          rem -= p - b1;
+          b1++;
+        }
+        b2 = b1 + rem;
+        const double2* w1 = W + (size_t)b1 * g.lw;
+        const double2* w2 = W + (size_t)b2 * g.lw;
+        for (int i = k; i < nvr; i += 16) {  // conj(w1) w2
+          const double2 x = w1[i], y = w2[i];
+          re = fma(x.x, y.x, fma(x.y, y.y, re));
+          im = fma(x.x, y.y, fma(-x.y, y.x, im));
+        }
       }
-      if (re != 0.0) atomicAdd(gacc + 2 * u, re);
-      if (im != 0.0) atomicAdd(gacc + 2 * u + 1, im);
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+      }
+      if (k == 0 && e < nent) {
+        const int v = b1 * p + b2;
+        if (re != 0.0) atomicAdd(gacc + 2 * v, re);
+        if (im != 0.0) atomicAdd(gacc + 2 * v + 1, im);
+      }
     }
   }
   co_grid_sync(P.st);
 
-  // ---- CholQR: G = L L^H, R = L^H (every CTA computes the same) ----
+  // ---- CholQR: G = R^H R (R upper triangular), R^{-1}; warp 0, lane b owns column b ----
   __shared__ int s_breakdown;
-  double2* R = G + p * p;  // R[c][b], upper triangular
-  if (tid == 0) {
-    const double* gacc = bk_gacc(K, par);
-    for (int u = 0; u < p * p; u++) {
+  if (wq == 0) {
+    for (int u = lane; u < p * p; u += 32) {
       const int b1 = u / p, b2 = u - b1 * p;
       const int v = b2 >= b1 ? u : b2 * p + b1;  // lower triangle from the upper one
-      double2 g = make_double2(__ldcg(gacc + 2 * v), __ldcg(gacc + 2 * v + 1));
-      if (b2 < b1) g.y = -g.y;
-      G[u] = g;
+      double2 gv = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < kBkCopies; c++) {
+        const double* gp = bk_gacc(K, par, c) + 2 * v;
+        gv.x += __ldcg(gp);
+        gv.y += __ldcg(gp + 1);
+      }
+      if (b2 < b1) gv.y = -gv.y;
+      G[u] = gv;
+      Rm[u] = make_double2(0.0, 0.0);
     }
-    double dmax = 0.0;
-    for (int b = 0; b < p; b++) dmax = fmax(dmax, G[b * p + b].x);
+    __syncwarp();
+    const double gown = lane < p ? G[lane * p + lane].x : 0.0;  // the column's own squared norm
+    double dmax = gown;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
     int bd = !(dmax > 0.0);
-    for (int u = 0; u < p * p; u++) R[u] = make_double2(0.0, 0.0);
-    // G = R^H R with R upper triangular (row-oriented Cholesky)
+    // right-looking: row c of R from the updated row c of G, then the trailing update
     for (int c = 0; c < p && !bd; c++) {
-      double d = G[c * p + c].x;
-      for (int k = 0; k < c; k++) d -= R[k * p + c].x * R[k * p + c].x + R[k * p + c].y * R[k * p + c].y;
+      const double d = G[c * p + c].x;
+      const double gcc = __shfl_sync(0xffffffffu, gown, c);
       // a column dependent on the earlier ones to within 1e-5 in angle (the
-      // pivot relative to the column's own norm), or a vanishing column: CholQR
-      // would lose orthogonality (its error grows like the square of that ratio)
-      const double gcc = G[c * p + c].x;
+      // pivot relative to the column's own norm), or a vanishing column:
+      // CholQR would lose orthogonality (its error grows like the square of that ratio)
       if (!(gcc > 1e-30 * dmax) || !(d > 1e-10 * gcc)) {
         bd = 1;
         break;
       }
-      const double rc = sqrt(d);
-      R[c * p + c] = make_double2(rc, 0.0);
-      for (int b = c + 1; b < p; b++) {
-        double2 x = G[c * p + b];
-        for (int k = 0; k < c; k++) {  // x -= conj(R[k][c]) R[k][b]
-          const double2 a = R[k * p + c], bb = R[k * p + b];
-          x.x -= a.x * bb.x + a.y * bb.y;
-          x.y -= a.x * bb.y - a.y * bb.x;
+      const double rc = sqrt(d), ri = 1.0 / rc;
+      double2 rcb = make_double2(0.0, 0.0);
+      if (lane == c) {
+        Rm[c * p + c] = make_double2(rc, 0.0);
+        rinv[c] = ri;
+      } else if (lane > c && lane < p) {
+        const double2 x = G[c * p + lane];
+        rcb = make_double2(x.x * ri, x.y * ri);
+        Rm[c * p + lane] = rcb;
+      }
+      __syncwarp();
+      if (lane > c && lane < p) {  // G[b1][lane] -= conj(R[c][b1]) R[c][lane], c < b1 <= lane
+        for (int b1 = c + 1; b1 <= lane; b1++) {
+          const double2 a = Rm[c * p + b1];
+          double2* gp = &G[b1 * p + lane];
+          gp->x -= a.x * rcb.x + a.y * rcb.y;
+          gp->y -= a.x * rcb.y - a.y * rcb.x;
         }
-        R[c * p + b] = make_double2(x.x / rc, x.y / rc);
+      }
+      __syncwarp();
+    }
+    if (!bd && lane < p) {
+      // column b = lane of R^{-1} by back substitution (into G, which is no longer needed)
+      const int b = lane;
+      for (int c = p - 1; c > b; c--) G[c * p + b] = make_double2(0.0, 0.0);
+      for (int c = b; c >= 0; c--) {
+        double2 x = make_double2(c == b ? 1.0 : 0.0, 0.0);
+        for (int k = c + 1; k <= b; k++) {  // x -= R[c][k] Ri[k][b]
+          const double2 r = Rm[c * p + k], y = G[k * p + b];
+          x.x -= r.x * y.x - r.y * y.y;
+          x.y -= r.x * y.y + r.y * y.x;
+        }
+        G[c * p + b] = make_double2(x.x * rinv[c], x.y * rinv[c]);
       }
     }
-    s_breakdown = bd;
+    if (lane == 0) s_breakdown = bd;
   }
   __syncthreads();
   const bool breakdown = s_breakdown != 0;
 
-  // ---- Q_{j+1} = W R^{-1}: per unknown, forward substitution over the columns ----
+  // ---- Q_{j+1} = W R^{-1}: thread per (unknown pair, column) ----
   if (!breakdown) {
     const int qa0 = (j + 1) * p;  // first basis vector of the new block
-    for (int pr = tid; pr < nr / 2; pr += kBkThreads) {
-      const int il = 2 * pr;
+    const int np2 = (nr + 1) / 2;
+    for (int u = tid; u < p * np2; u += kBkThreads) {
+      const int b = u / np2, il = 2 * (u - b * np2);
       if (il >= nvr) continue;
       const int i = i0 + il;
-      double2 q0[kBkMaxP], q1[kBkMaxP];
-#pragma unroll
-      for (int b = 0; b < kBkMaxP; b++) {
-        if (b < p) {
-          double2 x0 = W[b * nr + il], x1 = W[b * nr + il + 1];
-          for (int c = 0; c < b; c++) {
-            const double2 r = R[c * p + b];
-            x0.x -= q0[c].x * r.x - q0[c].y * r.y;
-            x0.y -= q0[c].x * r.y + q0[c].y * r.x;
-            x1.x -= q1[c].x * r.x - q1[c].y * r.y;
-            x1.y -= q1[c].x * r.y + q1[c].y * r.x;
-          }
-          const double inv = 1.0 / R[b * p + b].x;
-          q0[b] = make_double2(x0.x * inv, x0.y * inv);
-          q1[b] = make_double2(x1.x * inv, x1.y * inv);
-          const float2 f0 = make_float2((float)q0[b].x, (float)q0[b].y);
-          const float2 f1 = i + 1 < n ? make_float2((float)q1[b].x, (float)q1[b].y) : make_float2(0.f, 0.f);
-          *reinterpret_cast<float4*>(P.Vb + (size_t)(qa0 + b) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
-          store_operand(P, i, b, f0, f1);
-        }
+      double2 q0 = make_double2(0.0, 0.0), q1 = make_double2(0.0, 0.0);
+      for (int c = 0; c <= b; c++) {
+        const double2 r = G[c * p + b], x0 = W[(size_t)c * g.lw + il], x1 = W[(size_t)c * g.lw + il + 1];
+        q0.x += x0.x * r.x - x0.y * r.y;
+        q0.y += x0.x * r.y + x0.y * r.x;
+        q1.x += x1.x * r.x - x1.y * r.y;
+        q1.y += x1.x * r.y + x1.y * r.x;
       }
+      const float2 f0 = make_float2((float)q0.x, (float)q0.y);
+      const float2 f1 = i + 1 < n ? make_float2((float)q1.x, (float)q1.y) : make_float2(0.f, 0.f);
+      *reinterpret_cast<float4*>(P.Vb + (size_t)(qa0 + b) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+      store_operand(P, i, b, f0, f1);
     }
   }
 
   // ---- CTA 0: H column block and R to the host, step record ----
   if (blockIdx.x == 0) {
     if (mode == 0) {
-      for (int u = tid; u < p * p; u += kBkThreads) K.hostR0[u] = R[u];
+      for (int u = tid; u < p * p; u += kBkThreads) K.hostR0[u] = Rm[u];
     } else {
       double2* hj = K.hostH + (size_t)j * (K.nb + 1) * p * p;
       for (int u = tid; u < (na_all + p) * p; u += kBkThreads) {
         const int a = u / p;
-        hj[u] = a < na_all ? make_double2(__ldcg(hacc + 2 * u), __ldcg(hacc + 2 * u + 1)) : R[u - na_all * p];
+        hj[u] = a < na_all ? Hs[(size_t)a * PP + (u - a * p)] : Rm[u - na_all * p];
       }
     }
     __syncthreads();
@@ -2237,8 +2437,8 @@ Layout layout(int n, int m, int R, int precision) {
   // block solver state (used when 2 <= m <= kBkMaxP)
   const bool bk = m >= 2 && m <= kBkMaxP;
   const int nb = bk_steps(m, R);
-  L.bk_hacc = take(bk ? sizeof(double) * 2 * (size_t)(nb + 1) * m * m * 2 : 0);
-  L.bk_gacc = take(bk ? sizeof(double) * 2 * (size_t)m * m * 2 : 0);
+  L.bk_hacc = take(bk ? sizeof(double) * 2 * kBkCopies * (size_t)(nb + 1) * m * m * 2 : 0);
+  L.bk_gacc = take(bk ? sizeof(double) * 2 * kBkCopies * (size_t)m * m * 2 : 0);
   L.bk_y = take(bk ? sizeof(double2) * (size_t)nb * m * m : 0);
   L.bk_step = take(bk ? sizeof(int) : 0);
   L.tc = take(precision == BEM_PREC_FP32 ? 0 : tc_workspace_bytes(n, m, precision));
@@ -2343,64 +2543,84 @@ int block_host(int p, int nb, BlockHost** out) {
 // applied to the right-hand side Z = E1 R_0; the residual of right-hand side
 // b is the norm of Z's rows (k+1)p .. (k+2)p-1 below the triangle.
 struct BlockLS {
-  typedef std::complex<double> cd;
+  // complex values as (re, im) pairs with explicit arithmetic (no library
+  // complex multiply: its IEEE special-value handling makes it many times slower)
+  struct C {
+    double x, y;
+  };
+  static C mul(C a, C b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+  static C cmulc(C a, C b) { return {a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x}; }  // conj(a) b
   int p = 0, ld = 0, ncols = 0;
-  std::vector<cd> T, Z, U;   // T: ld x (nb p), Z: ld x p (column-major); U: reflections (p + 1 each)
-  std::vector<double> fac;   // 2 / (u^H u) of each reflection (0: identity)
+  std::vector<C> T, Z, U;   // T: ld x (nb p), Z: ld x p (column-major); U: reflections (p + 1 each)
+  std::vector<double> fac;  // 2 / (u^H u) of each reflection (0: identity)
   void init(int p_, int nb, const double2* R0) {
     p = p_;
     ld = (nb + 1) * p;
     ncols = 0;
-    T.assign((size_t)ld * nb * p, cd(0.0, 0.0));
-    Z.assign((size_t)ld * p, cd(0.0, 0.0));
-    U.assign((size_t)nb * p * (p + 1), cd(0.0, 0.0));
+    T.assign((size_t)ld * nb * p, C{0.0, 0.0});
+    Z.assign((size_t)ld * p, C{0.0, 0.0});
+    U.assign((size_t)nb * p * (p + 1), C{0.0, 0.0});
     fac.assign((size_t)nb * p, 0.0);
     for (int c = 0; c < p; c++)
-      for (int b = 0; b < p; b++) Z[(size_t)b * ld + c] = cd(R0[c * p + b].x, R0[c * p + b].y);
+      for (int b = 0; b < p; b++) Z[(size_t)b * ld + c] = C{R0[c * p + b].x, R0[c * p + b].y};
   }
   // y[r .. r+p] -= fac_r u_r (u_r^H y[r .. r+p])
-  void reflect(int r, cd* y) const {
-    const cd* u = &U[(size_t)r * (p + 1)];
-    cd d(0.0, 0.0);
-    for (int e = 0; e <= p; e++) d += std::conj(u[e]) * y[r + e];
-    d *= fac[r];
-    for (int e = 0; e <= p; e++) y[r + e] -= u[e] * d;
+  void reflect(int r, C* y) const {
+    const C* u = &U[(size_t)r * (p + 1)];
+    C d{0.0, 0.0};
+    for (int e = 0; e <= p; e++) {
+      const C t = cmulc(u[e], y[r + e]);
+      d.x += t.x;
+      d.y += t.y;
+    }
+    d.x *= fac[r];
+    d.y *= fac[r];
+    for (int e = 0; e <= p; e++) {
+      const C t = mul(u[e], d);
+      y[r + e].x -= t.x;
+      y[r + e].y -= t.y;
+    }
   }
   // block column j: hj[a][b], rows a < (j + 2) p; residual estimate per right-hand side.
   // Returns false if the triangular factor is singular (a lost direction).
   bool add(int j, const double2* hj, double* resid) {
     const int c0 = j * p;
     for (int t = 0; t < p; t++) {
-      cd* x = &T[(size_t)(c0 + t) * ld];
-      for (int a = 0; a < (j + 2) * p; a++) x[a] = cd(hj[a * p + t].x, hj[a * p + t].y);
-      for (int a = (j + 2) * p; a < ld; a++) x[a] = cd(0.0, 0.0);
+      C* x = &T[(size_t)(c0 + t) * ld];
+      for (int a = 0; a < (j + 2) * p; a++) x[a] = C{hj[a * p + t].x, hj[a * p + t].y};
+      for (int a = (j + 2) * p; a < ld; a++) x[a] = C{0.0, 0.0};
     }
     for (int t = 0; t < p; t++) {
       const int cc = c0 + t;
-      cd* x = &T[(size_t)cc * ld];
+      C* x = &T[(size_t)cc * ld];
       for (int r = 0; r < cc; r++)
         if (fac[r] != 0.0) reflect(r, x);
       // reflection for rows cc .. cc + p of column cc
       double nrm2 = 0.0;
-      for (int e = 0; e <= p; e++) nrm2 += std::norm(x[cc + e]);
+      for (int e = 0; e <= p; e++) nrm2 += x[cc + e].x * x[cc + e].x + x[cc + e].y * x[cc + e].y;
       const double nrm = std::sqrt(nrm2);
       if (!(nrm > 0.0)) return false;
-      const cd alpha = x[cc];
-      const cd ph = std::abs(alpha) > 0.0 ? alpha / std::abs(alpha) : cd(1.0, 0.0);
-      cd* u = &U[(size_t)cc * (p + 1)];
+      const C alpha = x[cc];
+      const double aa = std::sqrt(alpha.x * alpha.x + alpha.y * alpha.y);
+      const C ph = aa > 0.0 ? C{alpha.x / aa, alpha.y / aa} : C{1.0, 0.0};
+      C* u = &U[(size_t)cc * (p + 1)];
       for (int e = 0; e <= p; e++) u[e] = x[cc + e];
-      u[0] += ph * nrm;
+      u[0].x += ph.x * nrm;
+      u[0].y += ph.y * nrm;
       double uu = 0.0;
-      for (int e = 0; e <= p; e++) uu += std::norm(u[e]);
+      for (int e = 0; e <= p; e++) uu += u[e].x * u[e].x + u[e].y * u[e].y;
       fac[cc] = uu > 0.0 ? 2.0 / uu : 0.0;
-      x[cc] = -ph * nrm;
-      for (int e = 1; e <= p; e++) x[cc + e] = cd(0.0, 0.0);
+      x[cc] = C{-ph.x * nrm, -ph.y * nrm};
+      for (int e = 1; e <= p; e++) x[cc + e] = C{0.0, 0.0};
       for (int b = 0; b < p; b++) reflect(cc, &Z[(size_t)b * ld]);
     }
     ncols = c0 + p;
     for (int b = 0; b < p; b++) {
       double r2 = 0.0;
-      for (int a = (j + 1) * p; a < (j + 2) * p; a++) r2 += std::norm(Z[(size_t)b * ld + a]);
+      for (int a = (j + 1) * p; a < (j + 2) * p; a++) {
+        const C z = Z[(size_t)b * ld + a];
+        r2 += z.x * z.x + z.y * z.y;
+      }
       resid[b] = std::sqrt(r2);
     }
     return true;
@@ -2409,16 +2629,21 @@ struct BlockLS {
   void solve(int kk, std::vector<double2>& Y) const {
     const int nc = kk * p;
     Y.assign((size_t)nc * p, make_double2(0.0, 0.0));
-    std::vector<cd> y(nc);
+    std::vector<C> y(nc);
     for (int b = 0; b < p; b++) {
       for (int a = 0; a < nc; a++) y[a] = Z[(size_t)b * ld + a];
       for (int c = nc - 1; c >= 0; c--) {
-        const cd v = y[c] / T[(size_t)c * ld + c];
+        const C d = T[(size_t)c * ld + c];
+        const double dd = d.x * d.x + d.y * d.y;
+        const C v = {(y[c].x * d.x + y[c].y * d.y) / dd, (y[c].y * d.x - y[c].x * d.y) / dd};
         y[c] = v;
-        const cd* col = &T[(size_t)c * ld];
-        for (int a = 0; a < c; a++) y[a] -= col[a] * v;
+        const C* col = &T[(size_t)c * ld];
+        for (int a = 0; a < c; a++) {
+          y[a].x -= col[a].x * v.x - col[a].y * v.y;
+          y[a].y -= col[a].x * v.y + col[a].y * v.x;
+        }
       }
-      for (int a = 0; a < nc; a++) Y[(size_t)a * p + b] = make_double2(y[a].real(), y[a].imag());
+      for (int a = 0; a < nc; a++) Y[(size_t)a * p + b] = make_double2(y[a].x, y[a].y);
     }
   }
 };
@@ -2556,14 +2781,25 @@ int coop_shape(int n, int m, int R, CoShape* out) {
 }
 
 // Launch shape of gm_block_kernel: nr unknowns per CTA (even), one CTA per
-// SM at most, all resident (cooperative launch).
+// SM at most, all resident (cooperative launch); the most ring stages (4 .. 2)
+// that fit the shared memory.
 struct BkShape {
   int nr = 0, grid = 0;
+  BkGeom g{};
   size_t smem = 0;
 };
 
-int block_shape(int n, int p, BkShape* out) {
+template <int PP>
+int block_attr(int smem_optin) {
   static std::atomic<bool> attr{false};
+  if (!attr.load(std::memory_order_acquire)) {
+    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_block_kernel<PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin - 1024));
+    attr.store(true, std::memory_order_release);
+  }
+  return BEM_OK;
+}
+
+int block_shape(int n, int p, int R, BkShape* out) {
   int dev = 0, coop_ok = 0, smem_optin = 0;
   BEM_CUDA_TRY(cudaGetDevice(&dev));
   BEM_CUDA_TRY(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
@@ -2572,18 +2808,29 @@ int block_shape(int n, int p, BkShape* out) {
   const int sms = sm_count_linalg();
   int nr = (n + sms - 1) / sms;
   nr = std::max(16, (nr + 1) & ~1);
+  if (nr > 256) return BEM_ERR_UNSUPPORTED;
   const int grid = (n + nr - 1) / nr;
-  const size_t smem = bk_layout(p, nr).total;
-  if (smem > (size_t)smem_optin / 2) return BEM_ERR_UNSUPPORTED;
-  if (!attr.load(std::memory_order_acquire)) {
-    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin / 2));
-    attr.store(true, std::memory_order_release);
+  BkGeom g = bk_geom(p, nr);
+  const int na_max = bk_steps(p, R) * p;
+  size_t smem = 0;
+  for (g.stages = kBkMaxStages; g.stages >= 2; g.stages--) {
+    smem = bk_layout(p, nr, g, na_max).total;
+    if (smem + 1024 <= (size_t)smem_optin) break;
   }
+  if (g.stages < 2) return BEM_ERR_UNSUPPORTED;
+  int rc = g.pp == 4 ? block_attr<4>(smem_optin) : g.pp == 8 ? block_attr<8>(smem_optin) : block_attr<16>(smem_optin);
+  if (rc) return rc;
   int occ = 0;
-  BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel, kBkThreads, smem));
+  if (g.pp == 4)
+    BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel<4>, kBkThreads, smem));
+  else if (g.pp == 8)
+    BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel<8>, kBkThreads, smem));
+  else
+    BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel<16>, kBkThreads, smem));
   if (occ < 1 || grid > occ * sms) return BEM_ERR_UNSUPPORTED;
   out->nr = nr;
   out->grid = grid;
+  out->g = g;
   out->smem = smem;
   return BEM_OK;
 }
@@ -2599,7 +2846,12 @@ int launch_block(const GmPtrs& P, const BkPtrs& K, const BkShape& sh, int mode, 
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel, P, K, mode));
+  if (sh.g.pp == 4)
+    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel<4>, P, K, mode));
+  else if (sh.g.pp == 8)
+    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel<8>, P, K, mode));
+  else
+    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel<16>, P, K, mode));
   count_launch();
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
@@ -2680,7 +2932,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   BkPtrs K = {};
   BkShape bshape;
   BlockHost* bh = nullptr;
-  bool block = g_gmres_block == 0 && m >= 2 && m <= kBkMaxP && block_shape(n, m, &bshape) == BEM_OK;
+  bool block = g_gmres_block == 0 && m >= 2 && m <= kBkMaxP && block_shape(n, m, R, &bshape) == BEM_OK;
   const int nbk = bk_steps(m, R);
   if (block) {
     int rcb = block_host(m, nbk, &bh);
@@ -2688,6 +2940,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     K.p = m;
     K.nb = nbk;
     K.nr = bshape.nr;
+    K.g = bshape.g;
     K.hacc = (double*)(w + L.bk_hacc);
     K.gacc = (double*)(w + L.bk_gacc);
     K.Yb = (double2*)(w + L.bk_y);
@@ -2915,8 +3168,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       if (block) {
         // ---- one block Krylov space: start block Q_0 R_0 = r_in (CholQR) ----
         first_cycle = false;
-        BEM_CUDA_TRY(cudaMemsetAsync(K.hacc, 0, sizeof(double) * 2 * (size_t)(nbk + 1) * m * m * 2, s));
-        BEM_CUDA_TRY(cudaMemsetAsync(K.gacc, 0, sizeof(double) * 2 * (size_t)m * m * 2, s));
+        BEM_CUDA_TRY(cudaMemsetAsync(K.hacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)(nbk + 1) * m * m * 2, s));
+        BEM_CUDA_TRY(cudaMemsetAsync(K.gacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)m * m * 2, s));
         for (int q = 0; q <= nbk; q++) bh->S[q] = 0;  // no step of this solve is in flight here
         if ((rc = launch_block(P, K, bshape, 0, s))) return rc;
         BEM_CUDA_TRY(cudaMemcpyAsync(btol.data(), P.tol, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
