@@ -192,6 +192,119 @@ int launch_cmatmul(const float2* A, int n, const typename C2<T>::type* X, int ld
 }
 
 // ---------------------------------------------------------------------------
+// FP64 residual R = B - A X (A complex64, X and R complex128) for the outer
+// refinement, FP64 products and sums.  The work is FP64-bound (4 DFMA per
+// complex product, n^2 m of them), so the layout keeps the FP64 pipe fed:
+// thread = row, A read 16 complex (one 128-byte line) per lane per step, the
+// CTA's X columns staged in shared memory and read as warp broadcasts (one
+// wavefront per 16 bytes for all 32 rows), 8 right-hand sides accumulated
+// per thread.  CTAs cover 256 rows x kRsCols columns; the column ranges'
+// partial sums meet in R by FP64 atomics (R zeroed first), then
+// resid_finish_kernel forms B - R and the squared norms.  n even (16-byte
+// rows); odd n takes cmatmul_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kRsThreads = 256;
+constexpr int kRsCols = 320;  // columns per CTA (multiple of 16)
+constexpr int kRsRhs = 8;     // right-hand sides per CTA (blockIdx.z groups)
+
+__global__ void __launch_bounds__(kRsThreads, 2)
+    resid_f64_kernel(const float2* __restrict__ A, int n, const double2* __restrict__ X, int m,
+                     double2* __restrict__ R) {
+  __shared__ double2 xs[kRsCols * kRsRhs];  // [column][rhs]
+  const int c0 = blockIdx.y * kRsCols;
+  const int cn = min(kRsCols, n - c0);
+  const int s0 = blockIdx.z * kRsRhs;
+  const int ms = min(kRsRhs, m - s0);
+  for (int e = threadIdx.x; e < kRsCols * kRsRhs; e += kRsThreads) {
+    const int c = e / kRsRhs, s = e - c * kRsRhs;
+    xs[e] = (c < cn && s < ms) ? X[(size_t)(c0 + c) * m + s0 + s] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const int row = blockIdx.x * kRsThreads + threadIdx.x;
+  if (row >= n) return;  // after the only barrier
+  const float4* a4 = reinterpret_cast<const float4*>(A + (size_t)row * n + c0);  // n even: 16-byte aligned
+  double acc[kRsRhs][2];
+#pragma unroll
+  for (int s = 0; s < kRsRhs; s++) acc[s][0] = acc[s][1] = 0.0;
+  const int cfull = cn & ~15;
+  for (int c = 0; c < cfull; c += 16) {
+    float4 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = __ldcs(a4 + c / 2 + k);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const double ar = h ? v[k].z : v[k].x, ai = h ? v[k].w : v[k].y;
+        const double2* xc = xs + (size_t)(c + 2 * k + h) * kRsRhs;
+#pragma unroll
+        for (int s = 0; s < kRsRhs; s++) {
+          const double2 x = xc[s];
+          acc[s][0] = fma(ar, x.x, fma(-ai, x.y, acc[s][0]));
+          acc[s][1] = fma(ar, x.y, fma(ai, x.x, acc[s][1]));
+        }
+      }
+    }
+  }
+  const float2* a2 = A + (size_t)row * n + c0;
+  for (int c = cfull; c < cn; c++) {
+    const float2 v = __ldcs(a2 + c);
+    const double ar = v.x, ai = v.y;
+#pragma unroll
+    for (int s = 0; s < kRsRhs; s++) {
+      const double2 x = xs[(size_t)c * kRsRhs + s];
+      acc[s][0] = fma(ar, x.x, fma(-ai, x.y, acc[s][0]));
+      acc[s][1] = fma(ar, x.y, fma(ai, x.x, acc[s][1]));
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < kRsRhs; s++) {
+    if (s < ms) {
+      double* r = reinterpret_cast<double*>(R + (size_t)row * m + s0 + s);
+      atomicAdd(r, acc[s][0]);
+      atomicAdd(r + 1, acc[s][1]);
+    }
+  }
+}
+
+// R = B - R (R holding A X) and norm2[s] += |R[:, s]|^2.
+__global__ void __launch_bounds__(256) resid_finish_kernel(const float2* __restrict__ B, int n, int m,
+                                                           double2* __restrict__ R, double* __restrict__ norm2) {
+  __shared__ double red[256];
+  const int s = blockIdx.y;
+  double sum = 0.0;
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+    const size_t e = (size_t)i * m + s;
+    const float2 b = B[e];
+    double2 r = R[e];
+    r.x = (double)b.x - r.x;
+    r.y = (double)b.y - r.y;
+    R[e] = r;
+    sum += r.x * r.x + r.y * r.y;
+  }
+  red[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(&norm2[s], red[0]);
+}
+
+// R = B - A X, norm2[s] += |R[:, s]|^2 (X, R: n x m row-major complex128; B: complex64).
+int launch_resid_f64(const float2* A, int n, const double2* X, int m, double2* R, const float2* B, double* norm2,
+                     cudaStream_t s) {
+  if (n & 1) return launch_cmatmul<double, 1>(A, n, X, m, m, R, m, B, m, norm2, nullptr, s);
+  BEM_CUDA_TRY(cudaMemsetAsync(R, 0, sizeof(double2) * (size_t)n * m, s));
+  const dim3 grid((n + kRsThreads - 1) / kRsThreads, (n + kRsCols - 1) / kRsCols, (m + kRsRhs - 1) / kRsRhs);
+  (resid_f64_kernel<<<grid, kRsThreads, 0, s>>>(A, n, X, m, R), count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  (resid_finish_kernel<<<dim3(std::min(148, (n + 255) / 256), m), 256, 0, s>>>(B, n, m, R, norm2), count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // FP32 complex matvec Y += A X (HBM-streaming, CUDA cores, 4 FMA per complex
 // product), for the FP32 precision mode and the right-hand side -V g.
 //
@@ -1771,11 +1884,15 @@ __device__ __forceinline__ double* bk_gacc(const BkPtrs& K, int par, int copy) {
   return K.gacc + ((size_t)par * kBkCopies + copy) * K.p * K.p * 2;
 }
 
+// Unknown slices of the dots for padded block size pp (the host geometry and
+// the kernel's compile-time lane layout both take it from here).
+__host__ __device__ constexpr int bk_slices(int pp) { return 16 / (pp / 4); }
+
 __host__ __device__ inline BkGeom bk_geom(int p, int nr) {
   BkGeom g;
   g.pp = p <= 4 ? 4 : (p <= 8 ? 8 : 16);
   const int cg = g.pp / 4;
-  g.hs = 16 / cg;
+  g.hs = bk_slices(g.pp);
   g.L = ((nr + g.hs - 1) / g.hs) | 1;
   g.lw = g.L * g.hs;
   // rows rs apart with rs == hs (mod 16) and odd L: the dots' 8-byte loads
@@ -1853,7 +1970,7 @@ __device__ __forceinline__ void bk_issue(const GmPtrs& P, const BkPtrs& K, float
 // mode 0: cycle start (W = r_in from P.w, CholQR -> Q_0, R_0); mode 1: step j.
 template <int PP>
 __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtrs K, int mode) {
-  constexpr int CG = PP / 4, HS = 16 / CG;
+  constexpr int CG = PP / 4, HS = bk_slices(PP);
   extern __shared__ __align__(16) unsigned char bk_raw[];
   const int p = K.p, nr = K.nr, n = P.n;
   const BkGeom& g = K.g;
@@ -1876,6 +1993,10 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
   const int T = (na_all + kBkTile - 1) / kBkTile;  // basis tiles
   const int rot = T > 0 ? (int)(blockIdx.x % T) : 0;
   int* err = &P.st->err;
+  if (g.hs != HS) {  // host geometry built for another lane layout (uniform over the grid)
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
 
   // ---- ring start, W, clear the next step's sums ----
   if (mode == 1) {
@@ -3113,7 +3234,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     // outer FP64 residual r = b - A x against the FP32 matrix
     BEM_CUDA_TRY(cudaMemsetAsync(rnorm2, 0, sizeof(double) * m, s));
     if (x_nonzero) {
-      rc = launch_cmatmul<double, 1>((const float2*)A, n, P.x, m, m, P.r, m, (const float2*)B, m, rnorm2, nullptr, s);
+      rc = launch_resid_f64((const float2*)A, n, P.x, m, P.r, (const float2*)B, rnorm2, s);
       if (rc) return rc;
       matvecs++;
     } else {
