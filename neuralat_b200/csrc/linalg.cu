@@ -3210,7 +3210,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   BlockLS ls;
   std::vector<double> bres(m), btol(m);
   std::vector<double2> bY;
-  constexpr int kBkLookahead = 2;
+  constexpr int kBkLookahead = 1;  // one step queued behind the one the host examines
   HostRing* ring;
   int rc = host_ring(m, &ring);
   if (rc) return rc;
