@@ -469,26 +469,50 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     __syncthreads();
 
     // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
+    // Pass 1, in place: for every trial corner column, the row of test
+    // vertex A's first corner gets the sum over A's test corners (the corner
+    // rows of different vertices are disjoint).  Pass 2: entry (A, B) is the
+    // sum over B's trial corners along that row.  Short independent chains
+    // instead of one (corner x corner) loop per entry.
     const TileRec& TI = sm.tileI;
-    const int nJ = tileJ.nlv;
-    const int total = TI.nlv * nJ;
-    for (int e = tid; e < total; e += kSymThreads) {
+    const int nI = TI.nlv, nJ = tileJ.nlv;
+    const int ncol = 3 * ntriJ;
+    for (int e = tid; e < nI * ncol; e += kSymThreads) {
+      const int a = e / ncol;
+      const int col = e - a * ncol;
+      const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+      const int rep = TI.lv_corner[ca0];
+      float2 v = sm.slotV[rep][col], kk = sm.slotK[rep][col], mm = sm.slotM[rep][col];
+      for (int ca = ca0 + 1; ca < ca1; ca++) {
+        const int row = TI.lv_corner[ca];
+        const float2 v1 = sm.slotV[row][col], k1 = sm.slotK[row][col], m1 = sm.slotM[row][col];
+        v.x += v1.x;
+        v.y += v1.y;
+        kk.x += k1.x;
+        kk.y += k1.y;
+        mm.x += m1.x;
+        mm.y += m1.y;
+      }
+      sm.slotV[rep][col] = v;
+      sm.slotK[rep][col] = kk;
+      sm.slotM[rep][col] = mm;
+    }
+    __syncthreads();
+    for (int e = tid; e < nI * nJ; e += kSymThreads) {
       const int a = e / nJ;
       const int b = e - a * nJ;
-      float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f), acc_m = make_float2(0.f, 0.f);
-      const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+      const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
-      for (int ca = ca0; ca < ca1; ca++) {
-        const int row = TI.lv_corner[ca];
-        for (int cb = cb0; cb < cb1; cb++) {
-          const int col = tileJ.lv_corner[cb];
-          acc_v.x += sm.slotV[row][col].x;
-          acc_v.y += sm.slotV[row][col].y;
-          acc_k.x += sm.slotK[row][col].x;
-          acc_k.y += sm.slotK[row][col].y;
-          acc_m.x += sm.slotM[row][col].x;
-          acc_m.y += sm.slotM[row][col].y;
-        }
+      float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f), acc_m = make_float2(0.f, 0.f);
+      for (int cb = cb0; cb < cb1; cb++) {
+        const int col = tileJ.lv_corner[cb];
+        const float2 v1 = sm.slotV[rep][col], k1 = sm.slotK[rep][col], m1 = sm.slotM[rep][col];
+        acc_v.x += v1.x;
+        acc_v.y += v1.y;
+        acc_k.x += k1.x;
+        acc_k.y += k1.y;
+        acc_m.x += m1.x;
+        acc_m.y += m1.y;
       }
       const int A = TI.vid[a], B = tileJ.vid[b];
       if (acc_v.x != 0.f || acc_v.y != 0.f || acc_k.x != 0.f || acc_k.y != 0.f || acc_m.x != 0.f ||

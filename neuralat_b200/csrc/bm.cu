@@ -285,28 +285,56 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
     __syncthreads();
 
     // ---- reduce corner slots onto distinct vertices: (A, B) and (B, A) ----
+    // Pass 1, in place: for every trial corner column, the row of test
+    // vertex A's first corner gets the sum over A's test corners (corner rows
+    // of different vertices are disjoint); pass 2: entry (A, B) sums B's
+    // trial corners along that row.
     const TileRec& TI = sm.tileI;
-    const int nJ = tileJ.nlv;
-    const int total = TI.nlv * nJ;
-    for (int e = tid; e < total; e += kBmThreads) {
+    const int nI = TI.nlv, nJ = tileJ.nlv;
+    const int ncol = 3 * ntriJ;
+    for (int e = tid; e < nI * ncol; e += kBmThreads) {
+      const int a = e / ncol;
+      const int col = e - a * ncol;
+      const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+      const int rep = TI.lv_corner[ca0];
+      float2 l = sm.slotL[rep][col], lt = sm.slotLT[rep][col], rr = sm.slotR[rep][col], rt = sm.slotRT[rep][col];
+      for (int ca = ca0 + 1; ca < ca1; ca++) {
+        const int row = TI.lv_corner[ca];
+        const float2 l1 = sm.slotL[row][col], lt1 = sm.slotLT[row][col];
+        const float2 r1 = sm.slotR[row][col], rt1 = sm.slotRT[row][col];
+        l.x += l1.x;
+        l.y += l1.y;
+        lt.x += lt1.x;
+        lt.y += lt1.y;
+        rr.x += r1.x;
+        rr.y += r1.y;
+        rt.x += rt1.x;
+        rt.y += rt1.y;
+      }
+      sm.slotL[rep][col] = l;
+      sm.slotLT[rep][col] = lt;
+      sm.slotR[rep][col] = rr;
+      sm.slotRT[rep][col] = rt;
+    }
+    __syncthreads();
+    for (int e = tid; e < nI * nJ; e += kBmThreads) {
       const int a = e / nJ;
       const int b = e - a * nJ;
-      float2 l = make_float2(0.f, 0.f), lt = l, rr = l, rt = l;
-      const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+      const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
-      for (int ca = ca0; ca < ca1; ca++) {
-        const int row = TI.lv_corner[ca];
-        for (int cb = cb0; cb < cb1; cb++) {
-          const int col = tileJ.lv_corner[cb];
-          l.x += sm.slotL[row][col].x;
-          l.y += sm.slotL[row][col].y;
-          lt.x += sm.slotLT[row][col].x;
-          lt.y += sm.slotLT[row][col].y;
-          rr.x += sm.slotR[row][col].x;
-          rr.y += sm.slotR[row][col].y;
-          rt.x += sm.slotRT[row][col].x;
-          rt.y += sm.slotRT[row][col].y;
-        }
+      float2 l = make_float2(0.f, 0.f), lt = l, rr = l, rt = l;
+      for (int cb = cb0; cb < cb1; cb++) {
+        const int col = tileJ.lv_corner[cb];
+        const float2 l1 = sm.slotL[rep][col], lt1 = sm.slotLT[rep][col];
+        const float2 r1 = sm.slotR[rep][col], rt1 = sm.slotRT[rep][col];
+        l.x += l1.x;
+        l.y += l1.y;
+        lt.x += lt1.x;
+        lt.y += lt1.y;
+        rr.x += r1.x;
+        rr.y += r1.y;
+        rt.x += rt1.x;
+        rt.y += rt1.y;
       }
       const int A = TI.vid[a], B = tileJ.vid[b];
       if (l.x != 0.f || l.y != 0.f || lt.x != 0.f || lt.y != 0.f || rr.x != 0.f || rr.y != 0.f || rt.x != 0.f ||
