@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -1840,20 +1841,36 @@ __global__ void __launch_bounds__(kCoThreads, 1)
 // ends with the steps before it (at the start block: per-column spaces).
 // ---------------------------------------------------------------------------
 constexpr int kBkThreads = 512;
-constexpr int kBkTile = 32;  // basis vectors per ring stage
+constexpr int kBkTileMax = 32;  // basis vectors per ring stage: 32, or 16 when a CTA's unknowns are many
 constexpr int kBkMaxP = 16;
+constexpr int kBkMaxGroups = 4;                    // 17 .. 64 right-hand sides: groups of <= 16 columns,
+constexpr int kBkMaxRhs = kBkMaxP * kBkMaxGroups;  // each its own block space, one shared matvec per step
 constexpr int kBkVectors = 384;  // basis vectors per cycle: kBkVectors / m block steps (at most the restart length)
 constexpr int kBkCopies = 4;     // copies of the H and Gram sums (CTA c adds into copy c % kBkCopies)
 constexpr int kBkMaxStages = 4;
 
-// Block steps per cycle for m right-hand sides and restart length R.
-__host__ __device__ inline int bk_steps(int m, int R) {
-  const int nb = kBkVectors / m;
+// Block steps per cycle for blocks of p columns and restart length R.
+__host__ __device__ inline int bk_steps(int p, int R) {
+  const int nb = kBkVectors / p;
   return nb < R ? nb : R;
+}
+
+// Groups of m right-hand sides (2 <= m <= kBkMaxRhs): ceil(m / 16) groups,
+// sizes as equal as possible (each >= 2).
+inline int bk_groups(int m, int* size, int* col0) {
+  const int G = (m + kBkMaxP - 1) / kBkMaxP;
+  int c = 0;
+  for (int g = 0; g < G; g++) {
+    size[g] = m / G + (g < m % G ? 1 : 0);
+    col0[g] = c;
+    c += size[g];
+  }
+  return G;
 }
 
 // Shape of the per-CTA work (host-computed, see bk_geom).
 struct BkGeom {
+  int tile;    // basis vectors per ring stage (16 or 32)
   int pp;      // padded block size: 4, 8 or 16
   int hs;      // unknown slices of the dots (16 / (pp / 4))
   int L;       // unknowns per slice (odd)
@@ -1864,8 +1881,10 @@ struct BkGeom {
 };
 
 struct BkPtrs {
-  int p;           // block size (= number of right-hand sides)
-  int nb;          // block steps per cycle (bk_steps)
+  int p;           // block size (the right-hand sides of this group)
+  int col0;        // first right-hand side (column) of the group
+  int vbase;       // first basis row of the group in P.Vb
+  int nb;          // block steps per cycle
   int nr;          // unknowns per CTA (even)
   BkGeom g;
   double* hacc;    // [2][kBkCopies][(nb + 1) p][p][re, im]: H column block of the step, by step parity
@@ -1886,13 +1905,14 @@ __device__ __forceinline__ double* bk_gacc(const BkPtrs& K, int par, int copy) {
 
 // Unknown slices of the dots for padded block size pp (the host geometry and
 // the kernel's compile-time lane layout both take it from here).
-__host__ __device__ constexpr int bk_slices(int pp) { return 16 / (pp / 4); }
+__host__ __device__ constexpr int bk_slices(int pp, int tile) { return kBkThreads / (tile * (pp / 4)); }
 
-__host__ __device__ inline BkGeom bk_geom(int p, int nr) {
+__host__ __device__ inline BkGeom bk_geom(int p, int nr, int tile) {
   BkGeom g;
+  g.tile = tile;
   g.pp = p <= 4 ? 4 : (p <= 8 ? 8 : 16);
   const int cg = g.pp / 4;
-  g.hs = bk_slices(g.pp);
+  g.hs = bk_slices(g.pp, tile);
   g.L = ((nr + g.hs - 1) / g.hs) | 1;
   g.lw = g.L * g.hs;
   // rows rs apart with rs == hs (mod 16) and odd L: the dots' 8-byte loads
@@ -1918,7 +1938,7 @@ __host__ __device__ inline BkLayout bk_layout(int p, int nr, const BkGeom& g, in
     o = (o + b + 15) / 16 * 16;
     return r;
   };
-  const size_t ring = sizeof(float2) * (size_t)g.stages * kBkTile * g.rs;
+  const size_t ring = sizeof(float2) * (size_t)g.stages * g.tile * g.rs;
   const size_t part = sizeof(double2) * (size_t)(g.as - 1) * g.pp * nr;  // update slices, after the ring is drained
   L.ring = take(ring > part ? ring : part);
   L.W = take(sizeof(double2) * (size_t)g.pp * g.lw);
@@ -1929,14 +1949,16 @@ __host__ __device__ inline BkLayout bk_layout(int p, int nr, const BkGeom& g, in
   return L;
 }
 
-// Sum of 8 values over HS lanes (xor partners): afterwards lane h holds
-// value h & 7 (HS >= 8) or values 2h, 2h + 1 (HS == 4) in v[0] (and v[1]).
+// Sum of 8 values over HS lanes (xor partners, lane bits below HS): lanes
+// first fold whole sets while HS > 8, then exchange halves (transpose-
+// reduce); afterwards lane h holds value h & 7 (HS >= 8) or values 2h, 2h + 1
+// (HS == 4) in v[0] (and v[1]).
 template <int HS>
 __device__ __forceinline__ void bk_reduce8(double (&v)[8], int h) {
-  if constexpr (HS == 16) {
 #pragma unroll
-    for (int k = 0; k < 8; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 8);
-  }
+  for (int o = HS / 2; o >= 8; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
   constexpr int top = HS >= 8 ? 4 : HS / 2;
 #pragma unroll
   for (int o = top, half = 4; o >= 1; o >>= 1, half >>= 1) {
@@ -1957,27 +1979,27 @@ __device__ __forceinline__ void bk_issue(const GmPtrs& P, const BkPtrs& K, float
   const BkGeom& g = K.g;
   const int slot = s % g.stages;
   const int tile = (rot + s) % T;
-  const int a0 = tile * kBkTile, na = min(kBkTile, na_all - a0);
+  const int a0 = tile * g.tile, na = min(g.tile, na_all - a0);
   const int lane = threadIdx.x & 31;
   const uint32_t bytes = (uint32_t)nvc * sizeof(float2);
   if (lane == 0) mbar_expect_tx(&bars[slot], bytes * (uint32_t)na);
   __syncwarp();
   if (lane < na)
-    bulk_load(ring + ((size_t)slot * kBkTile + lane) * g.rs, P.Vb + (size_t)(a0 + lane) * P.ldv + i0, bytes,
+    bulk_load(ring + ((size_t)slot * g.tile + lane) * g.rs, P.Vb + (size_t)(K.vbase + a0 + lane) * P.ldv + i0, bytes,
               &bars[slot]);
 }
 
 // mode 0: cycle start (W = r_in from P.w, CholQR -> Q_0, R_0); mode 1: step j.
-template <int PP>
+template <int PP, int TILE>
 __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtrs K, int mode) {
-  constexpr int CG = PP / 4, HS = bk_slices(PP);
+  constexpr int CG = PP / 4, HS = bk_slices(PP, TILE);
   extern __shared__ __align__(16) unsigned char bk_raw[];
   const int p = K.p, nr = K.nr, n = P.n;
   const BkGeom& g = K.g;
   const int j = mode == 0 ? -1 : *K.step;  // read before any CTA can pass the second barrier
   const int na_all = (j + 1) * p;          // basis vectors 0 .. na_all - 1 exist
   const BkLayout Lo = bk_layout(p, nr, g, K.nb * p);
-  float2* ring = reinterpret_cast<float2*>(bk_raw + Lo.ring);  // [stages][kBkTile][rs]
+  float2* ring = reinterpret_cast<float2*>(bk_raw + Lo.ring);  // [stages][TILE][rs]
   double2* W = reinterpret_cast<double2*>(bk_raw + Lo.W);      // [PP][lw]
   double2* Hs = reinterpret_cast<double2*>(bk_raw + Lo.Hs);    // [na_all][PP]
   double2* G = reinterpret_cast<double2*>(bk_raw + Lo.G);      // [p][p]: G, then R^{-1}
@@ -1990,10 +2012,16 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
   const int nvc = (nvr + 1) & ~1;           // copied unknowns (the basis rows are zero-padded to even)
   const int par = j & 1;                    // this step's sums (the start uses parity 1)
   const int copy = blockIdx.x % kBkCopies;
-  const int T = (na_all + kBkTile - 1) / kBkTile;  // basis tiles
+  const int T = (na_all + TILE - 1) / TILE;  // basis tiles
+  // update units (unknown, 4-column group): one pass over the basis tiles if
+  // they fit the CTA's threads (slices of the vectors share out the rest),
+  // else one pass per kBkThreads units
+  const int nunits = nr * CG;
+  const int npass = (nunits + kBkThreads - 1) / kBkThreads;
+  const int ST = T * (1 + npass);  // ring stages of the step: dots, then the update passes
   const int rot = T > 0 ? (int)(blockIdx.x % T) : 0;
   int* err = &P.st->err;
-  if (g.hs != HS) {  // host geometry built for another lane layout (uniform over the grid)
+  if (g.hs != HS || g.tile != TILE) {  // host geometry built for another lane layout (uniform over the grid)
     if (tid == 0) atomicExch(err, 1);
     return;
   }
@@ -2006,26 +2034,26 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
     }
     __syncthreads();
     if (wq == 0)
-      for (int s = 0; s < min(g.stages, 2 * T); s++) bk_issue(P, K, ring, bars, s, T, rot, na_all, i0, nvc);
+      for (int s = 0; s < min(g.stages, ST); s++) bk_issue(P, K, ring, bars, s, T, rot, na_all, i0, nvc);
     // the unknowns [nvc, lw) of every ring row stay zero (never written by the copies)
     const int padw = g.lw - nvc;
-    for (int t = tid; t < g.stages * kBkTile * padw; t += kBkThreads) {
+    for (int t = tid; t < g.stages * TILE * padw; t += kBkThreads) {
       const int row = t / padw;
       ring[(size_t)row * g.rs + nvc + (t - row * padw)] = make_float2(0.f, 0.f);
     }
   }
   if (mode == 0) {
-    if (P.f16 && blockIdx.x == 0 && tid < p) P.cinv[tid] = 1.f / kF16VecScale;  // operand scale of Q_0, Q_1, ...
+    if (P.f16 && blockIdx.x == 0 && tid < p) P.cinv[K.col0 + tid] = 1.f / kF16VecScale;  // operand scale of Q_0, Q_1, ...
     for (int t = tid; t < PP * g.lw; t += kBkThreads) {
       const int b = t / g.lw, i = t - b * g.lw;
-      W[t] = (b < p && i < nvr) ? P.w[(size_t)b * n + i0 + i] : make_double2(0.0, 0.0);
+      W[t] = (b < p && i < nvr) ? P.w[(size_t)(K.col0 + b) * n + i0 + i] : make_double2(0.0, 0.0);
     }
   } else {
     for (int t = tid; t < PP * g.lw; t += kBkThreads) {
       const int i = t / PP, b = t - i * PP;
       double2 w = make_double2(0.0, 0.0);
       if (i < nvr && b < p) {
-        float2* y = P.Y + (size_t)(i0 + i) * P.m + b;
+        float2* y = P.Y + (size_t)(i0 + i) * P.m + K.col0 + b;
         const float2 yv = *y;
         w = make_double2(yv.x, yv.y);
         *y = make_float2(0.f, 0.f);
@@ -2056,9 +2084,9 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
     const int d_hs = lane % HS;
     for (int s = 0; s < T; s++) {
       const int slot = s % g.stages;
-      const int a0 = ((rot + s) % T) * kBkTile, na = min(kBkTile, na_all - a0);
+      const int a0 = ((rot + s) % T) * TILE, na = min(TILE, na_all - a0);
       mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
-      const float2* q = ring + ((size_t)slot * kBkTile + d_al) * g.rs + d_hs * g.L;
+      const float2* q = ring + ((size_t)slot * TILE + d_al) * g.rs + d_hs * g.L;
       const double2* w = W + (size_t)(d_cg * 4) * g.lw + d_hs * g.L;
       double v[8];
 #pragma unroll
@@ -2088,7 +2116,7 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
         }
       }
       __syncthreads();  // stage consumed by every warp
-      if (wq == 0 && s + g.stages < 2 * T) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
+      if (wq == 0 && s + g.stages < ST) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
     }
     co_grid_sync(P.st);
 
@@ -2108,65 +2136,72 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
     }
     __syncthreads();
 
-    // ---- W' = W - Q H: thread (unknown, 4 columns, vector slice) ----
-    const int u_as = tid / (nr * CG);
-    const int u_cg = (tid / nr) % CG;
-    const int u_i = tid % nr;
-    const bool u_on = u_as < g.as && u_i < nvr;
-    double2 acc[4];
+    // ---- W' = W - Q H: thread (unknown, 4 columns[, vector slice]) per pass ----
+    const int uas = npass == 1 ? g.as : 1;  // vector slices (one pass only)
+    for (int pass = 0; pass < npass; pass++) {
+      const int unit = npass == 1 ? tid % nunits : pass * kBkThreads + tid;
+      const int u_as = npass == 1 ? tid / nunits : 0;
+      const int u_cg = unit / nr;
+      const int u_i = unit - u_cg * nr;
+      const bool u_on = unit < nunits && u_as < uas && u_i < nvr;
+      double2 acc[4];
 #pragma unroll
-    for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
-    for (int s = T; s < 2 * T; s++) {
-      const int slot = s % g.stages;
-      const int a0 = ((rot + s) % T) * kBkTile, na = min(kBkTile, na_all - a0);
-      mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
-      if (u_on) {
-        const float2* q = ring + (size_t)slot * kBkTile * g.rs + u_i;
-        const double2* h = Hs + (size_t)a0 * PP + u_cg * 4;
-        for (int al = u_as; al < na; al += g.as) {
-          const float2 qf = q[(size_t)al * g.rs];
-          const double qx = qf.x, qy = qf.y;
+      for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
+      for (int s = T * (1 + pass); s < T * (2 + pass); s++) {
+        const int slot = s % g.stages;
+        const int a0 = ((rot + s) % T) * TILE, na = min(TILE, na_all - a0);
+        mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
+        if (u_on) {
+          const float2* q = ring + (size_t)slot * TILE * g.rs + u_i;
+          const double2* h = Hs + (size_t)a0 * PP + u_cg * 4;
+          for (int al = u_as; al < na; al += uas) {
+            const float2 qf = q[(size_t)al * g.rs];
+            const double qx = qf.x, qy = qf.y;
 #pragma unroll
-          for (int c = 0; c < 4; c++) {
-            const double2 hv = h[(size_t)al * PP + c];
-            acc[c].x = fma(qx, hv.x, fma(-qy, hv.y, acc[c].x));
-            acc[c].y = fma(qx, hv.y, fma(qy, hv.x, acc[c].y));
+            for (int c = 0; c < 4; c++) {
+              const double2 hv = h[(size_t)al * PP + c];
+              acc[c].x = fma(qx, hv.x, fma(-qy, hv.y, acc[c].x));
+              acc[c].y = fma(qx, hv.y, fma(qy, hv.x, acc[c].y));
+            }
           }
         }
+        __syncthreads();
+        if (wq == 0 && s + g.stages < ST) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
       }
+      if (pass + 1 == npass && tid == 0)
+        // every issued stage has been waited for (after an error, a wait may
+        // have given up: the last stage issued into each slot is drained
+        // before the ring is reused for the slice sums)
+        for (int sl = 0; sl < min(g.stages, ST); sl++) {
+          const int s_last = sl + ((ST - 1 - sl) / g.stages) * g.stages;
+          mbar_wait_drain(&bars[sl], (uint32_t)(s_last / g.stages) & 1u);
+        }
       __syncthreads();
-      if (wq == 0 && s + g.stages < 2 * T) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
-    }
-    // every issued stage has been waited for (after an error, a wait may have
-    // given up: the last stage issued into each slot is drained before the
-    // ring is reused for the slice sums)
-    if (tid == 0)
-      for (int sl = 0; sl < min(g.stages, 2 * T); sl++) {
-        const int s_last = sl + ((2 * T - 1 - sl) / g.stages) * g.stages;
-        mbar_wait_drain(&bars[sl], (uint32_t)(s_last / g.stages) & 1u);
-      }
-    __syncthreads();
-    double2* part = reinterpret_cast<double2*>(ring);  // [as - 1][CG][nr][4]
-    if (u_on && u_as > 0) {
-      double2* dst = part + (((size_t)(u_as - 1) * CG + u_cg) * nr + u_i) * 4;
+      if (uas > 1) {  // slice sums through the (drained) ring
+        double2* part = reinterpret_cast<double2*>(ring);  // [as - 1][CG][nr][4]
+        if (u_on && u_as > 0) {
+          double2* dst = part + (((size_t)(u_as - 1) * CG + u_cg) * nr + u_i) * 4;
 #pragma unroll
-      for (int c = 0; c < 4; c++) dst[c] = acc[c];
-    }
-    __syncthreads();
-    if (u_on && u_as == 0) {
-      for (int a = 1; a < g.as; a++) {
-        const double2* src = part + (((size_t)(a - 1) * CG + u_cg) * nr + u_i) * 4;
+          for (int c = 0; c < 4; c++) dst[c] = acc[c];
+        }
+        __syncthreads();
+        if (u_on && u_as == 0)
+          for (int a = 1; a < uas; a++) {
+            const double2* src = part + (((size_t)(a - 1) * CG + u_cg) * nr + u_i) * 4;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+              acc[c].x += src[c].x;
+              acc[c].y += src[c].y;
+            }
+          }
+      }
+      if (u_on && u_as == 0) {
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          acc[c].x += src[c].x;
-          acc[c].y += src[c].y;
+          double2* wp = W + (size_t)(u_cg * 4 + c) * g.lw + u_i;
+          wp->x -= acc[c].x;
+          wp->y -= acc[c].y;
         }
-      }
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        double2* wp = W + (size_t)(u_cg * 4 + c) * g.lw + u_i;
-        wp->x -= acc[c].x;
-        wp->y -= acc[c].y;
       }
     }
     __syncthreads();
@@ -2302,8 +2337,8 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
       }
       const float2 f0 = make_float2((float)q0.x, (float)q0.y);
       const float2 f1 = i + 1 < n ? make_float2((float)q1.x, (float)q1.y) : make_float2(0.f, 0.f);
-      *reinterpret_cast<float4*>(P.Vb + (size_t)(qa0 + b) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
-      store_operand(P, i, b, f0, f1);
+      *reinterpret_cast<float4*>(P.Vb + (size_t)(K.vbase + qa0 + b) * P.ldv + i) = make_float4(f0.x, f0.y, f1.x, f1.y);
+      store_operand(P, i, K.col0 + b, f0, f1);
     }
   }
 
@@ -2330,16 +2365,16 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
 // D(:, s) += sum_{a < na} Q_a Y[a][s] for the block solution of the cycle.
 __global__ void gm_block_xupdate_kernel(GmPtrs P, BkPtrs K, int na) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y;
-  if (i >= P.n) return;
-  double2 acc = P.d[(size_t)s * P.n + i];
+  const int s = blockIdx.y;  // column of the group
+  if (i >= P.n || s >= K.p) return;
+  double2 acc = P.d[(size_t)(K.col0 + s) * P.n + i];
   for (int a = 0; a < na; a++) {
-    const float2 v = P.Vb[(size_t)a * P.ldv + i];
+    const float2 v = P.Vb[(size_t)(K.vbase + a) * P.ldv + i];
     const double2 t = cmul(make_double2(v.x, v.y), K.Yb[(size_t)a * K.p + s]);
     acc.x += t.x;
     acc.y += t.y;
   }
-  P.d[(size_t)s * P.n + i] = acc;
+  P.d[(size_t)(K.col0 + s) * P.n + i] = acc;
 }
 
 // Back substitution H y = g on the Givens-reduced Hessenberg matrix, one
@@ -2556,12 +2591,22 @@ Layout layout(int n, int m, int R, int precision) {
   L.hacc = take(sizeof(double) * 2 * (size_t)m * 4 * (R + 1));
   L.nacc = take(sizeof(double) * 2 * (size_t)m * 3);
   // block solver state (used when 2 <= m <= kBkMaxP)
-  const bool bk = m >= 2 && m <= kBkMaxP;
-  const int nb = bk_steps(m, R);
-  L.bk_hacc = take(bk ? sizeof(double) * 2 * kBkCopies * (size_t)(nb + 1) * m * m * 2 : 0);
-  L.bk_gacc = take(bk ? sizeof(double) * 2 * kBkCopies * (size_t)m * m * 2 : 0);
-  L.bk_y = take(bk ? sizeof(double2) * (size_t)nb * m * m : 0);
-  L.bk_step = take(bk ? sizeof(int) : 0);
+  const bool bk = m >= 2 && m <= kBkMaxRhs;
+  size_t sh = 0, sg = 0, sy = 0;
+  if (bk) {
+    int gsz[kBkMaxGroups], gc0[kBkMaxGroups];
+    const int G = bk_groups(m, gsz, gc0);
+    const int nb = bk_steps(gsz[0], R);  // the largest group; a cycle never runs longer
+    for (int g = 0; g < G; g++) {
+      sh += 2 * kBkCopies * (size_t)(nb + 1) * gsz[g] * gsz[g] * 2;
+      sg += 2 * kBkCopies * (size_t)gsz[g] * gsz[g] * 2;
+      sy += (size_t)nb * gsz[g] * gsz[g];
+    }
+  }
+  L.bk_hacc = take(sizeof(double) * sh);
+  L.bk_gacc = take(sizeof(double) * sg);
+  L.bk_y = take(sizeof(double2) * sy);
+  L.bk_step = take(bk ? sizeof(int) * kBkMaxGroups : 0);
   L.tc = take(precision == BEM_PREC_FP32 ? 0 : tc_workspace_bytes(n, m, precision));
   L.total = o;
   return L;
@@ -2634,9 +2679,10 @@ struct BlockHost {
     if (S) cudaFreeHost(S);
   }
 };
-thread_local BlockHost t_block;
+thread_local BlockHost t_blocks[kBkMaxGroups];
 
-int block_host(int p, int nb, BlockHost** out) {
+int block_host(int group, int p, int nb, BlockHost** out) {
+  BlockHost& t_block = t_blocks[group];
   const size_t need = (size_t)nb * (nb + 1) * p * p;
   if (t_block.cap < need) {
     if (t_block.H) cudaFreeHost(t_block.H);
@@ -2902,77 +2948,109 @@ int coop_shape(int n, int m, int R, CoShape* out) {
 }
 
 // Launch shape of gm_block_kernel: nr unknowns per CTA (even), one CTA per
-// SM at most, all resident (cooperative launch); the most ring stages (4 .. 2)
-// that fit the shared memory.
+// SM at most, all resident (cooperative launch).  Preference, first fit in
+// shared memory: the full cycle length, 32-vector ring stages, more stages;
+// with many unknowns per CTA the stages shrink to 16 vectors and then the
+// cycle shortens.  One geometry per group (the groups differ in p by <= 1).
 struct BkShape {
-  int nr = 0, grid = 0;
-  BkGeom g{};
-  size_t smem = 0;
+  int nr = 0, grid = 0, nb = 0, groups = 0;
+  int p[kBkMaxGroups] = {}, col0[kBkMaxGroups] = {}, vbase[kBkMaxGroups] = {};
+  BkGeom g[kBkMaxGroups] = {};
+  size_t smem[kBkMaxGroups] = {};
 };
 
-template <int PP>
-int block_attr(int smem_optin) {
-  static std::atomic<bool> attr{false};
-  if (!attr.load(std::memory_order_acquire)) {
-    BEM_CUDA_TRY(cudaFuncSetAttribute(gm_block_kernel<PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin - 1024));
-    attr.store(true, std::memory_order_release);
+template <typename F>
+int block_dispatch(int pp, int tile, F&& f) {
+  if (tile == 32) {
+    if (pp == 4) return f(gm_block_kernel<4, 32>);
+    if (pp == 8) return f(gm_block_kernel<8, 32>);
+    return f(gm_block_kernel<16, 32>);
   }
-  return BEM_OK;
+  if (pp == 4) return f(gm_block_kernel<4, 16>);
+  if (pp == 8) return f(gm_block_kernel<8, 16>);
+  return f(gm_block_kernel<16, 16>);
 }
 
-int block_shape(int n, int p, int R, BkShape* out) {
+int block_shape(int n, int m, int R, BkShape* out) {
+  static std::mutex mu;
+  static bool attr_set[2][3] = {};
   int dev = 0, coop_ok = 0, smem_optin = 0;
   BEM_CUDA_TRY(cudaGetDevice(&dev));
   BEM_CUDA_TRY(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
   BEM_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (!coop_ok) return BEM_ERR_UNSUPPORTED;
+  if (!coop_ok || m < 2 || m > kBkMaxRhs) return BEM_ERR_UNSUPPORTED;
   const int sms = sm_count_linalg();
   int nr = (n + sms - 1) / sms;
   nr = std::max(16, (nr + 1) & ~1);
-  if (nr > 256) return BEM_ERR_UNSUPPORTED;
+  if (nr > 320) return BEM_ERR_UNSUPPORTED;
   const int grid = (n + nr - 1) / nr;
-  BkGeom g = bk_geom(p, nr);
-  const int na_max = bk_steps(p, R) * p;
-  size_t smem = 0;
-  for (g.stages = kBkMaxStages; g.stages >= 2; g.stages--) {
-    smem = bk_layout(p, nr, g, na_max).total;
-    if (smem + 1024 <= (size_t)smem_optin) break;
+  BkShape sh;
+  sh.groups = bk_groups(m, sh.p, sh.col0);
+  const int nb_full = bk_steps(sh.p[0], R);
+  bool fit = false;
+  for (int nb = nb_full; nb >= 4 && !fit; nb--) {
+    for (int tile = kBkTileMax; tile >= 16 && !fit; tile /= 2) {
+      for (int stages = kBkMaxStages; stages >= 2 && !fit; stages--) {
+        bool ok = true;
+        for (int g = 0; g < sh.groups && ok; g++) {
+          sh.g[g] = bk_geom(sh.p[g], nr, tile);
+          sh.g[g].stages = stages;
+          sh.smem[g] = bk_layout(sh.p[g], nr, sh.g[g], nb * sh.p[g]).total;
+          ok = sh.smem[g] + 1024 <= (size_t)smem_optin;
+        }
+        if (ok) {
+          fit = true;
+          sh.nb = nb;
+        }
+      }
+    }
   }
-  if (g.stages < 2) return BEM_ERR_UNSUPPORTED;
-  int rc = g.pp == 4 ? block_attr<4>(smem_optin) : g.pp == 8 ? block_attr<8>(smem_optin) : block_attr<16>(smem_optin);
-  if (rc) return rc;
-  int occ = 0;
-  if (g.pp == 4)
-    BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel<4>, kBkThreads, smem));
-  else if (g.pp == 8)
-    BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel<8>, kBkThreads, smem));
-  else
-    BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gm_block_kernel<16>, kBkThreads, smem));
-  if (occ < 1 || grid > occ * sms) return BEM_ERR_UNSUPPORTED;
-  out->nr = nr;
-  out->grid = grid;
-  out->g = g;
-  out->smem = smem;
+  if (!fit) return BEM_ERR_UNSUPPORTED;
+  for (int g = 0, row = 0; g < sh.groups; g++) {
+    sh.vbase[g] = row;
+    row += (sh.nb + 1) * sh.p[g];
+    const int pi = sh.g[g].pp == 4 ? 0 : sh.g[g].pp == 8 ? 1 : 2, ti = sh.g[g].tile == 32 ? 0 : 1;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!attr_set[ti][pi]) {
+        int rc = block_dispatch(sh.g[g].pp, sh.g[g].tile, [&](auto kern) -> int {
+          BEM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin - 1024));
+          return BEM_OK;
+        });
+        if (rc) return rc;
+        attr_set[ti][pi] = true;
+      }
+    }
+    int occ = 0;
+    int rc = block_dispatch(sh.g[g].pp, sh.g[g].tile, [&](auto kern) -> int {
+      BEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBkThreads, sh.smem[g]));
+      return BEM_OK;
+    });
+    if (rc) return rc;
+    if (occ < 1 || grid > occ * sms) return BEM_ERR_UNSUPPORTED;
+  }
+  sh.nr = nr;
+  sh.grid = grid;
+  *out = sh;
   return BEM_OK;
 }
 
-int launch_block(const GmPtrs& P, const BkPtrs& K, const BkShape& sh, int mode, cudaStream_t st) {
+int launch_block(const GmPtrs& P, const BkPtrs& K, const BkShape& sh, int group, int mode, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)sh.grid, 1, 1);
   cfg.blockDim = dim3(kBkThreads, 1, 1);
-  cfg.dynamicSmemBytes = sh.smem;
+  cfg.dynamicSmemBytes = sh.smem[group];
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeCooperative;
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  if (sh.g.pp == 4)
-    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel<4>, P, K, mode));
-  else if (sh.g.pp == 8)
-    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel<8>, P, K, mode));
-  else
-    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, gm_block_kernel<16>, P, K, mode));
+  int rc = block_dispatch(sh.g[group].pp, sh.g[group].tile, [&](auto kern) -> int {
+    BEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, P, K, mode));
+    return BEM_OK;
+  });
+  if (rc) return rc;
   count_launch();
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
@@ -3049,26 +3127,36 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
   double* rnorm2 = (double*)(w + L.rnorm2);
   void* tcws = w + L.tc;
   const int prec = params->precision;
-  // one block Krylov space for all right-hand sides (see gm_block_kernel)
-  BkPtrs K = {};
+  // block Krylov spaces (see gm_block_kernel): one for 2..16 right-hand
+  // sides, groups of <= 16 columns for up to 64, one shared matvec per step
+  BkPtrs K[kBkMaxGroups] = {};
   BkShape bshape;
-  BlockHost* bh = nullptr;
-  bool block = g_gmres_block == 0 && m >= 2 && m <= kBkMaxP && block_shape(n, m, R, &bshape) == BEM_OK;
-  const int nbk = bk_steps(m, R);
-  if (block) {
-    int rcb = block_host(m, nbk, &bh);
-    if (rcb) return rcb;
-    K.p = m;
-    K.nb = nbk;
-    K.nr = bshape.nr;
-    K.g = bshape.g;
-    K.hacc = (double*)(w + L.bk_hacc);
-    K.gacc = (double*)(w + L.bk_gacc);
-    K.Yb = (double2*)(w + L.bk_y);
-    K.step = (int*)(w + L.bk_step);
-    K.hostH = bh->dH;
-    K.hostR0 = bh->dR0;
-    K.hostS = bh->dS;
+  BlockHost* bh[kBkMaxGroups] = {};
+  bool block = g_gmres_block == 0 && m >= 2 && m <= kBkMaxRhs && block_shape(n, m, R, &bshape) == BEM_OK;
+  const int nbk = bshape.nb, ngr = block ? bshape.groups : 0;
+  {
+    size_t oh = 0, og = 0, oy = 0;
+    for (int g = 0; g < ngr; g++) {
+      const int pg = bshape.p[g];
+      int rcb = block_host(g, pg, nbk, &bh[g]);
+      if (rcb) return rcb;
+      K[g].p = pg;
+      K[g].col0 = bshape.col0[g];
+      K[g].vbase = bshape.vbase[g];
+      K[g].nb = nbk;
+      K[g].nr = bshape.nr;
+      K[g].g = bshape.g[g];
+      K[g].hacc = (double*)(w + L.bk_hacc) + oh;
+      K[g].gacc = (double*)(w + L.bk_gacc) + og;
+      K[g].Yb = (double2*)(w + L.bk_y) + oy;
+      K[g].step = (int*)(w + L.bk_step) + g;
+      K[g].hostH = bh[g]->dH;
+      K[g].hostR0 = bh[g]->dR0;
+      K[g].hostS = bh[g]->dS;
+      oh += 2 * kBkCopies * (size_t)(nbk + 1) * pg * pg * 2;
+      og += 2 * kBkCopies * (size_t)pg * pg * 2;
+      oy += (size_t)nbk * pg * pg;
+    }
   }
   if (prec != BEM_PREC_FP32) {
     int rc = tc_operator_prepare((const float2*)A, n, prec, tcws, s);
@@ -3201,13 +3289,15 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     int r2 = prec == BEM_PREC_FP32 ? launch_cgemv((const float2*)A, n, P.X, m, P.Y, nullptr, st, &P.st->err)
                                    : tc_gemm(tcws, n, prec, m, P.Y, nullptr, st);
     if (r2) return r2;
-    return launch_block(P, K, bshape, 1, st);
+    for (int g = 0; g < ngr; g++)
+      if ((r2 = launch_block(P, K[g], bshape, g, 1, st))) return r2;
+    return BEM_OK;
   };
   ExecGuard block_guard;
   cudaGraphExec_t& block_exec = block_guard.e;
   unsigned long long block_kernels = 0;
   bool block_direct_done = false;
-  BlockLS ls;
+  BlockLS ls[kBkMaxGroups];
   std::vector<double> bres(m), btol(m);
   std::vector<double2> bY;
   constexpr int kBkLookahead = 1;  // one step queued behind the one the host examines
@@ -3287,37 +3377,54 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       (gm_start_scalar_kernel<<<1, ((m + 31) / 32) * 32, 0, s>>>(P, rnorm2, inner_rtol, 0.5 * params->rtol), count_launch());
       BEM_CUDA_TRY(cudaMemsetAsync(P.Y, 0, sizeof(float2) * (size_t)n * m, s));
       if (block) {
-        // ---- one block Krylov space: start block Q_0 R_0 = r_in (CholQR) ----
+        // ---- block Krylov spaces: start blocks Q_0 R_0 = r_in (CholQR), one per group ----
         first_cycle = false;
-        BEM_CUDA_TRY(cudaMemsetAsync(K.hacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)(nbk + 1) * m * m * 2, s));
-        BEM_CUDA_TRY(cudaMemsetAsync(K.gacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)m * m * 2, s));
-        for (int q = 0; q <= nbk; q++) bh->S[q] = 0;  // no step of this solve is in flight here
-        if ((rc = launch_block(P, K, bshape, 0, s))) return rc;
+        for (int g = 0; g < ngr; g++) {
+          const int pg = bshape.p[g];
+          BEM_CUDA_TRY(cudaMemsetAsync(K[g].hacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)(nbk + 1) * pg * pg * 2, s));
+          BEM_CUDA_TRY(cudaMemsetAsync(K[g].gacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)pg * pg * 2, s));
+          for (int q = 0; q <= nbk; q++) bh[g]->S[q] = 0;  // no step of this solve is in flight here
+          if ((rc = launch_block(P, K[g], bshape, g, 0, s))) return rc;
+        }
         BEM_CUDA_TRY(cudaMemcpyAsync(btol.data(), P.tol, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
         BEM_CUDA_TRY(cudaStreamSynchronize(s));
-        if (reinterpret_cast<volatile int*>(bh->S)[nbk] != 1) {
-          // the residual block has lost rank (e.g. equal or zero columns):
+        bool start_ok = true;
+        for (int g = 0; g < ngr; g++) start_ok &= reinterpret_cast<volatile int*>(bh[g]->S)[nbk] == 1;
+        if (!start_ok) {
+          // a residual block has lost rank (e.g. equal or zero columns):
           // separate Krylov spaces for the rest of this solve
           block = false;
         } else {
-          ls.init(m, nbk, bh->R0);
-          int kk = 0, launched_c = 0, checked_c = 0;
-          bool conv = false, stop = false;
+          int kk[kBkMaxGroups] = {};
+          bool gstop[kBkMaxGroups] = {}, gconv[kBkMaxGroups] = {};
+          for (int g = 0; g < ngr; g++) ls[g].init(bshape.p[g], nbk, bh[g]->R0);
+          int launched_c = 0, checked_c = 0;
+          bool stop = false;
           const long long bbase = launched;
+          // step jj of every group: a group stops at a breakdown (keeping the
+          // steps before it) or when all its columns meet their tolerance
           auto process = [&](int jj) -> int {
             BEM_CUDA_TRY(cudaEventSynchronize(ring->ev[(bbase + jj) % kSnapRing]));
             if (stop) return BEM_OK;
-            if (reinterpret_cast<volatile int*>(bh->S)[jj] != 1 ||
-                !ls.add(jj, bh->H + (size_t)jj * (nbk + 1) * m * m, bres.data())) {
-              stop = true;  // breakdown: keep the steps before this one
-              return BEM_OK;
+            bool all_stopped = true, accepted = false;
+            for (int g = 0; g < ngr; g++) {
+              if (gstop[g]) continue;
+              const int pg = bshape.p[g], c0 = bshape.col0[g];
+              if (reinterpret_cast<volatile int*>(bh[g]->S)[jj] != 1 ||
+                  !ls[g].add(jj, bh[g]->H + (size_t)jj * (nbk + 1) * pg * pg, bres.data() + c0)) {
+                gstop[g] = true;
+                continue;
+              }
+              accepted = true;
+              kk[g] = jj + 1;
+              bool all = true;
+              for (int c = c0; c < c0 + pg; c++)
+                if (!(bres[c] <= btol[c])) all = false;
+              if (all) gconv[g] = gstop[g] = true;
+              all_stopped &= gstop[g];
             }
-            iters_done++;
-            kk = jj + 1;
-            bool all = true;
-            for (int c = 0; c < m; c++)
-              if (!(bres[c] <= btol[c])) all = false;
-            if (all) conv = stop = true;
+            if (accepted) iters_done++;
+            if (all_stopped) stop = true;
             return BEM_OK;
           };
           while (launched_c < nbk && total_iters < params->max_iters && !stop) {
@@ -3340,13 +3447,20 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
           }
           while (checked_c < launched_c)  // every launched step has finished after this
             if ((rc = process(checked_c++))) return rc;
-          if (kk > 0) {
-            ls.solve(kk, bY);
-            BEM_CUDA_TRY(cudaMemcpyAsync(K.Yb, bY.data(), sizeof(double2) * bY.size(), cudaMemcpyHostToDevice, s));
-            (gm_block_xupdate_kernel<<<gv, 256, 0, s>>>(P, K, kk * m), count_launch());
+          bool conv = true, none = true;
+          for (int g = 0; g < ngr; g++) {
+            conv &= gconv[g];
+            if (kk[g] == 0) continue;
+            none = false;
+            ls[g].solve(kk[g], bY);
+            BEM_CUDA_TRY(cudaMemcpyAsync(K[g].Yb, bY.data(), sizeof(double2) * bY.size(), cudaMemcpyHostToDevice, s));
+            // bY is reused by the next group: the copy must have read it
+            BEM_CUDA_TRY(cudaStreamSynchronize(s));
+            (gm_block_xupdate_kernel<<<dim3(gv.x, bshape.p[g]), 256, 0, s>>>(P, K[g], kk[g] * bshape.p[g]),
+             count_launch());
           }
           if (conv) break;
-          if (kk == 0 && stop) {  // broke down at its first step: separate Krylov spaces instead
+          if (none) {  // broke down at the first step: separate Krylov spaces instead
             block = false;
           }
           continue;

@@ -79,3 +79,28 @@ def test_monopole_known_answer_at_s6(large):
     exact = np.exp(1j * k * rp) / (4 * np.pi * rp)
     assert np.linalg.norm(p - exact) / np.linalg.norm(exact) <= 3e-2
     del V, A
+
+
+def test_grouped_block_gmres_at_s6(large):
+    """40 right-hand sides at N = 40 962: three block spaces of 14, 13 and 13
+    columns, 278 unknowns per CTA (16-vector ring stages, the W - Q H update
+    in three passes over the basis).  Same solution as one Krylov space per
+    column (residuals <= 1e-6 against the FP32 matrix, so the two agree to
+    cond(A) x 2e-6)."""
+    from neuralat_b200 import _lib as L
+    w, s, k, V, A = large
+    g = M.smoothed_gaussian_field(A.shape[0], s.triangles.cpu().numpy(), 40, seed=40).astype(np.complex64)
+    rhs = -cmatmul(V, torch.from_numpy(g).cuda())
+    info = {}
+    u = gmres(A, rhs, rtol=1e-6, precision="fp16x3", info=info)
+    assert info["status"] == 0 and info["rel_residual"] <= 1e-6, info
+    lib = L.lib()
+    try:
+        L.check(lib.bem_set_tuning(L.TUNE_GMRES_BLOCK, 1))
+        info1 = {}
+        u1 = gmres(A, rhs, rtol=1e-6, precision="fp16x3", info=info1)
+    finally:
+        L.check(lib.bem_set_tuning(L.TUNE_GMRES_BLOCK, 0))
+    assert info1["status"] == 0
+    err = float(torch.linalg.norm(u - u1) / torch.linalg.norm(u1))
+    assert err <= 1e-4, err
