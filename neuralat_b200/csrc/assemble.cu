@@ -214,31 +214,58 @@ __device__ __forceinline__ void regular_item(RegSmem<DO_V, DO_K>& sm, const Geom
       __syncthreads();
 
       // ---- reduce corner slots onto distinct vertices, one atomic per entry ----
+      // Pass 1, in place: for every trial corner column, the row of test
+      // vertex A's first corner gets the sum over A's test corners (corner
+      // rows of different vertices are disjoint); pass 2: entry (A, B) sums
+      // B's trial corners along that row.
       const int nI0 = sm.tileI[0].nlv;
       const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
       const int nJ = sm.tileJ.nlv;
-      const int total = (nI0 + nI1) * nJ;
-      for (int e = tid; e < total; e += kRegThreads) {
+      const int ncol = 3 * ntriJ;
+      for (int e = tid; e < (nI0 + nI1) * ncol; e += kRegThreads) {
+        const int ai = e / ncol;
+        const int col = e - ai * ncol;
+        const int s = ai >= nI0;
+        const int a = ai - s * nI0;
+        const TileRec& TI = sm.tileI[s];
+        const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
+        const int rep = s * kTileCorners + TI.lv_corner[ca0];
+        float2 v = make_float2(0.f, 0.f), kk = make_float2(0.f, 0.f);
+        if (DO_V) v = sm.slotV[rep][col];
+        if (DO_K) kk = sm.slotK[rep][col];
+        for (int ca = ca0 + 1; ca < ca1; ca++) {
+          const int row = s * kTileCorners + TI.lv_corner[ca];
+          if (DO_V) {
+            v.x += sm.slotV[row][col].x;
+            v.y += sm.slotV[row][col].y;
+          }
+          if (DO_K) {
+            kk.x += sm.slotK[row][col].x;
+            kk.y += sm.slotK[row][col].y;
+          }
+        }
+        if (DO_V) sm.slotV[rep][col] = v;
+        if (DO_K) sm.slotK[rep][col] = kk;
+      }
+      __syncthreads();
+      for (int e = tid; e < (nI0 + nI1) * nJ; e += kRegThreads) {
         const int ai = e / nJ;
         const int b = e - ai * nJ;
         const int s = ai >= nI0;
         const int a = ai - s * nI0;
         const TileRec& TI = sm.tileI[s];
+        const int rep = s * kTileCorners + TI.lv_corner[TI.lv_ptr[a]];
         float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f);
-        const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
         const int cb0 = sm.tileJ.lv_ptr[b], cb1 = sm.tileJ.lv_ptr[b + 1];
-        for (int ca = ca0; ca < ca1; ca++) {
-          const int row = s * kTileCorners + TI.lv_corner[ca];
-          for (int cb = cb0; cb < cb1; cb++) {
-            const int col = sm.tileJ.lv_corner[cb];
-            if (DO_V) {
-              acc_v.x += sm.slotV[row][col].x;
-              acc_v.y += sm.slotV[row][col].y;
-            }
-            if (DO_K) {
-              acc_k.x += sm.slotK[row][col].x;
-              acc_k.y += sm.slotK[row][col].y;
-            }
+        for (int cb = cb0; cb < cb1; cb++) {
+          const int col = sm.tileJ.lv_corner[cb];
+          if (DO_V) {
+            acc_v.x += sm.slotV[rep][col].x;
+            acc_v.y += sm.slotV[rep][col].y;
+          }
+          if (DO_K) {
+            acc_k.x += sm.slotK[rep][col].x;
+            acc_k.y += sm.slotK[rep][col].y;
           }
         }
         const size_t idx = (size_t)TI.vid[a] * nv + sm.tileJ.vid[b];
