@@ -199,8 +199,9 @@ enum {
                                         unissued, so the consumer's wait expires, the kernel drains its
                                         copies and returns, and bem_tc_status reports BEM_ERR_CUDA
                                         (no fault, no hang); 0 = off */
-  BEM_TUNE_GMRES_BLOCK = 9           /* bem_gmres_solve with 2..16 right-hand sides: 0 one block Krylov space
-                                        for all of them (block GMRES, the default), 1 one space per column */
+  BEM_TUNE_GMRES_BLOCK = 9           /* bem_gmres_solve with 2..64 right-hand sides: 0 block GMRES (the
+                                        default; one block Krylov space per group of <= 16 columns, the
+                                        groups sharing each matvec), 1 one space per column */
 };
 int bem_set_tuning(int key, int value);
 int bem_get_tuning(int key);
@@ -322,9 +323,12 @@ int bem_tc_status(const void* workspace, bem_stream_t stream);
 /* Workspace bytes for bem_gmres_solve (n unknowns, m right-hand sides). */
 size_t bem_gmres_workspace_bytes(int n, int m, const bem_solver_params* params);
 
-/* Solve A X = B for m right-hand sides with restarted GMRES (device-resident
- * Arnoldi, FP64 classical Gram-Schmidt with re-orthogonalisation and Givens
- * rotations) wrapped in FP64 iterative refinement against the FP32 matrix.
+/* Solve A X = B for m right-hand sides with restarted GMRES wrapped in FP64
+ * iterative refinement against the FP32 matrix.  2..64 right-hand sides: block
+ * GMRES (block Krylov spaces of <= 16 columns, FP64 block Gram-Schmidt and
+ * CholQR on the device, the small least-squares problems on the host);
+ * otherwise one Krylov space per column (device-resident Arnoldi, FP64
+ * classical Gram-Schmidt, Givens rotations).
  * A: n x n complex64 row-major.  B: (n, m) complex64.  X: (n, m) complex64,
  * used as the initial guess when `use_x0` != 0 and overwritten with the
  * solution.  `info` is a HOST pointer.  Synchronises `stream` once per
