@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <future>
 #include <mutex>
 #include <vector>
 
@@ -1847,12 +1848,25 @@ constexpr int kBkMaxGroups = 4;                    // 17 .. 64 right-hand sides:
 constexpr int kBkMaxRhs = kBkMaxP * kBkMaxGroups;  // each its own block space, one shared matvec per step
 constexpr int kBkVectors = 384;  // basis vectors per cycle: kBkVectors / m block steps (at most the restart length)
 constexpr int kBkCopies = 4;     // copies of the H and Gram sums (CTA c adds into copy c % kBkCopies)
+constexpr int kBkHostRing = 4;   // host-mapped H column blocks in flight (the host is at most 2 steps behind)
+constexpr int kBkStreamVectors = 1600;  // basis vectors per group and cycle with streamed H
 constexpr int kBkMaxStages = 4;
 
 // Block steps per cycle for blocks of p columns and restart length R.
 __host__ __device__ inline int bk_steps(int p, int R) {
   const int nb = kBkVectors / p;
   return nb < R ? nb : R;
+}
+
+// Device sums and least-squares solution of group g (doubles / double2),
+// sized for both step modes: staged H (kBkCopies copies, kBkVectors per
+// cycle) and streamed H (one copy, kBkStreamVectors per cycle).
+inline void bk_group_sizes(int p, int R, size_t* nh, size_t* ng, size_t* ny) {
+  const int nb_staged = std::min(kBkVectors / p, R), nb_stream = std::min(kBkStreamVectors / p, R);
+  const size_t hs = std::max((size_t)kBkCopies * (nb_staged + 1), (size_t)(nb_stream + 1));
+  *nh = 2 * hs * p * p * 2;
+  *ng = 2 * (size_t)kBkCopies * p * p * 2;
+  *ny = (size_t)std::max(nb_staged, nb_stream) * p * p;
 }
 
 // Groups of m right-hand sides (2 <= m <= kBkMaxRhs): ceil(m / 16) groups,
@@ -1870,6 +1884,7 @@ inline int bk_groups(int m, int* size, int* col0) {
 
 // Shape of the per-CTA work (host-computed, see bk_geom).
 struct BkGeom {
+  int hstream; // H streamed per tile (double-buffered [2][tile][pp]) instead of staged whole
   int tile;    // basis vectors per ring stage (16 or 32)
   int pp;      // padded block size: 4, 8 or 16
   int hs;      // unknown slices of the dots (16 / (pp / 4))
@@ -1886,21 +1901,23 @@ struct BkPtrs {
   int vbase;       // first basis row of the group in P.Vb
   int nb;          // block steps per cycle
   int nr;          // unknowns per CTA (even)
+  int ncopy;       // copies of the H and Gram sums (kBkCopies; 1 with streamed H)
+  int hstream;     // 1: H read per tile from the (single) sums, 0: the step's H staged whole in shared memory
   BkGeom g;
-  double* hacc;    // [2][kBkCopies][(nb + 1) p][p][re, im]: H column block of the step, by step parity
-  double* gacc;    // [2][kBkCopies][p][p][re, im]: Gram matrix of the step (parity 1 also serves the cycle start)
+  double* hacc;    // [2][ncopy][(nb + 1) p][p][re, im]: H column block of the step, by step parity
+  double* gacc;    // [2][ncopy][p][p][re, im]: Gram matrix of the step (parity 1 also serves the cycle start)
   double2* Yb;     // [nb p][p]: least-squares solution uploaded by the host
   int* step;       // block step j of the cycle (device)
-  double2* hostH;  // host-mapped [nb][(nb + 1) p][p]: H column block j incl. R_{j+1}
+  double2* hostH;  // host-mapped [kBkHostRing][(nb + 1) p][p]: H column block j (slot j % ring) incl. R_{j+1}
   double2* hostR0; // host-mapped [p][p]: R_0 of the cycle's start block
   int* hostS;      // host-mapped [nb + 1]: 1 step done, 2 breakdown (index nb: the start)
 };
 
 __device__ __forceinline__ double* bk_hacc(const BkPtrs& K, int par, int copy) {
-  return K.hacc + ((size_t)par * kBkCopies + copy) * (K.nb + 1) * K.p * K.p * 2;
+  return K.hacc + ((size_t)par * K.ncopy + copy) * (K.nb + 1) * K.p * K.p * 2;
 }
 __device__ __forceinline__ double* bk_gacc(const BkPtrs& K, int par, int copy) {
-  return K.gacc + ((size_t)par * kBkCopies + copy) * K.p * K.p * 2;
+  return K.gacc + ((size_t)par * K.ncopy + copy) * K.p * K.p * 2;
 }
 
 // Unknown slices of the dots for padded block size pp (the host geometry and
@@ -1910,6 +1927,7 @@ __host__ __device__ constexpr int bk_slices(int pp, int tile) { return kBkThread
 __host__ __device__ inline BkGeom bk_geom(int p, int nr, int tile) {
   BkGeom g;
   g.tile = tile;
+  g.hstream = 0;
   g.pp = p <= 4 ? 4 : (p <= 8 ? 8 : 16);
   const int cg = g.pp / 4;
   g.hs = bk_slices(g.pp, tile);
@@ -1942,7 +1960,7 @@ __host__ __device__ inline BkLayout bk_layout(int p, int nr, const BkGeom& g, in
   const size_t part = sizeof(double2) * (size_t)(g.as - 1) * g.pp * nr;  // update slices, after the ring is drained
   L.ring = take(ring > part ? ring : part);
   L.W = take(sizeof(double2) * (size_t)g.pp * g.lw);
-  L.Hs = take(sizeof(double2) * (size_t)na_max * g.pp);
+  L.Hs = take(sizeof(double2) * (size_t)(g.hstream ? 2 * g.tile : na_max) * g.pp);
   L.G = take(sizeof(double2) * 2 * (size_t)p * p + sizeof(double) * p);  // G / R^{-1}, R, 1 / R_cc
   L.bars = take(sizeof(uint64_t) * kBkMaxStages);
   L.total = o;
@@ -2001,7 +2019,7 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
   const BkLayout Lo = bk_layout(p, nr, g, K.nb * p);
   float2* ring = reinterpret_cast<float2*>(bk_raw + Lo.ring);  // [stages][TILE][rs]
   double2* W = reinterpret_cast<double2*>(bk_raw + Lo.W);      // [PP][lw]
-  double2* Hs = reinterpret_cast<double2*>(bk_raw + Lo.Hs);    // [na_all][PP]
+  double2* Hs = reinterpret_cast<double2*>(bk_raw + Lo.Hs);    // [na_all][PP], or [2][TILE][PP] with streamed H
   double2* G = reinterpret_cast<double2*>(bk_raw + Lo.G);      // [p][p]: G, then R^{-1}
   double2* Rm = G + p * p;                                      // [p][p]: R
   double* rinv = reinterpret_cast<double*>(Rm + p * p);         // [p]: 1 / R_cc
@@ -2011,7 +2029,7 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
   const int nvr = max(0, min(nr, n - i0));  // valid unknowns of this CTA
   const int nvc = (nvr + 1) & ~1;           // copied unknowns (the basis rows are zero-padded to even)
   const int par = j & 1;                    // this step's sums (the start uses parity 1)
-  const int copy = blockIdx.x % kBkCopies;
+  const int copy = blockIdx.x % K.ncopy;
   const int T = (na_all + TILE - 1) / TILE;  // basis tiles
   // update units (unknown, 4-column group): one pass over the basis tiles if
   // they fit the CTA's threads (slices of the vectors share out the rest),
@@ -2064,7 +2082,7 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
   {
     const int np = par ^ 1;
     const size_t nh = (size_t)(K.nb + 1) * p * p * 2, ng = (size_t)p * p * 2;
-    for (size_t t = (size_t)blockIdx.x * kBkThreads + tid; t < kBkCopies * (nh + ng);
+    for (size_t t = (size_t)blockIdx.x * kBkThreads + tid; t < (size_t)K.ncopy * (nh + ng);
          t += (size_t)gridDim.x * kBkThreads) {
       const int c = (int)(t / (nh + ng));
       const size_t u = t - (size_t)c * (nh + ng);
@@ -2120,13 +2138,13 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
     }
     co_grid_sync(P.st);
 
-    // ---- stage H (sum of the copies) ----
-    for (int t = tid; t < na_all * PP; t += kBkThreads) {
+    // ---- stage H (sum of the copies), unless it is streamed per tile ----
+    for (int t = tid; t < (g.hstream ? 0 : na_all * PP); t += kBkThreads) {
       const int a = t / PP, b = t - a * PP;
       double2 h = make_double2(0.0, 0.0);
       if (b < p) {
 #pragma unroll
-        for (int c = 0; c < kBkCopies; c++) {
+        for (int c = 0; c < K.ncopy; c++) {
           const double* hp = bk_hacc(K, par, c) + ((size_t)a * p + b) * 2;
           h.x += __ldcg(hp);
           h.y += __ldcg(hp + 1);
@@ -2147,13 +2165,28 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
       double2 acc[4];
 #pragma unroll
       for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
+      // streamed H: thread t < TILE * PP carries entry (t / PP, t % PP) of
+      // the next tile's rows in a register, stored after the current tile
+      const double2* Hg = reinterpret_cast<const double2*>(bk_hacc(K, par, 0));  // one copy when streamed
+      auto h_fetch = [&](int s2) -> double2 {
+        const int t = tid;
+        if (!g.hstream || t >= TILE * PP || s2 >= T * (2 + pass)) return make_double2(0.0, 0.0);
+        const int a = ((rot + s2) % T) * TILE + t / PP, b = t % PP;
+        return (a < na_all && b < p) ? __ldcg(Hg + (size_t)a * p + b) : make_double2(0.0, 0.0);
+      };
+      double2 hnext = h_fetch(T * (1 + pass));
       for (int s = T * (1 + pass); s < T * (2 + pass); s++) {
         const int slot = s % g.stages;
         const int a0 = ((rot + s) % T) * TILE, na = min(TILE, na_all - a0);
+        if (g.hstream) {  // this tile's H rows into buffer s & 1 (its previous readers passed the last barrier)
+          if (tid < TILE * PP) Hs[(size_t)(s & 1) * TILE * PP + tid] = hnext;
+          hnext = h_fetch(s + 1);
+          __syncthreads();
+        }
         mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
         if (u_on) {
           const float2* q = ring + (size_t)slot * TILE * g.rs + u_i;
-          const double2* h = Hs + (size_t)a0 * PP + u_cg * 4;
+          const double2* h = g.hstream ? Hs + (size_t)(s & 1) * TILE * PP + u_cg * 4 : Hs + (size_t)a0 * PP + u_cg * 4;
           for (int al = u_as; al < na; al += uas) {
             const float2 qf = q[(size_t)al * g.rs];
             const double qx = qf.x, qy = qf.y;
@@ -2253,7 +2286,7 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
       const int v = b2 >= b1 ? u : b2 * p + b1;  // lower triangle from the upper one
       double2 gv = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int c = 0; c < kBkCopies; c++) {
+      for (int c = 0; c < K.ncopy; c++) {
         const double* gp = bk_gacc(K, par, c) + 2 * v;
         gv.x += __ldcg(gp);
         gv.y += __ldcg(gp + 1);
@@ -2347,10 +2380,11 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
     if (mode == 0) {
       for (int u = tid; u < p * p; u += kBkThreads) K.hostR0[u] = Rm[u];
     } else {
-      double2* hj = K.hostH + (size_t)j * (K.nb + 1) * p * p;
+      double2* hj = K.hostH + (size_t)(j % kBkHostRing) * (K.nb + 1) * p * p;
+      const double2* Hg = reinterpret_cast<const double2*>(bk_hacc(K, par, 0));
       for (int u = tid; u < (na_all + p) * p; u += kBkThreads) {
         const int a = u / p;
-        hj[u] = a < na_all ? Hs[(size_t)a * PP + (u - a * p)] : Rm[u - na_all * p];
+        hj[u] = a < na_all ? (g.hstream ? __ldcg(Hg + u) : Hs[(size_t)a * PP + (u - a * p)]) : Rm[u - na_all * p];
       }
     }
     __syncthreads();
@@ -2596,11 +2630,12 @@ Layout layout(int n, int m, int R, int precision) {
   if (bk) {
     int gsz[kBkMaxGroups], gc0[kBkMaxGroups];
     const int G = bk_groups(m, gsz, gc0);
-    const int nb = bk_steps(gsz[0], R);  // the largest group; a cycle never runs longer
     for (int g = 0; g < G; g++) {
-      sh += 2 * kBkCopies * (size_t)(nb + 1) * gsz[g] * gsz[g] * 2;
-      sg += 2 * kBkCopies * (size_t)gsz[g] * gsz[g] * 2;
-      sy += (size_t)nb * gsz[g] * gsz[g];
+      size_t a, b, c;
+      bk_group_sizes(gsz[g], R, &a, &b, &c);
+      sh += a;
+      sg += b;
+      sy += c;
     }
   }
   L.bk_hacc = take(sizeof(double) * sh);
@@ -2666,7 +2701,7 @@ int capture_graph(const std::function<int(cudaStream_t)>& body, cudaGraphExec_t*
 // Host-mapped buffers of the block solver (H column blocks, R_0, step
 // status), one set per host thread, grown on demand.
 struct BlockHost {
-  double2* H = nullptr;  // host view [nb][(nb + 1) p][p]
+  double2* H = nullptr;  // host view [kBkHostRing][(nb + 1) p][p]
   double2* dH = nullptr;  // device view
   double2* R0 = nullptr;
   double2* dR0 = nullptr;
@@ -2683,7 +2718,8 @@ thread_local BlockHost t_blocks[kBkMaxGroups];
 
 int block_host(int group, int p, int nb, BlockHost** out) {
   BlockHost& t_block = t_blocks[group];
-  const size_t need = (size_t)nb * (nb + 1) * p * p;
+  // H column blocks of the steps in flight (slot j % kBkHostRing), and the step records
+  const size_t need = std::max((size_t)kBkHostRing * (nb + 1) * p * p, (size_t)nb + 1);
   if (t_block.cap < need) {
     if (t_block.H) cudaFreeHost(t_block.H);
     if (t_block.R0) cudaFreeHost(t_block.R0);
@@ -2693,7 +2729,7 @@ int block_host(int group, int p, int nb, BlockHost** out) {
     t_block.cap = 0;
     BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.H, sizeof(double2) * need, cudaHostAllocMapped));
     BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.R0, sizeof(double2) * kBkMaxP * kBkMaxP, cudaHostAllocMapped));
-    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.S, sizeof(int) * (kBkVectors + 1), cudaHostAllocMapped));
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&t_block.S, sizeof(int) * need, cudaHostAllocMapped));
     BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_block.dH, t_block.H, 0));
     BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_block.dR0, t_block.R0, 0));
     BEM_CUDA_TRY(cudaHostGetDevicePointer((void**)&t_block.dS, t_block.S, 0));
@@ -2757,10 +2793,15 @@ struct BlockLS {
       for (int a = 0; a < (j + 2) * p; a++) x[a] = C{hj[a * p + t].x, hj[a * p + t].y};
       for (int a = (j + 2) * p; a < ld; a++) x[a] = C{0.0, 0.0};
     }
+    // the reflections of the earlier block columns: each one to all p new
+    // columns while it is in cache
+    for (int r = 0; r < c0; r++)
+      if (fac[r] != 0.0)
+        for (int t = 0; t < p; t++) reflect(r, &T[(size_t)(c0 + t) * ld]);
     for (int t = 0; t < p; t++) {
       const int cc = c0 + t;
       C* x = &T[(size_t)cc * ld];
-      for (int r = 0; r < cc; r++)
+      for (int r = c0; r < cc; r++)
         if (fac[r] != 0.0) reflect(r, x);
       // reflection for rows cc .. cc + p of column cc
       double nrm2 = 0.0;
@@ -2986,15 +3027,18 @@ int block_shape(int n, int m, int R, BkShape* out) {
   const int grid = (n + nr - 1) / nr;
   BkShape sh;
   sh.groups = bk_groups(m, sh.p, sh.col0);
-  const int nb_full = bk_steps(sh.p[0], R);
+  // staged H at the full cycle length; else H streamed per tile (one copy of
+  // its sums, the cycle up to kBkStreamVectors basis vectors per group)
   bool fit = false;
-  for (int nb = nb_full; nb >= 4 && !fit; nb--) {
+  for (int hstream = 0; hstream <= 1 && !fit; hstream++) {
+    const int nb = hstream ? std::min(kBkStreamVectors / sh.p[0], R) : bk_steps(sh.p[0], R);
     for (int tile = kBkTileMax; tile >= 16 && !fit; tile /= 2) {
       for (int stages = kBkMaxStages; stages >= 2 && !fit; stages--) {
         bool ok = true;
         for (int g = 0; g < sh.groups && ok; g++) {
           sh.g[g] = bk_geom(sh.p[g], nr, tile);
           sh.g[g].stages = stages;
+          sh.g[g].hstream = hstream;
           sh.smem[g] = bk_layout(sh.p[g], nr, sh.g[g], nb * sh.p[g]).total;
           ok = sh.smem[g] + 1024 <= (size_t)smem_optin;
         }
@@ -3146,6 +3190,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       K[g].nb = nbk;
       K[g].nr = bshape.nr;
       K[g].g = bshape.g[g];
+      K[g].hstream = bshape.g[g].hstream;
+      K[g].ncopy = K[g].hstream ? 1 : kBkCopies;
       K[g].hacc = (double*)(w + L.bk_hacc) + oh;
       K[g].gacc = (double*)(w + L.bk_gacc) + og;
       K[g].Yb = (double2*)(w + L.bk_y) + oy;
@@ -3153,9 +3199,11 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
       K[g].hostH = bh[g]->dH;
       K[g].hostR0 = bh[g]->dR0;
       K[g].hostS = bh[g]->dS;
-      oh += 2 * kBkCopies * (size_t)(nbk + 1) * pg * pg * 2;
-      og += 2 * kBkCopies * (size_t)pg * pg * 2;
-      oy += (size_t)nbk * pg * pg;
+      size_t a, b, c;
+      bk_group_sizes(pg, R, &a, &b, &c);
+      oh += a;
+      og += b;
+      oy += c;
     }
   }
   if (prec != BEM_PREC_FP32) {
@@ -3381,8 +3429,8 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
         first_cycle = false;
         for (int g = 0; g < ngr; g++) {
           const int pg = bshape.p[g];
-          BEM_CUDA_TRY(cudaMemsetAsync(K[g].hacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)(nbk + 1) * pg * pg * 2, s));
-          BEM_CUDA_TRY(cudaMemsetAsync(K[g].gacc, 0, sizeof(double) * 2 * kBkCopies * (size_t)pg * pg * 2, s));
+          BEM_CUDA_TRY(cudaMemsetAsync(K[g].hacc, 0, sizeof(double) * 2 * K[g].ncopy * (size_t)(nbk + 1) * pg * pg * 2, s));
+          BEM_CUDA_TRY(cudaMemsetAsync(K[g].gacc, 0, sizeof(double) * 2 * K[g].ncopy * (size_t)pg * pg * 2, s));
           for (int q = 0; q <= nbk; q++) bh[g]->S[q] = 0;  // no step of this solve is in flight here
           if ((rc = launch_block(P, K[g], bshape, g, 0, s))) return rc;
         }
@@ -3403,26 +3451,39 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
           const long long bbase = launched;
           // step jj of every group: a group stops at a breakdown (keeping the
           // steps before it) or when all its columns meet their tolerance
+          // one group's least-squares step (groups touch disjoint state)
+          auto group_step = [&](int g, int jj) -> bool {
+            const int pg = bshape.p[g], c0 = bshape.col0[g];
+            if (reinterpret_cast<volatile int*>(bh[g]->S)[jj] != 1 ||
+                !ls[g].add(jj, bh[g]->H + (size_t)(jj % kBkHostRing) * (nbk + 1) * pg * pg, bres.data() + c0)) {
+              gstop[g] = true;
+              return false;
+            }
+            kk[g] = jj + 1;
+            bool all = true;
+            for (int c = c0; c < c0 + pg; c++)
+              if (!(bres[c] <= btol[c])) all = false;
+            if (all) gconv[g] = gstop[g] = true;
+            return true;
+          };
           auto process = [&](int jj) -> int {
             BEM_CUDA_TRY(cudaEventSynchronize(ring->ev[(bbase + jj) % kSnapRing]));
             if (stop) return BEM_OK;
-            bool all_stopped = true, accepted = false;
-            for (int g = 0; g < ngr; g++) {
-              if (gstop[g]) continue;
-              const int pg = bshape.p[g], c0 = bshape.col0[g];
-              if (reinterpret_cast<volatile int*>(bh[g]->S)[jj] != 1 ||
-                  !ls[g].add(jj, bh[g]->H + (size_t)jj * (nbk + 1) * pg * pg, bres.data() + c0)) {
-                gstop[g] = true;
-                continue;
-              }
-              accepted = true;
-              kk[g] = jj + 1;
-              bool all = true;
-              for (int c = c0; c < c0 + pg; c++)
-                if (!(bres[c] <= btol[c])) all = false;
-              if (all) gconv[g] = gstop[g] = true;
-              all_stopped &= gstop[g];
+            bool accepted = false;
+            const double work = (double)(jj + 1) * bshape.p[0] * bshape.p[0] * bshape.p[0];
+            if (ngr > 1 && work >= 65536.0) {  // the block QR grows with the cycle: groups on their own threads
+              std::future<bool> f[kBkMaxGroups];
+              for (int g = 1; g < ngr; g++)
+                if (!gstop[g]) f[g] = std::async(std::launch::async, group_step, g, jj);
+              if (!gstop[0]) accepted |= group_step(0, jj);
+              for (int g = 1; g < ngr; g++)
+                if (f[g].valid()) accepted |= f[g].get();
+            } else {
+              for (int g = 0; g < ngr; g++)
+                if (!gstop[g]) accepted |= group_step(g, jj);
             }
+            bool all_stopped = true;
+            for (int g = 0; g < ngr; g++) all_stopped &= gstop[g];
             if (accepted) iters_done++;
             if (all_stopped) stop = true;
             return BEM_OK;
