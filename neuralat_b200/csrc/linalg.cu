@@ -2031,12 +2031,13 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
   const int par = j & 1;                    // this step's sums (the start uses parity 1)
   const int copy = blockIdx.x % K.ncopy;
   const int T = (na_all + TILE - 1) / TILE;  // basis tiles
-  // update units (unknown, 4-column group): one pass over the basis tiles if
-  // they fit the CTA's threads (slices of the vectors share out the rest),
-  // else one pass per kBkThreads units
+  // update units (unknown, 4-column group): if they fit the CTA's threads,
+  // register accumulators over all tiles (slices of the vectors share out
+  // the spare threads); else every tile updates W in shared memory unit by
+  // unit (a unit belongs to one thread within a tile)
   const int nunits = nr * CG;
-  const int npass = (nunits + kBkThreads - 1) / kBkThreads;
-  const int ST = T * (1 + npass);  // ring stages of the step: dots, then the update passes
+  const bool inplace = nunits > kBkThreads;
+  const int ST = 2 * T;  // ring stages of the step: dots, then the update
   const int rot = T > 0 ? (int)(blockIdx.x % T) : 0;
   int* err = &P.st->err;
   if (g.hs != HS || g.tile != TILE) {  // host geometry built for another lane layout (uniform over the grid)
@@ -2154,62 +2155,74 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
     }
     __syncthreads();
 
-    // ---- W' = W - Q H: thread (unknown, 4 columns[, vector slice]) per pass ----
-    const int uas = npass == 1 ? g.as : 1;  // vector slices (one pass only)
-    for (int pass = 0; pass < npass; pass++) {
-      const int unit = npass == 1 ? tid % nunits : pass * kBkThreads + tid;
-      const int u_as = npass == 1 ? tid / nunits : 0;
-      const int u_cg = unit / nr;
-      const int u_i = unit - u_cg * nr;
-      const bool u_on = unit < nunits && u_as < uas && u_i < nvr;
-      double2 acc[4];
+    // ---- W' = W - Q H ----
+    const int uas = inplace ? 1 : g.as;  // vector slices (register mode)
+    const int u_as = inplace ? 0 : tid / nunits;
+    double2 acc[4];
 #pragma unroll
-      for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
-      // streamed H: thread t < TILE * PP carries entry (t / PP, t % PP) of
-      // the next tile's rows in a register, stored after the current tile
-      const double2* Hg = reinterpret_cast<const double2*>(bk_hacc(K, par, 0));  // one copy when streamed
-      auto h_fetch = [&](int s2) -> double2 {
-        const int t = tid;
-        if (!g.hstream || t >= TILE * PP || s2 >= T * (2 + pass)) return make_double2(0.0, 0.0);
-        const int a = ((rot + s2) % T) * TILE + t / PP, b = t % PP;
-        return (a < na_all && b < p) ? __ldcg(Hg + (size_t)a * p + b) : make_double2(0.0, 0.0);
-      };
-      double2 hnext = h_fetch(T * (1 + pass));
-      for (int s = T * (1 + pass); s < T * (2 + pass); s++) {
-        const int slot = s % g.stages;
-        const int a0 = ((rot + s) % T) * TILE, na = min(TILE, na_all - a0);
-        if (g.hstream) {  // this tile's H rows into buffer s & 1 (its previous readers passed the last barrier)
-          if (tid < TILE * PP) Hs[(size_t)(s & 1) * TILE * PP + tid] = hnext;
-          hnext = h_fetch(s + 1);
-          __syncthreads();
-        }
-        mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
-        if (u_on) {
-          const float2* q = ring + (size_t)slot * TILE * g.rs + u_i;
-          const double2* h = g.hstream ? Hs + (size_t)(s & 1) * TILE * PP + u_cg * 4 : Hs + (size_t)a0 * PP + u_cg * 4;
-          for (int al = u_as; al < na; al += uas) {
-            const float2 qf = q[(size_t)al * g.rs];
-            const double qx = qf.x, qy = qf.y;
+    for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
+    // streamed H: thread t < TILE * PP carries entry (t / PP, t % PP) of the
+    // next tile's rows in a register, stored after the current tile
+    const double2* Hg = reinterpret_cast<const double2*>(bk_hacc(K, par, 0));  // one copy when streamed
+    auto h_fetch = [&](int s2) -> double2 {
+      if (!g.hstream || tid >= TILE * PP || s2 >= 2 * T) return make_double2(0.0, 0.0);
+      const int a = ((rot + s2) % T) * TILE + tid / PP, b = tid % PP;
+      return (a < na_all && b < p) ? __ldcg(Hg + (size_t)a * p + b) : make_double2(0.0, 0.0);
+    };
+    double2 hnext = h_fetch(T);
+    for (int s = T; s < 2 * T; s++) {
+      const int slot = s % g.stages;
+      const int a0 = ((rot + s) % T) * TILE, na = min(TILE, na_all - a0);
+      if (g.hstream) {  // this tile's H rows into buffer s & 1 (its previous readers passed the last barrier)
+        if (tid < TILE * PP) Hs[(size_t)(s & 1) * TILE * PP + tid] = hnext;
+        hnext = h_fetch(s + 1);
+        __syncthreads();
+      }
+      mbar_wait(&bars[slot], (uint32_t)(s / g.stages) & 1u, err);
+      const double2* hbase = g.hstream ? Hs + (size_t)(s & 1) * TILE * PP : Hs + (size_t)a0 * PP;
+      for (int unit = inplace ? tid : tid % nunits; unit < (inplace ? nunits : tid % nunits + 1);
+           unit += kBkThreads) {
+        const int u_cg = unit / nr, u_i = unit - u_cg * nr;
+        if (u_as >= uas || u_i >= nvr) continue;
+        if (inplace)
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-              const double2 hv = h[(size_t)al * PP + c];
-              acc[c].x = fma(qx, hv.x, fma(-qy, hv.y, acc[c].x));
-              acc[c].y = fma(qx, hv.y, fma(qy, hv.x, acc[c].y));
-            }
+          for (int c = 0; c < 4; c++) acc[c] = make_double2(0.0, 0.0);
+        const float2* q = ring + (size_t)slot * TILE * g.rs + u_i;
+        const double2* h = hbase + u_cg * 4;
+        for (int al = u_as; al < na; al += uas) {
+          const float2 qf = q[(size_t)al * g.rs];
+          const double qx = qf.x, qy = qf.y;
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            const double2 hv = h[(size_t)al * PP + c];
+            acc[c].x = fma(qx, hv.x, fma(-qy, hv.y, acc[c].x));
+            acc[c].y = fma(qx, hv.y, fma(qy, hv.x, acc[c].y));
           }
         }
-        __syncthreads();
-        if (wq == 0 && s + g.stages < ST) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
+        if (inplace)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            double2* wp = W + (size_t)(u_cg * 4 + c) * g.lw + u_i;
+            wp->x -= acc[c].x;
+            wp->y -= acc[c].y;
+          }
       }
-      if (pass + 1 == npass && tid == 0)
-        // every issued stage has been waited for (after an error, a wait may
-        // have given up: the last stage issued into each slot is drained
-        // before the ring is reused for the slice sums)
-        for (int sl = 0; sl < min(g.stages, ST); sl++) {
-          const int s_last = sl + ((ST - 1 - sl) / g.stages) * g.stages;
-          mbar_wait_drain(&bars[sl], (uint32_t)(s_last / g.stages) & 1u);
-        }
       __syncthreads();
+      if (wq == 0 && s + g.stages < ST) bk_issue(P, K, ring, bars, s + g.stages, T, rot, na_all, i0, nvc);
+    }
+    // every issued stage has been waited for (after an error, a wait may have
+    // given up: the last stage issued into each slot is drained before the
+    // ring is reused for the slice sums)
+    if (tid == 0)
+      for (int sl = 0; sl < min(g.stages, ST); sl++) {
+        const int s_last = sl + ((ST - 1 - sl) / g.stages) * g.stages;
+        mbar_wait_drain(&bars[sl], (uint32_t)(s_last / g.stages) & 1u);
+      }
+    __syncthreads();
+    if (!inplace) {
+      const int unit = tid % nunits;
+      const int u_cg = unit / nr, u_i = unit - u_cg * nr;
+      const bool u_on = u_as < uas && u_i < nvr;
       if (uas > 1) {  // slice sums through the (drained) ring
         double2* part = reinterpret_cast<double2*>(ring);  // [as - 1][CG][nr][4]
         if (u_on && u_as > 0) {
@@ -2228,14 +2241,13 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
             }
           }
       }
-      if (u_on && u_as == 0) {
+      if (u_on && u_as == 0)
 #pragma unroll
         for (int c = 0; c < 4; c++) {
           double2* wp = W + (size_t)(u_cg * 4 + c) * g.lw + u_i;
           wp->x -= acc[c].x;
           wp->y -= acc[c].y;
         }
-      }
     }
     __syncthreads();
   }
