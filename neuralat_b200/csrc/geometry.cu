@@ -47,35 +47,59 @@ struct HostGeom {
 int analyse_host(HostGeom& g);
 
 // The most recent analysis of this host thread: bem_geometry_bytes followed by
-// bem_geometry_build on an unchanged mesh analyses it once.
+// bem_geometry_build on an unchanged mesh analyses it once, and a rebuild of
+// an unchanged mesh re-uploads its staged integer tables.
 thread_local HostGeom t_last;
 thread_local bool t_last_valid = false;
 
-int analyse(const float* d_vertices, int nv, const int* d_triangles, int nt, cudaStream_t s, HostGeom& g) {
-  if (nv <= 0 || nt <= 0 || !d_vertices || !d_triangles) return BEM_ERR_INVALID_ARGUMENT;
-  std::vector<float> vh(3 * (size_t)nv);
-  std::vector<int> th(3 * (size_t)nt);
-  BEM_CUDA_TRY(cudaMemcpyAsync(vh.data(), d_vertices, sizeof(float) * 3 * nv, cudaMemcpyDeviceToHost, s));
-  BEM_CUDA_TRY(cudaMemcpyAsync(th.data(), d_triangles, sizeof(int) * 3 * nt, cudaMemcpyDeviceToHost, s));
-  BEM_CUDA_TRY(cudaStreamSynchronize(s));
-  if (t_last_valid && t_last.nv == nv && t_last.nt == nt &&
-      std::memcmp(t_last.vertices.data(), vh.data(), vh.size() * sizeof(float)) == 0 &&
-      std::memcmp(t_last.triangles.data(), th.data(), th.size() * sizeof(int)) == 0) {
-    g = t_last;
+// Pinned host buffer of this thread (grown on demand).
+struct PinnedBuf {
+  char* p = nullptr;
+  size_t cap = 0;
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  int ensure(size_t n) {
+    if (cap >= n) return BEM_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    BEM_CUDA_TRY(cudaHostAlloc((void**)&p, n, cudaHostAllocDefault));
+    cap = n;
     return BEM_OK;
   }
-  g = HostGeom{};
-  g.nv = nv;
-  g.nt = nt;
-  g.vertices.swap(vh);
-  g.triangles.swap(th);
-  t_last_valid = false;
-  const int rc = analyse_host(g);
-  if (rc == BEM_OK) {
-    t_last = g;
-    t_last_valid = true;
+};
+thread_local PinnedBuf t_download;  // the mesh read back for the comparison with t_last
+thread_local PinnedBuf t_stage;     // t_last's integer tables as uploaded (valid if t_stage_ok)
+thread_local bool t_stage_ok = false;
+
+// Analysis of the mesh on the device (t_last; valid until the next call on
+// this thread).
+int analyse(const float* d_vertices, int nv, const int* d_triangles, int nt, cudaStream_t s, const HostGeom** out) {
+  if (nv <= 0 || nt <= 0 || !d_vertices || !d_triangles) return BEM_ERR_INVALID_ARGUMENT;
+  const size_t vb = sizeof(float) * 3 * (size_t)nv, tb = sizeof(int) * 3 * (size_t)nt;
+  int rc = t_download.ensure(vb + tb);
+  if (rc) return rc;
+  BEM_CUDA_TRY(cudaMemcpyAsync(t_download.p, d_vertices, vb, cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaMemcpyAsync(t_download.p + vb, d_triangles, tb, cudaMemcpyDeviceToHost, s));
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (t_last_valid && t_last.nv == nv && t_last.nt == nt && std::memcmp(t_last.vertices.data(), t_download.p, vb) == 0 &&
+      std::memcmp(t_last.triangles.data(), t_download.p + vb, tb) == 0) {
+    *out = &t_last;
+    return BEM_OK;
   }
-  return rc;
+  t_last_valid = false;
+  t_stage_ok = false;
+  t_last = HostGeom{};
+  t_last.nv = nv;
+  t_last.nt = nt;
+  t_last.vertices.assign((const float*)t_download.p, (const float*)t_download.p + 3 * (size_t)nv);
+  t_last.triangles.assign((const int*)(t_download.p + vb), (const int*)(t_download.p + vb) + 3 * (size_t)nt);
+  rc = analyse_host(t_last);
+  if (rc) return rc;
+  t_last_valid = true;
+  *out = &t_last;
+  return BEM_OK;
 }
 
 int analyse_host(HostGeom& g) {
@@ -356,38 +380,46 @@ using namespace bemb;
 extern "C" int bem_geometry_bytes(const float* vertices, int nv, const int* triangles, int nt, size_t* bytes,
                                   bem_stream_t stream) {
   if (!bytes) return BEM_ERR_INVALID_ARGUMENT;
-  HostGeom g;
-  int rc = analyse(vertices, nv, triangles, nt, (cudaStream_t)stream, g);
+  const HostGeom* g = nullptr;
+  int rc = analyse(vertices, nv, triangles, nt, (cudaStream_t)stream, &g);
   if (rc) return rc;
-  *bytes = (size_t)g.hdr.bytes;
+  *bytes = (size_t)g->hdr.bytes;
   return BEM_OK;
 }
 
 extern "C" int bem_geometry_build(const float* vertices, int nv, const int* triangles, int nt, void* geom,
                                   size_t geom_bytes, bem_stream_t stream) {
   cudaStream_t s = (cudaStream_t)stream;
-  HostGeom g;
-  int rc = analyse(vertices, nv, triangles, nt, s, g);
+  const HostGeom* gp = nullptr;
+  int rc = analyse(vertices, nv, triangles, nt, s, &gp);
   if (rc) return rc;
+  const HostGeom& g = *gp;
   if (!geom || geom_bytes < g.hdr.bytes) return BEM_ERR_WORKSPACE;
   const GeomHeader& h = g.hdr;
-  // stage the integer tables in one pinned host buffer, then one upload
-  std::vector<char> stage(h.off_trirec, 0);
-  std::memcpy(stage.data(), &h, sizeof(h));
-  std::memcpy(stage.data() + h.off_vertices, g.vertices.data(), sizeof(float) * 3 * (size_t)nv);
-  std::memcpy(stage.data() + h.off_triangles, g.triangles.data(), sizeof(int) * 3 * (size_t)nt);
-  std::memcpy(stage.data() + h.off_perm, g.perm.data(), sizeof(int) * (size_t)nt);
-  std::memcpy(stage.data() + h.off_tiles, g.tiles.data(), sizeof(TileRec) * (size_t)g.ntiles);
-  if (h.n_edge) std::memcpy(stage.data() + h.off_edge_pairs, g.edge_pairs.data(), sizeof(int2) * h.n_edge);
-  if (h.n_vert) std::memcpy(stage.data() + h.off_vert_pairs, g.vert_pairs.data(), sizeof(int2) * h.n_vert);
-  BEM_CUDA_TRY(cudaMemcpyAsync(geom, stage.data(), stage.size(), cudaMemcpyHostToDevice, s));
+  // the integer tables in one pinned staging buffer (kept while the mesh is
+  // unchanged), then one upload
+  const size_t nstage = h.off_trirec;
+  if (!t_stage_ok) {
+    if ((rc = t_stage.ensure(nstage))) return rc;
+    char* st = t_stage.p;
+    std::memset(st, 0, nstage);
+    std::memcpy(st, &h, sizeof(h));
+    std::memcpy(st + h.off_vertices, g.vertices.data(), sizeof(float) * 3 * (size_t)nv);
+    std::memcpy(st + h.off_triangles, g.triangles.data(), sizeof(int) * 3 * (size_t)nt);
+    std::memcpy(st + h.off_perm, g.perm.data(), sizeof(int) * (size_t)nt);
+    std::memcpy(st + h.off_tiles, g.tiles.data(), sizeof(TileRec) * (size_t)g.ntiles);
+    if (h.n_edge) std::memcpy(st + h.off_edge_pairs, g.edge_pairs.data(), sizeof(int2) * h.n_edge);
+    if (h.n_vert) std::memcpy(st + h.off_vert_pairs, g.vert_pairs.data(), sizeof(int2) * h.n_vert);
+    t_stage_ok = true;
+  }
+  BEM_CUDA_TRY(cudaMemcpyAsync(geom, t_stage.p, nstage, cudaMemcpyHostToDevice, s));
   char* b = (char*)geom;
   (geom_records_kernel<<<(nt + 127) / 128, 128, 0, s>>>(
       nt, (const float*)(b + h.off_vertices), (const int*)(b + h.off_triangles), (const int*)(b + h.off_perm),
       (TriRec*)(b + h.off_trirec), (TriRec*)(b + h.off_trirec_orig), (float*)(b + h.off_normals),
       (float*)(b + h.off_curls), (BmRec*)(b + h.off_bmrec)), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
-  BEM_CUDA_TRY(cudaStreamSynchronize(s));  // staging buffer is pageable host memory
+  BEM_CUDA_TRY(cudaStreamSynchronize(s));  // the staging buffer serves the next build of this thread
   cache_put(geom, h);
   return BEM_OK;
 }
