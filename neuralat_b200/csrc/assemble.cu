@@ -222,8 +222,9 @@ __device__ __forceinline__ void regular_item(RegSmem<DO_V, DO_K>& sm, const Geom
       const int nI1 = has_t1 ? sm.tileI[1].nlv : 0;
       const int nJ = sm.tileJ.nlv;
       const int ncol = 3 * ntriJ;
+      const float rcol = 1.f / (float)ncol, rJ = 1.f / (float)(nJ > 0 ? nJ : 1);
       for (int e = tid; e < (nI0 + nI1) * ncol; e += kRegThreads) {
-        const int ai = e / ncol;
+        const int ai = div_by(e, ncol, rcol);
         const int col = e - ai * ncol;
         const int s = ai >= nI0;
         const int a = ai - s * nI0;
@@ -249,7 +250,7 @@ __device__ __forceinline__ void regular_item(RegSmem<DO_V, DO_K>& sm, const Geom
       }
       __syncthreads();
       for (int e = tid; e < (nI0 + nI1) * nJ; e += kRegThreads) {
-        const int ai = e / nJ;
+        const int ai = div_by(e, nJ, rJ);
         const int b = e - ai * nJ;
         const int s = ai >= nI0;
         const int a = ai - s * nI0;
@@ -504,8 +505,9 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     const TileRec& TI = sm.tileI;
     const int nI = TI.nlv, nJ = tileJ.nlv;
     const int ncol = 3 * ntriJ;
+    const float rcol = 1.f / (float)ncol, rJ = 1.f / (float)(nJ > 0 ? nJ : 1);
     for (int e = tid; e < nI * ncol; e += kSymThreads) {
-      const int a = e / ncol;
+      const int a = div_by(e, ncol, rcol);
       const int col = e - a * ncol;
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int rep = TI.lv_corner[ca0];
@@ -526,7 +528,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
     }
     __syncthreads();
     for (int e = tid; e < nI * nJ; e += kSymThreads) {
-      const int a = e / nJ;
+      const int a = div_by(e, nJ, rJ);
       const int b = e - a * nJ;
       const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];

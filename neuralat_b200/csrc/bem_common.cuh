@@ -39,6 +39,16 @@ constexpr float kEps = 1e-3f;  // r clamp of the reference kernels (potential.h:
 // One instruction applies the same IEEE round-to-nearest operation to both
 // lanes of a float2, so a packed expression gives bit-identical results to
 // the two scalar ones while issuing half the instructions.
+// e / d for 0 <= e < 2^24 and d >= 1, with rd = 1.f / d computed once by the
+// caller: a float multiply and one correction step instead of an integer
+// division sequence in the inner loops.
+__device__ __forceinline__ int div_by(int e, int d, float rd) {
+  int q = __float2int_rz((float)e * rd);
+  const int r = e - q * d;
+  q += (r >= d) - (r < 0);
+  return q;
+}
+
 __device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) {
   float2 d;
   asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"

@@ -292,8 +292,9 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
     const TileRec& TI = sm.tileI;
     const int nI = TI.nlv, nJ = tileJ.nlv;
     const int ncol = 3 * ntriJ;
+    const float rcol = 1.f / (float)ncol, rJ = 1.f / (float)(nJ > 0 ? nJ : 1);
     for (int e = tid; e < nI * ncol; e += kBmThreads) {
-      const int a = e / ncol;
+      const int a = div_by(e, ncol, rcol);
       const int col = e - a * ncol;
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int rep = TI.lv_corner[ca0];
@@ -318,7 +319,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
     }
     __syncthreads();
     for (int e = tid; e < nI * nJ; e += kBmThreads) {
-      const int a = e / nJ;
+      const int a = div_by(e, nJ, rJ);
       const int b = e - a * nJ;
       const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
