@@ -512,6 +512,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int rep = TI.lv_corner[ca0];
       float2 v = sm.slotV[rep][col], kk = sm.slotK[rep][col], mm = sm.slotM[rep][col];
+#pragma unroll 4
       for (int ca = ca0 + 1; ca < ca1; ca++) {
         const int row = TI.lv_corner[ca];
         const float2 v1 = sm.slotV[row][col], k1 = sm.slotK[row][col], m1 = sm.slotM[row][col];
@@ -533,6 +534,7 @@ __device__ __forceinline__ void regular_sym_item(SymSmem& sm, const GeomView& g,
       const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
       float2 acc_v = make_float2(0.f, 0.f), acc_k = make_float2(0.f, 0.f), acc_m = make_float2(0.f, 0.f);
+#pragma unroll 4
       for (int cb = cb0; cb < cb1; cb++) {
         const int col = tileJ.lv_corner[cb];
         const float2 v1 = sm.slotV[rep][col], k1 = sm.slotK[rep][col], m1 = sm.slotM[rep][col];

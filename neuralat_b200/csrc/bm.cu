@@ -299,6 +299,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int rep = TI.lv_corner[ca0];
       float2 l = sm.slotL[rep][col], lt = sm.slotLT[rep][col], rr = sm.slotR[rep][col], rt = sm.slotRT[rep][col];
+#pragma unroll 4
       for (int ca = ca0 + 1; ca < ca1; ca++) {
         const int row = TI.lv_corner[ca];
         const float2 l1 = sm.slotL[row][col], lt1 = sm.slotLT[row][col];
@@ -324,6 +325,7 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
       float2 l = make_float2(0.f, 0.f), lt = l, rr = l, rt = l;
+#pragma unroll 4
       for (int cb = cb0; cb < cb1; cb++) {
         const int col = tileJ.lv_corner[cb];
         const float2 l1 = sm.slotL[rep][col], lt1 = sm.slotLT[rep][col];
