@@ -416,10 +416,22 @@ __global__ void __launch_bounds__(256) tc_split_a_f16_kernel(const float* __rest
                                                             __half* __restrict__ Ah, __half* __restrict__ Al,
                                                             float* __restrict__ rinv) {
   __shared__ float red[8];
+  // n even: rows start 16-byte aligned (float4 reads) and ld is a multiple of
+  // 4 (8-byte stores of four halves per plane)
+  const bool vec = (n & 1) == 0 && (ld & 3) == 0;
   for (int r = blockIdx.x; r < n; r += gridDim.x) {
     const float* row = A + (size_t)r * 2 * n;
     float mx = 0.f;
-    for (int c = threadIdx.x; c < 2 * n; c += 256) mx = fmaxf(mx, fabsf(row[c]));
+    if (vec) {
+      const float4* row4 = reinterpret_cast<const float4*>(row);
+#pragma unroll 4
+      for (int c = threadIdx.x; c < n / 2; c += 256) {
+        const float4 v = row4[c];
+        mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+      }
+    } else {
+      for (int c = threadIdx.x; c < 2 * n; c += 256) mx = fmaxf(mx, fabsf(row[c]));
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
@@ -429,11 +441,36 @@ __global__ void __launch_bounds__(256) tc_split_a_f16_kernel(const float* __rest
     for (int w = 0; w < 8; w++) rmx = fmaxf(rmx, red[w]);
     const float q = f16_scale(rmx);
     if (threadIdx.x == 0) rinv[r] = 1.f / q;
-    for (int c = threadIdx.x; c < ld; c += 256) {
-      const float a = c < 2 * n ? row[c] * q : 0.f;
-      const __half h = __float2half_rn(a);
-      Ah[(size_t)r * ld + c] = h;
-      Al[(size_t)r * ld + c] = __float2half_rn(a - __half2float(h));
+    if (vec) {
+      const float4* row4 = reinterpret_cast<const float4*>(row);
+      uint2* h4 = reinterpret_cast<uint2*>(Ah + (size_t)r * ld);
+      uint2* l4 = reinterpret_cast<uint2*>(Al + (size_t)r * ld);
+#pragma unroll 4
+      for (int c = threadIdx.x; c < ld / 4; c += 256) {
+        float a[4] = {0.f, 0.f, 0.f, 0.f};
+        if (c < n / 2) {
+          const float4 v = row4[c];
+          a[0] = v.x * q;
+          a[1] = v.y * q;
+          a[2] = v.z * q;
+          a[3] = v.w * q;
+        }
+        __align__(8) __half hi[4], lo[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          hi[e] = __float2half_rn(a[e]);
+          lo[e] = __float2half_rn(a[e] - __half2float(hi[e]));
+        }
+        h4[c] = *reinterpret_cast<const uint2*>(hi);
+        l4[c] = *reinterpret_cast<const uint2*>(lo);
+      }
+    } else {
+      for (int c = threadIdx.x; c < ld; c += 256) {
+        const float a = c < 2 * n ? row[c] * q : 0.f;
+        const __half h = __float2half_rn(a);
+        Ah[(size_t)r * ld + c] = h;
+        Al[(size_t)r * ld + c] = __float2half_rn(a - __half2float(h));
+      }
     }
     __syncthreads();  // red is reused by the next row
   }
