@@ -613,9 +613,30 @@ template <>
 __device__ __forceinline__ void sincos_t<double>(double x, double* s, double* c) {
   sincos(x, s, c);
 }
+// FP32 (edge and vertex pairs): the hardware approximation, accurate to a few
+// 1e-7 absolute for the |k r| <= ~1 of touching triangles (the regular kernels
+// use it at larger arguments).
 template <>
 __device__ __forceinline__ void sincos_t<float>(float x, float* s, float* c) {
-  sincosf(x, s, c);
+  __sincosf(x, s, c);
+}
+
+// 1 / r and r from r^2 (r clamped to kEps as in potential.h): rsqrt in FP32, a
+// correctly rounded sqrt and division in FP64.
+template <typename R>
+__device__ __forceinline__ void inv_dist(R r2, R* r, R* inv_r);
+template <>
+__device__ __forceinline__ void inv_dist<double>(double r2, double* r, double* inv_r) {
+  double rr = sqrt(r2);
+  if (rr < kEps) rr = kEps;
+  *r = rr;
+  *inv_r = 1.0 / rr;
+}
+template <>
+__device__ __forceinline__ void inv_dist<float>(float r2, float* r, float* inv_r) {
+  const float ri = fminf(rsqrtf(r2), 1.0f / kEps);
+  *inv_r = ri;
+  *r = fmaxf(r2 * ri, kEps);
 }
 
 // Re-ordering of the reference (integrand.h:351-387): for a common edge the
@@ -678,12 +699,11 @@ struct SingularAcc {
     const R yy = ly0 * b[0].y + ly1 * b[1].y + ly2 * b[2].y;
     const R yz = ly0 * b[0].z + ly1 * b[1].z + ly2 * b[2].z;
     const R dx = yx - xx, dy = yy - xy, dz = yz - xz;
-    R r = sqrt(dx * dx + dy * dy + dz * dz);
-    if (r < R(kEps)) r = R(kEps);
+    R r, inv_r;
+    inv_dist<R>(dx * dx + dy * dy + dz * dz, &r, &inv_r);
     R s, c;
     const R kr = k * r;
     sincos_t<R>(kr, &s, &c);
-    const R inv_r = R(1) / r;
     const R gvr = c * inv_r * ww, gvi = s * inv_r * ww;
     R gkr = 0, gki = 0;
     if (DO_K) {
