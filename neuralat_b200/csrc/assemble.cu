@@ -824,26 +824,47 @@ __device__ __forceinline__ void singular_pair(const GeomView& g, int ti, int tj,
     const R w0 = R(gl4_w(i0)) * R(gl4_w(i1)) * R(gl4_w(i2)) * R(gl4_w(i3)) * jw;
     acc.point(xi, e1, e2, e3, w0);
   }
-  // reduce; lane e (< 9) owns V entry e, lane 9 + e owns K entry e
+  // reduce: values 0..31 by a transpose-reduce (lane L ends with the warp
+  // total of value L), values 32..35 by plain sums; then lane e (< 9) takes
+  // V entry e, lane 9 + e K entry e
+  constexpr int NV = (DO_V ? 18 : 0) + (DO_K ? 18 : 0);
+  R t[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) {
+    const int vi = i, ki = DO_V ? i - 18 : i;
+    t[i] = (DO_V && vi < 18) ? acc.v[vi] : ((DO_K && ki >= 0 && ki < 18) ? acc.kk[ki] : R(0));
+  }
+  R extra[4] = {R(0), R(0), R(0), R(0)};
+  if (NV > 32) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) extra[i] = warp_sum(acc.kk[14 + i]);
+  }
+#pragma unroll
+  for (int o = 16, half = 16; o >= 1; o >>= 1, half >>= 1) {
+    const bool hi = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < half; i++) {
+      const R send = hi ? t[i] : t[i + half];
+      const R keep = hi ? t[i + half] : t[i];
+      t[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  const R mine = t[0];  // warp total of value `lane`
+  // value indices of this lane's entry (re, im)
+  const int e = lane < 9 ? lane : lane - 9;
+  const int base = lane < 9 ? 0 : (DO_V ? 18 : 0);
+  const int ire = base + 2 * e, iim = ire + 1;
+  const R vre = __shfl_sync(0xffffffffu, mine, ire & 31), vim = __shfl_sync(0xffffffffu, mine, iim & 31);
+  R re = ire < 32 ? vre : extra[ire - 32 < 4 ? ire - 32 : 0];
+  R im = iim < 32 ? vim : extra[iim - 32 < 4 ? iim - 32 : 0];
   float out_re = 0.f, out_im = 0.f;
   int out_row = -1, out_col = -1;
-#pragma unroll
-  for (int e = 0; e < 9; e++) {
-    R vr = DO_V ? warp_sum(acc.v[2 * e]) : R(0), vi = DO_V ? warp_sum(acc.v[2 * e + 1]) : R(0);
-    R kr = DO_K ? warp_sum(acc.kk[2 * e]) : R(0), ki = DO_K ? warp_sum(acc.kk[2 * e + 1]) : R(0);
-    const int ii = e / 3, jj = e % 3;
-    if (lane == e) {
-      out_re = (float)(vr * R(v_scale));
-      out_im = (float)(vi * R(v_scale));
-      out_row = pick3(s0, s1, s2, pi_[ii]);
-      out_col = pick3(t0, t1, t2, pj_[jj]);
-    }
-    if (lane == 9 + e) {
-      out_re = (float)(kr * R(k_scale));
-      out_im = (float)(ki * R(k_scale));
-      out_row = pick3(s0, s1, s2, pi_[ii]);
-      out_col = pick3(t0, t1, t2, pj_[jj]);
-    }
+  if (lane < 18) {
+    const R sc = lane < 9 ? R(v_scale) : R(k_scale);
+    out_re = (float)(re * sc);
+    out_im = (float)(im * sc);
+    out_row = pick3(s0, s1, s2, pi_[e / 3]);
+    out_col = pick3(t0, t1, t2, pj_[e % 3]);
   }
   const size_t nv = (size_t)g.nv;
   if (lane < 9 && DO_V) atomicAdd(&V[out_row * nv + out_col], make_float2(out_re, out_im));
