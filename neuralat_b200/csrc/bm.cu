@@ -69,10 +69,12 @@ __device__ __forceinline__ float bm_point(const TriRec& r, const BmRec& b, int c
 }
 
 struct BmSmem {
+  // rhs_ji[b][a] is not stored: rhs_ji^T - rhs_ij = (i/k)(T - U) =
+  // (i/k)(lhs_ij - lhs_ji^T) entry by entry, so it follows from the three
+  // reduced slots of each vertex pair.
   float2 slotL[kBmCorners][kBmStride];   // lhs_ij[a][b] at [3 tl + a][3 tt + b]
   float2 slotLT[kBmCorners][kBmStride];  // lhs_ji[b][a], same indexing
   float2 slotR[kBmCorners][kBmStride];
-  float2 slotRT[kBmCorners][kBmStride];
   float xs[18][kBmTest];                 // test quadrature points [coordinate][tl]
   float xc[9][kBmTest];                  // test curls [3 a + d][tl]
   TriRec trial[2][kTile];                // trial tile, double-buffered
@@ -269,7 +271,6 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
           sm.slotL[3 * tl + a][3 * tt + b] = make_float2(lx + Tx, ly + Ty);
           sm.slotLT[3 * tl + a][3 * tt + b] = make_float2(lx + Ux, ly + Uy);
           sm.slotR[3 * tl + a][3 * tt + b] = make_float2(fmaf(-Uy, kinv, -Sx), fmaf(Ux, kinv, -Sy));
-          sm.slotRT[3 * tl + a][3 * tt + b] = make_float2(fmaf(-Ty, kinv, -Sx), fmaf(Tx, kinv, -Sy));
         }
     } else if (tt < ntriJ) {
 #pragma unroll
@@ -279,7 +280,6 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
           sm.slotL[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
           sm.slotLT[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
           sm.slotR[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
-          sm.slotRT[3 * tl + a][3 * tt + b] = make_float2(0.f, 0.f);
         }
     }
     __syncthreads();
@@ -298,25 +298,21 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       const int col = e - a * ncol;
       const int ca0 = TI.lv_ptr[a], ca1 = TI.lv_ptr[a + 1];
       const int rep = TI.lv_corner[ca0];
-      float2 l = sm.slotL[rep][col], lt = sm.slotLT[rep][col], rr = sm.slotR[rep][col], rt = sm.slotRT[rep][col];
+      float2 l = sm.slotL[rep][col], lt = sm.slotLT[rep][col], rr = sm.slotR[rep][col];
 #pragma unroll 4
       for (int ca = ca0 + 1; ca < ca1; ca++) {
         const int row = TI.lv_corner[ca];
-        const float2 l1 = sm.slotL[row][col], lt1 = sm.slotLT[row][col];
-        const float2 r1 = sm.slotR[row][col], rt1 = sm.slotRT[row][col];
+        const float2 l1 = sm.slotL[row][col], lt1 = sm.slotLT[row][col], r1 = sm.slotR[row][col];
         l.x += l1.x;
         l.y += l1.y;
         lt.x += lt1.x;
         lt.y += lt1.y;
         rr.x += r1.x;
         rr.y += r1.y;
-        rt.x += rt1.x;
-        rt.y += rt1.y;
       }
       sm.slotL[rep][col] = l;
       sm.slotLT[rep][col] = lt;
       sm.slotR[rep][col] = rr;
-      sm.slotRT[rep][col] = rt;
     }
     __syncthreads();
     for (int e = tid; e < nI * nJ; e += kBmThreads) {
@@ -324,24 +320,21 @@ __device__ __forceinline__ void bm_item(BmSmem& sm, const GeomView& g, float k, 
       const int b = e - a * nJ;
       const int rep = TI.lv_corner[TI.lv_ptr[a]];
       const int cb0 = tileJ.lv_ptr[b], cb1 = tileJ.lv_ptr[b + 1];
-      float2 l = make_float2(0.f, 0.f), lt = l, rr = l, rt = l;
+      float2 l = make_float2(0.f, 0.f), lt = l, rr = l;
 #pragma unroll 4
       for (int cb = cb0; cb < cb1; cb++) {
         const int col = tileJ.lv_corner[cb];
-        const float2 l1 = sm.slotL[rep][col], lt1 = sm.slotLT[rep][col];
-        const float2 r1 = sm.slotR[rep][col], rt1 = sm.slotRT[rep][col];
+        const float2 l1 = sm.slotL[rep][col], lt1 = sm.slotLT[rep][col], r1 = sm.slotR[rep][col];
         l.x += l1.x;
         l.y += l1.y;
         lt.x += lt1.x;
         lt.y += lt1.y;
         rr.x += r1.x;
         rr.y += r1.y;
-        rt.x += rt1.x;
-        rt.y += rt1.y;
       }
+      const float2 rt = make_float2(fmaf(lt.y - l.y, kinv, rr.x), fmaf(l.x - lt.x, kinv, rr.y));
       const int A = TI.vid[a], B = tileJ.vid[b];
-      if (l.x != 0.f || l.y != 0.f || lt.x != 0.f || lt.y != 0.f || rr.x != 0.f || rr.y != 0.f || rt.x != 0.f ||
-          rt.y != 0.f) {
+      if (l.x != 0.f || l.y != 0.f || lt.x != 0.f || lt.y != 0.f || rr.x != 0.f || rr.y != 0.f) {
         atomicAdd(&L[(size_t)A * nv + B], l);
         atomicAdd(&L[(size_t)B * nv + A], lt);
         atomicAdd(&Rm[(size_t)A * nv + B], rr);
