@@ -607,38 +607,6 @@ struct R3 {
   R x, y, z;
 };
 
-template <typename R>
-__device__ __forceinline__ void sincos_t(R x, R* s, R* c);
-template <>
-__device__ __forceinline__ void sincos_t<double>(double x, double* s, double* c) {
-  sincos(x, s, c);
-}
-// FP32 (edge and vertex pairs): the hardware approximation, accurate to a few
-// 1e-7 absolute for the |k r| <= ~1 of touching triangles (the regular kernels
-// use it at larger arguments).
-template <>
-__device__ __forceinline__ void sincos_t<float>(float x, float* s, float* c) {
-  __sincosf(x, s, c);
-}
-
-// 1 / r and r from r^2 (r clamped to kEps as in potential.h): rsqrt in FP32, a
-// correctly rounded sqrt and division in FP64.
-template <typename R>
-__device__ __forceinline__ void inv_dist(R r2, R* r, R* inv_r);
-template <>
-__device__ __forceinline__ void inv_dist<double>(double r2, double* r, double* inv_r) {
-  double rr = sqrt(r2);
-  if (rr < kEps) rr = kEps;
-  *r = rr;
-  *inv_r = 1.0 / rr;
-}
-template <>
-__device__ __forceinline__ void inv_dist<float>(float r2, float* r, float* inv_r) {
-  const float ri = fminf(rsqrtf(r2), 1.0f / kEps);
-  *inv_r = ri;
-  *r = fmaxf(r2 * ri, kEps);
-}
-
 // Re-ordering of the reference (integrand.h:351-387): for a common edge the
 // shared vertices take local slots 0,1 in trial order; for a common vertex it
 // is swapped into slot 0 on both triangles.  Kept in scalar registers (no

@@ -437,20 +437,16 @@ __global__ void __launch_bounds__(kBmThreads, 2)
   }
 }
 
-__device__ __forceinline__ void bm_sincos(double x, double* s, double* c) { sincos(x, s, c); }
-__device__ __forceinline__ void bm_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
-
 // Both Burton-Miller kernels at d = y - x, without the 1/(4 pi):
 // lhs_main = -ik nn G + H d.n_j, aux = (i/k) G, rhs = -G + (i/k) H (-d).n_i.
 template <typename R>
 __device__ __forceinline__ void bm_eval(R dx, R dy, R dz, const R (&ni)[3], const R (&nj)[3], R nn, R k, R kinv,
                                         R& lr, R& li, R& ar, R& ai, R& rr, R& ri) {
-  R r = sqrt(dx * dx + dy * dy + dz * dz);
-  if (r < R(kEps)) r = R(kEps);
-  R s, c;
-  bm_sincos(k * r, &s, &c);
-  const R ir = R(1) / r;
+  R r, ir;
+  inv_dist<R>(dx * dx + dy * dy + dz * dz, &r, &ir);
   const R kr = k * r;
+  R s, c;
+  sincos_t<R>(kr, &s, &c);
   const R gr = c * ir, gi = s * ir;
   const R ir2 = ir * ir;
   const R hr = (c + kr * s) * ir * ir2, hi = (s - kr * c) * ir * ir2;
@@ -464,11 +460,24 @@ __device__ __forceinline__ void bm_eval(R dx, R dy, R dz, const R (&ni)[3], cons
   ri = -gi + hr * dni * kinv;
 }
 
-// One touching pair (index `local` of its type), one warp; the coincident
-// pass also adds 1/2 M to lhs and -(i/(2k)) M to rhs.
+// Lanes per touching pair: the LN^4 Gauss points of the 4-D rule are split
+// over 16 lanes when there are at most 16 of them (two pairs per warp, at
+// the 2-point rule of the <2,3> orders), else over the whole warp.
+template <int LN>
+struct BmSingLanes {
+  static constexpr int kPoints = LN * LN * LN * LN;
+  static constexpr int kW = kPoints <= 16 ? 16 : 32;
+  static constexpr int kPairsPerWarp = 32 / kW;
+};
+
+// One touching pair (index `local` of its type) on W = BmSingLanes<LN>::kW
+// lanes (lane `sub` of them); the coincident pass also adds 1/2 M to lhs and
+// -(i/(2k)) M to rhs.  `store` is false for the idle half of a warp whose
+// last pair is missing (it computes a copy of a valid pair, for the
+// shuffles, and adds nothing).
 template <typename R, int NCOMMON, int LN>
-__device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local) {
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local, int sub, bool store) {
+  constexpr int W = BmSingLanes<LN>::kW;
   const GeomView& g = P.g;
   int ti = local, tj = local;
   if (NCOMMON == 2) {
@@ -512,9 +521,12 @@ __device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local) 
   }
   const R kk = (R)P.k, kinv = R(1) / kk;
   const R nn = ni[0] * nj[0] + ni[1] * nj[1] + ni[2] * nj[2];
-  R accL[18], accR[18], aux[2] = {0, 0};
+  // t[4 e + (0, 1, 2, 3)] = (lhs re, lhs im, rhs re, rhs im) of block entry
+  // e = 3 ii + jj (re-ordered slots), t[36], t[37] = the weight sum of the
+  // curl term's (i/k) G; t[38..63] stay zero (padding for the reduction)
+  R t[64];
 #pragma unroll
-  for (int e = 0; e < 18; e++) accL[e] = accR[e] = 0;
+  for (int e = 0; e < 64; e++) t[e] = 0;
   auto region = [&](R x1, R x2, R y1, R y2, R ww) {
     const R lx[3] = {R(1) - x1, x1 - x2, x2};
     const R ly[3] = {R(1) - y1, y1 - y2, y2};
@@ -531,75 +543,102 @@ __device__ __forceinline__ void singular_bm_pair(const BmProblem& P, int local) 
 #pragma unroll
       for (int jj = 0; jj < 3; jj++) {
         const R f = lx[ii] * ly[jj] * ww;
-        accL[2 * (3 * ii + jj)] += lr * f;
-        accL[2 * (3 * ii + jj) + 1] += li * f;
-        accR[2 * (3 * ii + jj)] += rr * f;
-        accR[2 * (3 * ii + jj) + 1] += ri * f;
+        const int e = 3 * ii + jj;
+        t[4 * e] += lr * f;
+        t[4 * e + 1] += li * f;
+        t[4 * e + 2] += rr * f;
+        t[4 * e + 3] += ri * f;
       }
-    aux[0] += ar * ww;
-    aux[1] += ai * ww;
+    t[36] += ar * ww;
+    t[37] += ai * ww;
   };
   const R jw = Ji * Jj / R(16);
-  constexpr int NPT = LN * LN * LN * LN;
+  constexpr int NPT = BmSingLanes<LN>::kPoints;
 #pragma unroll 1
-  for (int pt = lane; pt < NPT; pt += 32) {
+  for (int pt = sub; pt < NPT; pt += W) {
     const int i0 = pt / (LN * LN * LN), i1 = (pt / (LN * LN)) % LN, i2 = (pt / LN) % LN, i3 = pt % LN;
     const R xi = R(0.5) * (R(gl_x<LN>(i0)) + R(1)), e1 = R(0.5) * (R(gl_x<LN>(i1)) + R(1));
     const R e2 = R(0.5) * (R(gl_x<LN>(i2)) + R(1)), e3 = R(0.5) * (R(gl_x<LN>(i3)) + R(1));
     const R w0 = R(gl_w<LN>(i0)) * R(gl_w<LN>(i1)) * R(gl_w<LN>(i2)) * R(gl_w<LN>(i3)) * jw;
     ss_regions<NCOMMON, R>(xi, e1, e2, e3, w0, region);
   }
+  // transpose-reduce over the W lanes (xor offsets < W stay inside the
+  // pair's lanes): every round halves the values a lane keeps, so lane `sub`
+  // ends with the totals of values (64 / W) sub + i in t[i]
 #pragma unroll
-  for (int e = 0; e < 18; e++) {
+  for (int o = W / 2, half = 32; o >= 1; o >>= 1, half >>= 1) {
+    const bool hi = (sub & o) != 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      accL[e] += __shfl_xor_sync(0xffffffffu, accL[e], o);
-      accR[e] += __shfl_xor_sync(0xffffffffu, accR[e], o);
+    for (int i = 0; i < half; i++) {
+      const R send = hi ? t[i] : t[i + half];
+      const R keep = hi ? t[i + half] : t[i];
+      t[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    aux[0] += __shfl_xor_sync(0xffffffffu, aux[0], o);
-    aux[1] += __shfl_xor_sync(0xffffffffu, aux[1], o);
-  }
-  if (lane < 9) {
-    const int ii = lane / 3, jj = lane % 3;  // re-ordered slots
-    const int ia = pi_[ii], jb = pj_[jj];    // original local vertices
+  // W = 16: lane e (< 9) holds entry e (lhs re, im, rhs re, im), lane 9 the
+  // curl sums; W = 32: lane 2e holds entry e's lhs, lane 2e + 1 its rhs,
+  // lane 18 the curl sums
+  constexpr int kAuxLane = W == 16 ? 9 : 18;
+  const R aux_re = __shfl_sync(0xffffffffu, t[0], kAuxLane, W);
+  const R aux_im = __shfl_sync(0xffffffffu, t[1], kAuxLane, W);
+  const int e = W == 16 ? sub : (sub >> 1);
+  const bool do_lhs = W == 16 ? sub < 9 : (sub < 18 && (sub & 1) == 0);
+  const bool do_rhs = W == 16 ? sub < 9 : (sub < 18 && (sub & 1) == 1);
+  if (!store || !(do_lhs || do_rhs)) return;
+  const int ii = e / 3, jj = e % 3;      // re-ordered slots
+  const int ia = pi_[ii], jb = pj_[jj];  // original local vertices
+  const R sc = R(kInv4Pi);
+  const R m = NCOMMON == 3 ? R(0.5) * Ji * (ia == jb ? R(2) : R(1)) / R(12) : R(0);  // P1 mass: area (1 + [a == b]) / 12
+  const size_t at = (size_t)sel3(s0, s1, s2, ia) * g.nv + sel3(t0, t1, t2, jb);
+  if (do_lhs) {
     R cp = 0;
     for (int d = 0; d < 3; d++) cp += (R)g.curls[9 * ti + 3 * ia + d] * (R)g.curls[9 * tj + 3 * jb + d];
-    R lre = accL[2 * lane] + aux[0] * cp, lim = accL[2 * lane + 1] + aux[1] * cp;
-    R rre = accR[2 * lane], rim = accR[2 * lane + 1];
-    const R sc = R(kInv4Pi);
-    lre *= sc;
-    lim *= sc;
-    rre *= sc;
-    rim *= sc;
-    if (NCOMMON == 3) {  // P1 mass: area (1 + [a == b]) / 12
-      const R m = R(0.5) * Ji * (ia == jb ? R(2) : R(1)) / R(12);
-      lre += R(0.5) * m;
-      rim -= R(0.5) * kinv * m;
-    }
-    const size_t at = (size_t)sel3(s0, s1, s2, ia) * g.nv + sel3(t0, t1, t2, jb);
+    R lre = (t[0] + aux_re * cp) * sc, lim = (t[1] + aux_im * cp) * sc;
+    if (NCOMMON == 3) lre += R(0.5) * m;
     atomicAdd(&P.L[at], make_float2((float)lre, (float)lim));
+  }
+  if (do_rhs) {
+    const int o = W == 16 ? 2 : 0;
+    R rre = t[o] * sc, rim = t[o + 1] * sc;
+    if (NCOMMON == 3) rim -= R(0.5) * kinv * m;
     atomicAdd(&P.R[at], make_float2((float)rre, (float)rim));
   }
 }
 
+// Pair index of this warp's lanes (kPairsPerWarp pairs per warp): `first` is
+// the warp's first pair, `sub` the lane within the pair.
+template <int LN>
+__device__ __forceinline__ long long bm_sing_pair_index(long long* first, int* sub) {
+  constexpr int W = BmSingLanes<LN>::kW, PPW = BmSingLanes<LN>::kPairsPerWarp;
+  const int lane = threadIdx.x & 31;
+  *first = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * PPW;
+  *sub = lane & (W - 1);
+  return *first + lane / W;
+}
+
 template <typename R, int NCOMMON, int LN>
 __global__ void __launch_bounds__(128) singular_bm_kernel(const __grid_constant__ BmProblem P, int npairs) {
-  const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (pair >= npairs) return;
-  singular_bm_pair<R, NCOMMON, LN>(P, pair);
+  long long first;
+  int sub;
+  const long long pair = bm_sing_pair_index<LN>(&first, &sub);
+  if (first >= npairs) return;  // uniform over the warp
+  const bool store = pair < npairs;
+  singular_bm_pair<R, NCOMMON, LN>(P, (int)(store ? pair : first), sub, store);
 }
 
 template <typename R, int NCOMMON, int LN>
 __global__ void __launch_bounds__(128)
     singular_bm_batch_kernel(const BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
   constexpr int which = NCOMMON == 3 ? 0 : (NCOMMON == 2 ? 1 : 2);
-  const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (pair >= hdr->total_pairs[which]) return;
+  long long first;
+  int sub;
+  long long pair = bm_sing_pair_index<LN>(&first, &sub);
+  const long long total = hdr->total_pairs[which];
+  if (first >= total) return;  // uniform over the warp
+  const bool store = pair < total;
+  if (!store) pair = first;
   const BmProblem& P = probs[bm_find(probs, hdr->nproblems, pair, which)];
-  singular_bm_pair<R, NCOMMON, LN>(P, (int)(pair - P.pair_begin[which]));
+  singular_bm_pair<R, NCOMMON, LN>(P, (int)(pair - P.pair_begin[which]), sub, store);
 }
 
 inline size_t al256(size_t x) { return (x + 255) / 256 * 256; }
@@ -684,13 +723,13 @@ void bm_single_launch(const BmProblem& P, long long grid, long long items, cudaS
   if (items > 0)
     (regular_bm_kernel<TN><<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(P, (int)items),
      count_launch());
-  const int wpb = 4;
-  (singular_bm_kernel<double, 3, LN><<<(g.nt + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.nt), count_launch());
+  const int wpb = 4, ppb = wpb * BmSingLanes<LN>::kPairsPerWarp;  // warps, pairs per block
+  (singular_bm_kernel<double, 3, LN><<<(g.nt + ppb - 1) / ppb, 32 * wpb, 0, s>>>(P, g.nt), count_launch());
   if (g.n_edge)
-    (singular_bm_kernel<float, 2, LN><<<(g.n_edge + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_edge),
+    (singular_bm_kernel<float, 2, LN><<<(g.n_edge + ppb - 1) / ppb, 32 * wpb, 0, s>>>(P, g.n_edge),
      count_launch());
   if (g.n_vert)
-    (singular_bm_kernel<float, 1, LN><<<(g.n_vert + wpb - 1) / wpb, 32 * wpb, 0, s>>>(P, g.n_vert),
+    (singular_bm_kernel<float, 1, LN><<<(g.n_vert + ppb - 1) / ppb, 32 * wpb, 0, s>>>(P, g.n_vert),
      count_launch());
 }
 
@@ -700,15 +739,15 @@ void bm_batch_launch(BmHeader* dh, BmProblem* dp, long long grid, long long item
   if (items > 0)
     (regular_bm_batch_kernel<TN><<<(unsigned)(grid < items ? grid : items), kBmThreads, sizeof(BmSmem), s>>>(dh, dp),
      count_launch());
-  const int wpb = 4;
+  const int wpb = 4, ppb = wpb * BmSingLanes<LN>::kPairsPerWarp;  // warps, pairs per block
   if (pairs[0])
-    (singular_bm_batch_kernel<double, 3, LN><<<(unsigned)((pairs[0] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+    (singular_bm_batch_kernel<double, 3, LN><<<(unsigned)((pairs[0] + ppb - 1) / ppb), 32 * wpb, 0, s>>>(dh, dp),
      count_launch());
   if (pairs[1])
-    (singular_bm_batch_kernel<float, 2, LN><<<(unsigned)((pairs[1] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+    (singular_bm_batch_kernel<float, 2, LN><<<(unsigned)((pairs[1] + ppb - 1) / ppb), 32 * wpb, 0, s>>>(dh, dp),
      count_launch());
   if (pairs[2])
-    (singular_bm_batch_kernel<float, 1, LN><<<(unsigned)((pairs[2] + wpb - 1) / wpb), 32 * wpb, 0, s>>>(dh, dp),
+    (singular_bm_batch_kernel<float, 1, LN><<<(unsigned)((pairs[2] + ppb - 1) / ppb), 32 * wpb, 0, s>>>(dh, dp),
      count_launch());
 }
 
