@@ -52,6 +52,8 @@ int tc_b_planes(void* ws, int n, int m, int precision, __nv_bfloat16** bh, __nv_
                 float** cinv);
 int encode_map_2d_f32(CUtensorMap* map, const void* ptr, unsigned long long cols, unsigned long long rows,
                       unsigned long long ld_bytes, unsigned box_cols, unsigned box_rows);
+int encode_map_2d_f32_sw128(CUtensorMap* map, const void* ptr, unsigned long long cols, unsigned long long rows,
+                            unsigned long long ld_bytes, unsigned box_cols, unsigned box_rows);
 int tc_gemm(const void* ws, int n, int precision, int m, float2* Y, const int* active, cudaStream_t s);
 
 namespace {
@@ -293,13 +295,168 @@ __global__ void __launch_bounds__(256) resid_finish_kernel(const float2* __restr
   if (threadIdx.x == 0) atomicAdd(&norm2[s], red[0]);
 }
 
+// ---------------------------------------------------------------------------
+// resid_tma_kernel: the same R = A X (FP64 products and sums) with the
+// matrix streamed through shared memory, so that the rows are read from HBM
+// coalesced instead of one 128-byte line per lane.  A producer warp loads
+// 256-row x 16-column tiles of A (2-D tensor map over the matrix as FP32
+// pairs, 128-byte swizzle, no multicast; rows and columns past n arrive
+// zero-filled) into a ring of kRtStages stages; compute threads t and
+// t + 256 own row r0 + t, each for 4 of the 8 right-hand sides (16 compute
+// warps to cover the FP64 and shared-memory latencies), and read the row's
+// 128-byte slice as 8 float4 chunks (chunk k at k ^ (t & 7): the 32 lanes of
+// a warp read 512 bytes in 4 wavefronts); the item's X columns are staged
+// once in shared memory and read as broadcasts.
+// Items (256-row block, group of cb columns, 8 right-hand sides) are taken
+// from blockIdx.x on, gridDim.x apart; every wait is bounded (err).
+// ---------------------------------------------------------------------------
+inline int device_sms() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+constexpr int kRtRows = 256;                                            // rows per item
+constexpr int kRtSplit = 1;                                             // compute threads per row
+constexpr int kRtRhs = kRsRhs / kRtSplit;                               // right-hand sides per thread
+constexpr int kRtThreads = kRtSplit * kRtRows + 32;                     // + the producer warp
+constexpr int kRtTileCols = 16;                                         // complex columns per stage: 128 B per row
+constexpr int kRtStages = 4;
+constexpr size_t kRtStageBytes = sizeof(float2) * kRtRows * kRtTileCols;  // 32 KB
+constexpr int kRtMaxCols = 640;                                         // columns per item (multiple of 16)
+constexpr size_t kRtXBytes = sizeof(double2) * kRtMaxCols * kRsRhs;     // 80 KB
+constexpr size_t kRtSmem = kRtStageBytes * kRtStages + kRtXBytes + 2 * kRtStages * sizeof(uint64_t);
+
+__global__ void __launch_bounds__(kRtThreads, 1)
+    resid_tma_kernel(const __grid_constant__ CUtensorMap amap, int n, const double2* __restrict__ X, int m,
+                     double2* __restrict__ R, int cb, int n_cg, int n_items, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char rt_raw[];
+  const float4* ring = reinterpret_cast<const float4*>(rt_raw);                     // [stage][row][8 chunks]
+  double2* xs = reinterpret_cast<double2*>(rt_raw + kRtStageBytes * kRtStages);       // [column][rhs]
+  uint64_t* full = reinterpret_cast<uint64_t*>(rt_raw + kRtStageBytes * kRtStages + kRtXBytes);
+  uint64_t* empty = full + kRtStages;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int kComputeWarps = kRtSplit * kRtRows / 32;
+  if ((smem_u32(rt_raw) & 1023u) != 0u) {  // the swizzled tiles need 1024-byte alignment (uniform)
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  if (tid == 0) {
+    for (int st = 0; st < kRtStages; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kComputeWarps);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const int n_rb = (n + kRtRows - 1) / kRtRows;
+  unsigned g = 0;  // ring stages used so far (producer and consumers count alike)
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int sg = item / (n_rb * n_cg);
+    const int rem = item - sg * n_rb * n_cg;
+    const int cg = rem / n_rb, rb = rem - cg * n_rb;
+    const int r0 = rb * kRtRows, c0 = cg * cb;
+    const int cn = min(cb, n - c0);
+    const int s0 = sg * kRsRhs, ms = min(kRsRhs, m - s0);
+    const int ntiles = (cn + kRtTileCols - 1) / kRtTileCols;
+    __syncthreads();  // the previous item's readers are done with xs
+    for (int e = tid; e < ntiles * kRtTileCols * kRsRhs; e += kRtThreads) {
+      const int c = e / kRsRhs, sl = e - c * kRsRhs;
+      xs[e] = (c < cn && sl < ms) ? X[(size_t)(c0 + c) * m + s0 + sl] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (warp == kComputeWarps) {  // producer
+      if (lane == 0) {
+        const uint64_t pol = l2_evict_first_policy();
+        for (int t = 0; t < ntiles; t++) {
+          const unsigned gi = g + t;
+          const int st = (int)(gi % kRtStages);
+          if (gi >= kRtStages && !mbar_wait(&empty[st], (gi / kRtStages - 1u) & 1u, err)) break;
+          mbar_expect_tx(&full[st], (uint32_t)kRtStageBytes);
+          tma_load_2d_hint(rt_raw + (size_t)st * kRtStageBytes, &amap, 2 * (c0 + t * kRtTileCols), r0, &full[st],
+                           pol);
+        }
+      }
+    } else {
+      const int rl = tid % kRtRows, sh = (tid / kRtRows) * kRtRhs;  // row in the item, first right-hand side
+      const int row = r0 + rl;
+      double acc[kRtRhs][2];
+#pragma unroll
+      for (int sl = 0; sl < kRtRhs; sl++) acc[sl][0] = acc[sl][1] = 0.0;
+      for (int t = 0; t < ntiles; t++) {
+        const unsigned gi = g + t;
+        const int st = (int)(gi % kRtStages);
+        mbar_wait(&full[st], (gi / kRtStages) & 1u, err);
+        if (row < n) {
+          const float4* rp = ring + ((size_t)st * kRtRows + rl) * 8;
+          const double2* xt = xs + (size_t)t * kRtTileCols * kRsRhs + sh;
+#pragma unroll 4
+          for (int k = 0; k < 8; k++) {
+            const float4 v = rp[k ^ (rl & 7)];  // columns 2k, 2k + 1 of the tile
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const double ar = h ? v.z : v.x, ai = h ? v.w : v.y;
+              const double2* xc = xt + (size_t)(2 * k + h) * kRsRhs;
+#pragma unroll
+              for (int sl = 0; sl < kRtRhs; sl++) {
+                const double2 x = xc[sl];
+                acc[sl][0] = fma(ar, x.x, fma(-ai, x.y, acc[sl][0]));
+                acc[sl][1] = fma(ar, x.y, fma(ai, x.x, acc[sl][1]));
+              }
+            }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[st]);
+      }
+      if (row < n) {
+#pragma unroll
+        for (int sl = 0; sl < kRtRhs; sl++) {
+          if (sh + sl < ms) {
+            double* r = reinterpret_cast<double*>(R + (size_t)row * m + s0 + sh + sl);
+            atomicAdd(r, acc[sl][0]);
+            atomicAdd(r + 1, acc[sl][1]);
+          }
+        }
+      }
+    }
+    g += (unsigned)ntiles;
+  }
+  // every issued copy has landed before the CTA exits (a wait above may have
+  // given up after an error): the last use of each slot
+  __syncthreads();
+  if (tid == 0)
+    for (int st = 0; st < kRtStages; st++)
+      if (g > (unsigned)st) mbar_wait_drain(&full[st], ((g - 1u - (unsigned)st) / kRtStages) & 1u);
+}
+
 // R = B - A X, norm2[s] += |R[:, s]|^2 (X, R: n x m row-major complex128; B: complex64).
+// err (device int, raised when a bounded wait expires) selects the streamed
+// kernel for n even and a 16-byte aligned A; else the row-per-thread kernel.
 int launch_resid_f64(const float2* A, int n, const double2* X, int m, double2* R, const float2* B, double* norm2,
-                     cudaStream_t s) {
+                     cudaStream_t s, int* err = nullptr) {
   if (n & 1) return launch_cmatmul<double, 1>(A, n, X, m, m, R, m, B, m, norm2, nullptr, s);
   BEM_CUDA_TRY(cudaMemsetAsync(R, 0, sizeof(double2) * (size_t)n * m, s));
-  const dim3 grid((n + kRsThreads - 1) / kRsThreads, (n + kRsCols - 1) / kRsCols, (m + kRsRhs - 1) / kRsRhs);
-  (resid_f64_kernel<<<grid, kRsThreads, 0, s>>>(A, n, X, m, R), count_launch());
+  if (err && ((uintptr_t)A & 15) == 0) {
+    static std::atomic<bool> attr{false};
+    if (!attr.load(std::memory_order_acquire)) {
+      BEM_CUDA_TRY(cudaFuncSetAttribute(resid_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem));
+      attr.store(true, std::memory_order_release);
+    }
+    CUtensorMap map;
+    int rc = encode_map_2d_f32_sw128(&map, A, 2ull * n, (unsigned long long)n, 8ull * n, 2 * kRtTileCols, kRtRows);
+    if (rc) return rc;
+    const int n_cg = (n + kRtMaxCols - 1) / kRtMaxCols;
+    const int cb = ((n + n_cg - 1) / n_cg + kRtTileCols - 1) / kRtTileCols * kRtTileCols;
+    const long long n_items = (long long)((n + kRtRows - 1) / kRtRows) * n_cg * ((m + kRsRhs - 1) / kRsRhs);
+    const int grid = (int)std::min<long long>(n_items, device_sms());
+    (resid_tma_kernel<<<grid, kRtThreads, kRtSmem, s>>>(map, n, X, m, R, cb, n_cg, (int)n_items, err),
+     count_launch());
+  } else {
+    const dim3 grid((n + kRsThreads - 1) / kRsThreads, (n + kRsCols - 1) / kRsCols, (m + kRsRhs - 1) / kRsRhs);
+    (resid_f64_kernel<<<grid, kRsThreads, 0, s>>>(A, n, X, m, R), count_launch());
+  }
   BEM_CUDA_TRY(cudaGetLastError());
   (resid_finish_kernel<<<dim3(std::min(148, (n + 255) / 256), m), 256, 0, s>>>(B, n, m, R, norm2), count_launch());
   BEM_CUDA_TRY(cudaGetLastError());
@@ -534,13 +691,6 @@ __global__ void __launch_bounds__(kGtThreads, 1)
     }
     cgemv_flush<MR>(acc, lane, r_begin + b * kGtBlockRows + warp * kGvRows, r_end, s0, m, Y);
   }
-}
-
-inline int device_sms() {
-  int dev = 0, n = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-  return n > 0 ? n : 1;
 }
 
 template <int MR>
@@ -3384,7 +3534,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
     // outer FP64 residual r = b - A x against the FP32 matrix
     BEM_CUDA_TRY(cudaMemsetAsync(rnorm2, 0, sizeof(double) * m, s));
     if (x_nonzero) {
-      rc = launch_resid_f64((const float2*)A, n, P.x, m, P.r, (const float2*)B, rnorm2, s);
+      rc = launch_resid_f64((const float2*)A, n, P.x, m, P.r, (const float2*)B, rnorm2, s, &P.st->err);
       if (rc) return rc;
       matvecs++;
     } else {

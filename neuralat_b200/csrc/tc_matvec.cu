@@ -574,6 +574,24 @@ int encode_map_2d_f32(CUtensorMap* map, const void* ptr, unsigned long long cols
   return r == CUDA_SUCCESS ? BEM_OK : BEM_ERR_CUDA;
 }
 
+// Same with the 128-byte swizzle (box_cols * 4 bytes must be 128): 16-byte
+// chunk k of box row r lands at chunk k ^ (r & 7) of its 128-byte row, so
+// lanes that read one chunk each of consecutive rows hit distinct banks.
+int encode_map_2d_f32_sw128(CUtensorMap* map, const void* ptr, unsigned long long cols, unsigned long long rows,
+                            unsigned long long ld_bytes, unsigned box_cols, unsigned box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return BEM_ERR_CUDA;
+  if (((uintptr_t)ptr & 15) || (ld_bytes & 15) || box_cols * 4 != 128) return BEM_ERR_INVALID_ARGUMENT;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? BEM_OK : BEM_ERR_CUDA;
+}
+
 namespace {
 
 // Workspace: [header: error flag][column maxima (m)][cinv (m)][rinv (n)]
