@@ -30,8 +30,8 @@
 // double-buffered in shared memory by bulk copies, each warp taking two trial
 // triangles (one per half-warp); the 3x3 blocks go to corner slabs that are
 // reduced on chip onto the tiles' distinct vertices, four vector atomics per
-// entry.  The slabs are small enough for two CTAs per SM, so one CTA's
-// reduction and barriers overlap the other's evaluation.
+// entry.  The slabs are small enough for three CTAs per SM, so one CTA's
+// reduction and barriers overlap the others' evaluation.
 // Touching pairs: one warp per pair evaluates both kernels at each
 // Sauter-Schwab point (shared r and sincos); the coincident pass (FP64) adds
 // the mass terms.  A batch (meshes, wavenumbers) uses the same kernels with a
@@ -397,10 +397,16 @@ __device__ __forceinline__ void bm_init_barriers(BmSmem& sm) {
   }
 }
 
+// CTAs per SM of the regular kernels: three at the 1- and 3-point rules
+// (80 registers, the slabs of three CTAs fit in shared memory: the barriers
+// and the on-chip reduction of one CTA overlap two others' evaluation), two at
+// the 6-point rule (whose accumulators would spill at 80 registers).
+__host__ __device__ constexpr int bm_min_ctas(int tn) { return tn == 6 ? 2 : 3; }
+
 // Regular pairs of one problem: equal work items dealt round-robin to a
 // persistent grid.
 template <int TN>
-__global__ void __launch_bounds__(kBmThreads, 2)
+__global__ void __launch_bounds__(kBmThreads, bm_min_ctas(TN))
     regular_bm_kernel(const __grid_constant__ BmProblem P, int n_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BmSmem& sm = *reinterpret_cast<BmSmem*>(smem_raw);
@@ -415,7 +421,7 @@ __global__ void __launch_bounds__(kBmThreads, 2)
 
 // Regular pairs of a batch: CTAs drain one queue of work items.
 template <int TN>
-__global__ void __launch_bounds__(kBmThreads, 2)
+__global__ void __launch_bounds__(kBmThreads, bm_min_ctas(TN))
     regular_bm_batch_kernel(BmHeader* __restrict__ hdr, const BmProblem* __restrict__ probs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BmSmem& sm = *reinterpret_cast<BmSmem*>(smem_raw);
