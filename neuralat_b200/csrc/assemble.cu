@@ -362,7 +362,11 @@ __device__ __forceinline__ void pair_block_sym(const float (*xs)[kSymTest], int 
   for (int p = 0; p < 6; p++) {
     const float px = xs[3 * p][tl], py = xs[3 * p + 1][tl], pz = xs[3 * p + 2][tl];
     const float dn = njx * (cjx - px) + njy * (cjy - py) + njz * (cjz - pz);
+    // the rule is symmetric: phi_b(q) = a_q + (1 - 3 a_q) [b = own vertex of
+    // q], so each point adds its own-vertex excess to one trial sum and its
+    // common weight to c*, which all three sums receive at the end
     float2 tV[3], tK[3], uK[3];
+    float2 cV = make_float2(0.f, 0.f), cK = cV, cU = cV;
 #pragma unroll
     for (int b = 0; b < 3; b++) {
       tV[b] = make_float2(0.f, 0.f);
@@ -389,14 +393,21 @@ __device__ __forceinline__ void pair_block_sym(const float (*xs)[kSymTest], int 
         const float2 gv = f2_mul(make_float2(sc[j][1], sc[j][0]), f2(ri));                  // (c, s) / r
         const float2 gk = f2_mul(f2_fma(kk, make_float2(sc[j][0], sc[j][1]), gv), f2(ri2));  // (c + kr s, s - kr c) / r^3
         const float2 mk = f2_mul(f2(dq[q]), gk);
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-          const float2 w = f2((float)(tri6_w(q) * tri6_phi(q, b)));
-          tV[b] = f2_fma(w, gv, tV[b]);
-          tK[b] = f2_fma(w, gk, tK[b]);
-          uK[b] = f2_fma(w, mk, uK[b]);
-        }
+        const int b = tri6_own(q);
+        const float2 wo = f2((float)tri6_w_own(q)), wc = f2((float)tri6_w_common(q));
+        tV[b] = f2_fma(wo, gv, tV[b]);
+        tK[b] = f2_fma(wo, gk, tK[b]);
+        uK[b] = f2_fma(wo, mk, uK[b]);
+        cV = f2_fma(wc, gv, cV);
+        cK = f2_fma(wc, gk, cK);
+        cU = f2_fma(wc, mk, cU);
       }
+    }
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      tV[b] = f2_fma(f2(1.f), cV, tV[b]);
+      tK[b] = f2_fma(f2(1.f), cK, tK[b]);
+      uK[b] = f2_fma(f2(1.f), cU, uK[b]);
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {

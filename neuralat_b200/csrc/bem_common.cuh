@@ -24,6 +24,10 @@ __host__ __device__ constexpr double tri6_phi(int q, int b) {
   return (q < 3) ? ((q == b) ? 1.0 - 2.0 * kTriA1 : kTriA1) : ((q - 3 == b) ? 1.0 - 2.0 * kTriA2 : kTriA2);
 }
 __host__ __device__ constexpr double tri6_w(int q) { return q < 3 ? kTriW1 : kTriW2; }
+// The rule is symmetric: w_q phi_b(q) = tri6_w_common(q) + tri6_w_own(q) [b == tri6_own(q)].
+__host__ __device__ constexpr int tri6_own(int q) { return q < 3 ? q : q - 3; }
+__host__ __device__ constexpr double tri6_w_common(int q) { return tri6_w(q) * (q < 3 ? kTriA1 : kTriA2); }
+__host__ __device__ constexpr double tri6_w_own(int q) { return tri6_w(q) * (1.0 - 3.0 * (q < 3 ? kTriA1 : kTriA2)); }
 
 // Gauss-Legendre 4-point rule on [-1, 1] (gauss.h:44-54).
 constexpr double kGL4x0 = 0.86113631159405258, kGL4x1 = 0.33998104358485626;
