@@ -2901,95 +2901,148 @@ int block_host(int group, int p, int nb, BlockHost** out) {
   return BEM_OK;
 }
 
+// Reflection of rows r .. r + p of the columns [t0, t1) of a row-major
+// [row][p] (re, im) pair of arrays: y -= f u (u^H y).  The loops run over the
+// columns, contiguous in memory, so that they vectorise; the body is stamped
+// twice, for x86-64 CPUs with AVX2 and FMA and for any other.
+#define BK_REFLECT_BODY                                         \
+  double dr[kBkMaxP], di[kBkMaxP];                              \
+  for (int t = t0; t < t1; t++) dr[t] = di[t] = 0.0;            \
+  for (int e = 0; e <= p; e++) {                                \
+    const double a = ur[e], b = ui[e];                          \
+    const double* xr = yr + (size_t)e * p;                      \
+    const double* xi = yi + (size_t)e * p;                      \
+    _Pragma("GCC ivdep") for (int t = t0; t < t1; t++) {        \
+      dr[t] += a * xr[t] + b * xi[t];                           \
+      di[t] += a * xi[t] - b * xr[t];                           \
+    }                                                           \
+  }                                                             \
+  for (int t = t0; t < t1; t++) {                               \
+    dr[t] *= f;                                                 \
+    di[t] *= f;                                                 \
+  }                                                             \
+  for (int e = 0; e <= p; e++) {                                \
+    const double a = ur[e], b = ui[e];                          \
+    double* xr = yr + (size_t)e * p;                            \
+    double* xi = yi + (size_t)e * p;                            \
+    _Pragma("GCC ivdep") for (int t = t0; t < t1; t++) {        \
+      xr[t] -= a * dr[t] - b * di[t];                           \
+      xi[t] -= a * di[t] + b * dr[t];                           \
+    }                                                           \
+  }
+
+__attribute__((target("avx2,fma"))) void bk_reflect_avx2(const double* __restrict ur, const double* __restrict ui,
+                                                          double f, int p, int t0, int t1, double* __restrict yr,
+                                                          double* __restrict yi) {
+  BK_REFLECT_BODY
+}
+void bk_reflect_generic(const double* __restrict ur, const double* __restrict ui, double f, int p, int t0, int t1,
+                        double* __restrict yr, double* __restrict yi) {
+  BK_REFLECT_BODY
+}
+#undef BK_REFLECT_BODY
+typedef void (*BkReflectFn)(const double*, const double*, double, int, int, int, double*, double*);
+BkReflectFn bk_reflect() {
+  static const BkReflectFn fn =
+      (__builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma")) ? bk_reflect_avx2 : bk_reflect_generic;
+  return fn;
+}
+
 // The block least-squares problem min || E1 R_0 - H_k Y || of block GMRES,
 // solved incrementally on the host: Householder reflections triangularise
 // the block Hessenberg matrix one block column at a time (column c has
 // nonzeros down to row c + p, so each reflection acts on p + 1 rows) and are
 // applied to the right-hand side Z = E1 R_0; the residual of right-hand side
 // b is the norm of Z's rows (k+1)p .. (k+2)p-1 below the triangle.
+// Each new block column is reflected by every earlier reflection across all
+// its p columns at once (row-major [row][column] working copy, vectorised).
 struct BlockLS {
-  // complex values as (re, im) pairs with explicit arithmetic (no library
-  // complex multiply: its IEEE special-value handling makes it many times slower)
-  struct C {
-    double x, y;
-  };
-  static C mul(C a, C b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
-  static C cmulc(C a, C b) { return {a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x}; }  // conj(a) b
   int p = 0, ld = 0, ncols = 0;
-  std::vector<C> T, Z, U;   // T: ld x (nb p), Z: ld x p (column-major); U: reflections (p + 1 each)
-  std::vector<double> fac;  // 2 / (u^H u) of each reflection (0: identity)
+  std::vector<double> Tre, Tim;  // triangular factor, column-major: [column][row], ld rows
+  std::vector<double> Zre, Zim;  // rotated right-hand side, row-major: [row][p]
+  std::vector<double> Ure, Uim;  // reflections, p + 1 entries each
+  std::vector<double> fac;       // 2 / (u^H u) of each reflection (0: identity)
+  std::vector<double> Xre, Xim;  // the new block column, row-major: [row][p]
+  BkReflectFn refl = nullptr;
   void init(int p_, int nb, const double2* R0) {
     p = p_;
     ld = (nb + 1) * p;
     ncols = 0;
-    T.assign((size_t)ld * nb * p, C{0.0, 0.0});
-    Z.assign((size_t)ld * p, C{0.0, 0.0});
-    U.assign((size_t)nb * p * (p + 1), C{0.0, 0.0});
+    refl = bk_reflect();
+    Tre.assign((size_t)ld * nb * p, 0.0);
+    Tim.assign((size_t)ld * nb * p, 0.0);
+    Zre.assign((size_t)ld * p, 0.0);
+    Zim.assign((size_t)ld * p, 0.0);
+    Ure.assign((size_t)nb * p * (p + 1), 0.0);
+    Uim.assign((size_t)nb * p * (p + 1), 0.0);
     fac.assign((size_t)nb * p, 0.0);
+    Xre.assign((size_t)ld * p, 0.0);
+    Xim.assign((size_t)ld * p, 0.0);
     for (int c = 0; c < p; c++)
-      for (int b = 0; b < p; b++) Z[(size_t)b * ld + c] = C{R0[c * p + b].x, R0[c * p + b].y};
-  }
-  // y[r .. r+p] -= fac_r u_r (u_r^H y[r .. r+p])
-  void reflect(int r, C* y) const {
-    const C* u = &U[(size_t)r * (p + 1)];
-    C d{0.0, 0.0};
-    for (int e = 0; e <= p; e++) {
-      const C t = cmulc(u[e], y[r + e]);
-      d.x += t.x;
-      d.y += t.y;
-    }
-    d.x *= fac[r];
-    d.y *= fac[r];
-    for (int e = 0; e <= p; e++) {
-      const C t = mul(u[e], d);
-      y[r + e].x -= t.x;
-      y[r + e].y -= t.y;
-    }
+      for (int b = 0; b < p; b++) {
+        Zre[(size_t)c * p + b] = R0[c * p + b].x;
+        Zim[(size_t)c * p + b] = R0[c * p + b].y;
+      }
   }
   // block column j: hj[a][b], rows a < (j + 2) p; residual estimate per right-hand side.
   // Returns false if the triangular factor is singular (a lost direction).
   bool add(int j, const double2* hj, double* resid) {
-    const int c0 = j * p;
-    for (int t = 0; t < p; t++) {
-      C* x = &T[(size_t)(c0 + t) * ld];
-      for (int a = 0; a < (j + 2) * p; a++) x[a] = C{hj[a * p + t].x, hj[a * p + t].y};
-      for (int a = (j + 2) * p; a < ld; a++) x[a] = C{0.0, 0.0};
-    }
-    // the reflections of the earlier block columns: each one to all p new
-    // columns while it is in cache
+    const int c0 = j * p, nrow = (j + 2) * p;
+    for (int a = 0; a < nrow; a++)
+      for (int t = 0; t < p; t++) {
+        Xre[(size_t)a * p + t] = hj[a * p + t].x;
+        Xim[(size_t)a * p + t] = hj[a * p + t].y;
+      }
+    // the reflections of the earlier block columns, each to all p new columns
     for (int r = 0; r < c0; r++)
       if (fac[r] != 0.0)
-        for (int t = 0; t < p; t++) reflect(r, &T[(size_t)(c0 + t) * ld]);
+        refl(&Ure[(size_t)r * (p + 1)], &Uim[(size_t)r * (p + 1)], fac[r], p, 0, p, &Xre[(size_t)r * p],
+             &Xim[(size_t)r * p]);
     for (int t = 0; t < p; t++) {
-      const int cc = c0 + t;
-      C* x = &T[(size_t)cc * ld];
-      for (int r = c0; r < cc; r++)
-        if (fac[r] != 0.0) reflect(r, x);
-      // reflection for rows cc .. cc + p of column cc
+      const int cc = c0 + t;  // reflection for rows cc .. cc + p of column cc
       double nrm2 = 0.0;
-      for (int e = 0; e <= p; e++) nrm2 += x[cc + e].x * x[cc + e].x + x[cc + e].y * x[cc + e].y;
+      for (int e = 0; e <= p; e++) {
+        const double xr = Xre[(size_t)(cc + e) * p + t], xi = Xim[(size_t)(cc + e) * p + t];
+        nrm2 += xr * xr + xi * xi;
+      }
       const double nrm = std::sqrt(nrm2);
       if (!(nrm > 0.0)) return false;
-      const C alpha = x[cc];
-      const double aa = std::sqrt(alpha.x * alpha.x + alpha.y * alpha.y);
-      const C ph = aa > 0.0 ? C{alpha.x / aa, alpha.y / aa} : C{1.0, 0.0};
-      C* u = &U[(size_t)cc * (p + 1)];
-      for (int e = 0; e <= p; e++) u[e] = x[cc + e];
-      u[0].x += ph.x * nrm;
-      u[0].y += ph.y * nrm;
+      const double ax = Xre[(size_t)cc * p + t], ay = Xim[(size_t)cc * p + t];
+      const double aa = std::sqrt(ax * ax + ay * ay);
+      const double phx = aa > 0.0 ? ax / aa : 1.0, phy = aa > 0.0 ? ay / aa : 0.0;
+      double* ur = &Ure[(size_t)cc * (p + 1)];
+      double* ui = &Uim[(size_t)cc * (p + 1)];
+      for (int e = 0; e <= p; e++) {
+        ur[e] = Xre[(size_t)(cc + e) * p + t];
+        ui[e] = Xim[(size_t)(cc + e) * p + t];
+      }
+      ur[0] += phx * nrm;
+      ui[0] += phy * nrm;
       double uu = 0.0;
-      for (int e = 0; e <= p; e++) uu += u[e].x * u[e].x + u[e].y * u[e].y;
+      for (int e = 0; e <= p; e++) uu += ur[e] * ur[e] + ui[e] * ui[e];
       fac[cc] = uu > 0.0 ? 2.0 / uu : 0.0;
-      x[cc] = C{-ph.x * nrm, -ph.y * nrm};
-      for (int e = 1; e <= p; e++) x[cc + e] = C{0.0, 0.0};
-      for (int b = 0; b < p; b++) reflect(cc, &Z[(size_t)b * ld]);
+      Xre[(size_t)cc * p + t] = -phx * nrm;
+      Xim[(size_t)cc * p + t] = -phy * nrm;
+      for (int e = 1; e <= p; e++) {
+        Xre[(size_t)(cc + e) * p + t] = 0.0;
+        Xim[(size_t)(cc + e) * p + t] = 0.0;
+      }
+      if (fac[cc] != 0.0) {  // the block's later columns and Z
+        if (t + 1 < p) refl(ur, ui, fac[cc], p, t + 1, p, &Xre[(size_t)cc * p], &Xim[(size_t)cc * p]);
+        refl(ur, ui, fac[cc], p, 0, p, &Zre[(size_t)cc * p], &Zim[(size_t)cc * p]);
+      }
     }
+    for (int t = 0; t < p; t++)
+      for (int a = 0; a < nrow; a++) {
+        Tre[(size_t)(c0 + t) * ld + a] = Xre[(size_t)a * p + t];
+        Tim[(size_t)(c0 + t) * ld + a] = Xim[(size_t)a * p + t];
+      }
     ncols = c0 + p;
     for (int b = 0; b < p; b++) {
       double r2 = 0.0;
       for (int a = (j + 1) * p; a < (j + 2) * p; a++) {
-        const C z = Z[(size_t)b * ld + a];
-        r2 += z.x * z.x + z.y * z.y;
+        const double zr = Zre[(size_t)a * p + b], zi = Zim[(size_t)a * p + b];
+        r2 += zr * zr + zi * zi;
       }
       resid[b] = std::sqrt(r2);
     }
@@ -2999,21 +3052,26 @@ struct BlockLS {
   void solve(int kk, std::vector<double2>& Y) const {
     const int nc = kk * p;
     Y.assign((size_t)nc * p, make_double2(0.0, 0.0));
-    std::vector<C> y(nc);
+    std::vector<double> yr(nc), yi(nc);
     for (int b = 0; b < p; b++) {
-      for (int a = 0; a < nc; a++) y[a] = Z[(size_t)b * ld + a];
+      for (int a = 0; a < nc; a++) {
+        yr[a] = Zre[(size_t)a * p + b];
+        yi[a] = Zim[(size_t)a * p + b];
+      }
       for (int c = nc - 1; c >= 0; c--) {
-        const C d = T[(size_t)c * ld + c];
-        const double dd = d.x * d.x + d.y * d.y;
-        const C v = {(y[c].x * d.x + y[c].y * d.y) / dd, (y[c].y * d.x - y[c].x * d.y) / dd};
-        y[c] = v;
-        const C* col = &T[(size_t)c * ld];
+        const double dx = Tre[(size_t)c * ld + c], dy = Tim[(size_t)c * ld + c];
+        const double dd = dx * dx + dy * dy;
+        const double vx = (yr[c] * dx + yi[c] * dy) / dd, vy = (yi[c] * dx - yr[c] * dy) / dd;
+        yr[c] = vx;
+        yi[c] = vy;
+        const double* cr = &Tre[(size_t)c * ld];
+        const double* ci = &Tim[(size_t)c * ld];
         for (int a = 0; a < c; a++) {
-          y[a].x -= col[a].x * v.x - col[a].y * v.y;
-          y[a].y -= col[a].x * v.y + col[a].y * v.x;
+          yr[a] -= cr[a] * vx - ci[a] * vy;
+          yi[a] -= cr[a] * vy + ci[a] * vx;
         }
       }
-      for (int a = 0; a < nc; a++) Y[(size_t)a * p + b] = make_double2(y[a].x, y[a].y);
+      for (int a = 0; a < nc; a++) Y[(size_t)a * p + b] = make_double2(yr[a], yi[a]);
     }
   }
 };
