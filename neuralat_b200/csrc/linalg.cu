@@ -2559,18 +2559,71 @@ __global__ void __launch_bounds__(kBkThreads, 1) gm_block_kernel(GmPtrs P, BkPtr
 }
 
 // D(:, s) += sum_{a < na} Q_a Y[a][s] for the block solution of the cycle.
-__global__ void gm_block_xupdate_kernel(GmPtrs P, BkPtrs K, int na) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y;  // column of the group
-  if (i >= P.n || s >= K.p) return;
-  double2 acc = P.d[(size_t)(K.col0 + s) * P.n + i];
-  for (int a = 0; a < na; a++) {
-    const float2 v = P.Vb[(size_t)(K.vbase + a) * P.ldv + i];
-    const double2 t = cmul(make_double2(v.x, v.y), K.Yb[(size_t)a * K.p + s]);
-    acc.x += t.x;
-    acc.y += t.y;
+// Thread = unknown i, all PP (>= p) columns of the group, so every basis
+// element is read once; blockIdx.y takes one of gridDim.y slices of the basis
+// vectors (the slices meet in D by FP64 atomics); Y staged in shared memory
+// chunk by chunk, the basis loads unrolled so that several are in flight.
+constexpr int kXuThreads = 128;
+constexpr int kXuChunk = 64;  // basis vectors per shared-memory chunk of Y
+template <int PP>
+__global__ void __launch_bounds__(kXuThreads) gm_block_xupdate_kernel(GmPtrs P, BkPtrs K, int na) {
+  __shared__ double2 ys[kXuChunk][PP];
+  const int i = blockIdx.x * kXuThreads + threadIdx.x;
+  const int p = K.p;
+  const int per = (na + gridDim.y - 1) / gridDim.y;
+  const int a_begin = blockIdx.y * per, a_end = min(na, a_begin + per);
+  double2 acc[PP];
+#pragma unroll
+  for (int c = 0; c < PP; c++) acc[c] = make_double2(0.0, 0.0);
+  for (int a0 = a_begin; a0 < a_end; a0 += kXuChunk) {
+    const int nc = min(kXuChunk, a_end - a0);
+    __syncthreads();  // the previous chunk's readers are done
+    for (int e = threadIdx.x; e < kXuChunk * PP; e += kXuThreads) {
+      const int a = e / PP, c = e - a * PP;
+      ys[a][c] = (a < nc && c < p) ? K.Yb[(size_t)(a0 + a) * p + c] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (i < P.n) {
+      const float2* q = P.Vb + (size_t)(K.vbase + a0) * P.ldv + i;
+#pragma unroll 8
+      for (int a = 0; a < nc; a++) {
+        const float2 v = q[(size_t)a * P.ldv];
+        const double vx = v.x, vy = v.y;
+#pragma unroll
+        for (int c = 0; c < PP; c++) {
+          const double2 y = ys[a][c];
+          acc[c].x = fma(vx, y.x, fma(-vy, y.y, acc[c].x));
+          acc[c].y = fma(vx, y.y, fma(vy, y.x, acc[c].y));
+        }
+      }
+    }
   }
-  P.d[(size_t)(K.col0 + s) * P.n + i] = acc;
+  if (i < P.n && a_begin < a_end) {
+#pragma unroll
+    for (int c = 0; c < PP; c++)
+      if (c < p) {
+        double* d = reinterpret_cast<double*>(P.d + (size_t)(K.col0 + c) * P.n + i);
+        atomicAdd(d, acc[c].x);
+        atomicAdd(d + 1, acc[c].y);
+      }
+  }
+}
+
+// D(:, col0 + c) += sum_{a < na} Q_a Y[a][c] for the p columns of group K.
+int launch_block_xupdate(const GmPtrs& P, const BkPtrs& K, int na, cudaStream_t s) {
+  if (na <= 0) return BEM_OK;
+  const int bx = (P.n + kXuThreads - 1) / kXuThreads;
+  int by = (2 * device_sms() + bx - 1) / bx;  // about two CTAs per SM in all
+  by = std::max(1, std::min(by, (na + kXuChunk - 1) / kXuChunk));
+  const dim3 grid(bx, by);
+  if (K.p <= 4)
+    (gm_block_xupdate_kernel<4><<<grid, kXuThreads, 0, s>>>(P, K, na), count_launch());
+  else if (K.p <= 8)
+    (gm_block_xupdate_kernel<8><<<grid, kXuThreads, 0, s>>>(P, K, na), count_launch());
+  else
+    (gm_block_xupdate_kernel<16><<<grid, kXuThreads, 0, s>>>(P, K, na), count_launch());
+  BEM_CUDA_TRY(cudaGetLastError());
+  return BEM_OK;
 }
 
 // Back substitution H y = g on the Givens-reduced Hessenberg matrix, one
@@ -3737,8 +3790,7 @@ extern "C" int bem_gmres_solve(const void* A, int n, const void* B, int m, void*
             BEM_CUDA_TRY(cudaMemcpyAsync(K[g].Yb, bY.data(), sizeof(double2) * bY.size(), cudaMemcpyHostToDevice, s));
             // bY is reused by the next group: the copy must have read it
             BEM_CUDA_TRY(cudaStreamSynchronize(s));
-            (gm_block_xupdate_kernel<<<dim3(gv.x, bshape.p[g]), 256, 0, s>>>(P, K[g], kk[g] * bshape.p[g]),
-             count_launch());
+            if ((rc = launch_block_xupdate(P, K[g], kk[g] * bshape.p[g], s))) return rc;
           }
           if (conv) break;
           if (none) {  // broke down at the first step: separate Krylov spaces instead
