@@ -476,6 +476,58 @@ __global__ void __launch_bounds__(256) tc_split_a_f16_kernel(const float* __rest
   }
 }
 
+// The same split with the row staged in shared memory (n even, ld a
+// multiple of 4, n / 2 float4 per row in dynamic shared memory): the matrix
+// is read from HBM once, for the maximum, and split from shared memory.
+__global__ void __launch_bounds__(256) tc_split_a_f16_smem_kernel(const float* __restrict__ A, int n, int ld,
+                                                                 __half* __restrict__ Ah, __half* __restrict__ Al,
+                                                                 float* __restrict__ rinv) {
+  extern __shared__ float4 rowbuf[];  // [n / 2]
+  __shared__ float red[8];
+  const int nv = n / 2;
+  for (int r = blockIdx.x; r < n; r += gridDim.x) {
+    const float4* row4 = reinterpret_cast<const float4*>(A + (size_t)r * 2 * n);
+    float mx = 0.f;
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nv; c += 256) {
+      const float4 v = __ldcs(row4 + c);
+      rowbuf[c] = v;
+      mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();  // also: rowbuf complete
+    float rmx = 0.f;
+#pragma unroll
+    for (int w = 0; w < 8; w++) rmx = fmaxf(rmx, red[w]);
+    const float q = f16_scale(rmx);
+    if (threadIdx.x == 0) rinv[r] = 1.f / q;
+    uint2* h4 = reinterpret_cast<uint2*>(Ah + (size_t)r * ld);
+    uint2* l4 = reinterpret_cast<uint2*>(Al + (size_t)r * ld);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < ld / 4; c += 256) {
+      float a[4] = {0.f, 0.f, 0.f, 0.f};
+      if (c < nv) {
+        const float4 v = rowbuf[c];
+        a[0] = v.x * q;
+        a[1] = v.y * q;
+        a[2] = v.z * q;
+        a[3] = v.w * q;
+      }
+      __align__(8) __half hi[4], lo[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        hi[e] = __float2half_rn(a[e]);
+        lo[e] = __float2half_rn(a[e] - __half2float(hi[e]));
+      }
+      h4[c] = *reinterpret_cast<const uint2*>(hi);
+      l4[c] = *reinterpret_cast<const uint2*>(lo);
+    }
+    __syncthreads();  // red and rowbuf are reused by the next row
+  }
+}
+
 // Column maxima of X (n x m complex64) for the fp16 scales: grid (blocks, m).
 __global__ void tc_colmax_kernel(const float2* __restrict__ X, int n, int m, unsigned* __restrict__ cmax) {
   const int s = blockIdx.y;
@@ -682,9 +734,28 @@ int tc_operator_prepare(const float2* A, int n, int precision, void* ws, cudaStr
   char* w = (char*)ws;
   BEM_CUDA_TRY(cudaMemsetAsync(w + L.hdr, 0, 256, s));
   if (precision == BEM_PREC_FP16X3) {
-    (tc_split_a_f16_kernel<<<n < 1184 ? n : 1184, 256, 0, s>>>((const float*)A, n, L.ld, (__half*)(w + L.ah),
-                                                                (__half*)(w + L.alo), (float*)(w + L.rinv)),
-     count_launch());
+    // a row of up to 96 KB staged in shared memory (two CTAs per SM), else two reads of it
+    const size_t row_bytes = sizeof(float4) * (size_t)(n / 2);
+    const bool staged = (n & 1) == 0 && (L.ld & 3) == 0 && ((uintptr_t)A & 15) == 0 && row_bytes <= 96 * 1024;
+    if (staged) {
+      static std::atomic<bool> attr{false};
+      if (!attr.load(std::memory_order_acquire)) {
+        BEM_CUDA_TRY(cudaFuncSetAttribute(tc_split_a_f16_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          96 * 1024));
+        attr.store(true, std::memory_order_release);
+      }
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const int grid = std::min(n, 2 * sms);
+      (tc_split_a_f16_smem_kernel<<<grid, 256, row_bytes, s>>>((const float*)A, n, L.ld, (__half*)(w + L.ah),
+                                                               (__half*)(w + L.alo), (float*)(w + L.rinv)),
+       count_launch());
+    } else {
+      (tc_split_a_f16_kernel<<<n < 1184 ? n : 1184, 256, 0, s>>>((const float*)A, n, L.ld, (__half*)(w + L.ah),
+                                                                  (__half*)(w + L.alo), (float*)(w + L.rinv)),
+       count_launch());
+    }
   } else {
     (tc_split_a_kernel<<<1184, 256, 0, s>>>((const float*)A, n, L.ld, (__nv_bfloat16*)(w + L.ah),
                                             precision == BEM_PREC_BF16X3 ? (__nv_bfloat16*)(w + L.alo) : nullptr),
