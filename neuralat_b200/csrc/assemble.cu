@@ -32,6 +32,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "async_copy.cuh"
 #include "bem_common.cuh"
@@ -692,20 +693,47 @@ struct SingularAcc {
       gki = (s - kr * c) * f;
     }
     const R lx[3] = {lx0, lx1, lx2}, ly[3] = {ly0, ly1, ly2};
-#pragma unroll
-    for (int ii = 0; ii < 3; ii++)
+    if constexpr (std::is_same<R, float>::value) {
+      // packed FP32: (re, im) pairs, the trial weight applied first (3 + 3
+      // multiplies, then one packed FMA per entry and kernel)
+      float2 gy[3], ky[3];
 #pragma unroll
       for (int jj = 0; jj < 3; jj++) {
-        const R f = lx[ii] * ly[jj];
-        if (DO_V) {
-          v[2 * (3 * ii + jj)] += gvr * f;
-          v[2 * (3 * ii + jj) + 1] += gvi * f;
-        }
-        if (DO_K) {
-          kk[2 * (3 * ii + jj)] += gkr * f;
-          kk[2 * (3 * ii + jj) + 1] += gki * f;
-        }
+        gy[jj] = f2_mul(f2(ly[jj]), make_float2(gvr, gvi));
+        ky[jj] = f2_mul(f2(ly[jj]), make_float2(gkr, gki));
       }
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+          const int e = 3 * ii + jj;
+          if (DO_V) {
+            const float2 t = f2_fma(f2(lx[ii]), gy[jj], make_float2(v[2 * e], v[2 * e + 1]));
+            v[2 * e] = t.x;
+            v[2 * e + 1] = t.y;
+          }
+          if (DO_K) {
+            const float2 t = f2_fma(f2(lx[ii]), ky[jj], make_float2(kk[2 * e], kk[2 * e + 1]));
+            kk[2 * e] = t.x;
+            kk[2 * e + 1] = t.y;
+          }
+        }
+    } else {
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+          const R f = lx[ii] * ly[jj];
+          if (DO_V) {
+            v[2 * (3 * ii + jj)] += gvr * f;
+            v[2 * (3 * ii + jj) + 1] += gvi * f;
+          }
+          if (DO_K) {
+            kk[2 * (3 * ii + jj)] += gkr * f;
+            kk[2 * (3 * ii + jj) + 1] += gki * f;
+          }
+        }
+    }
   }
 
   // One 4D Gauss point (xi, e1, e2, e3 on [0,1]) of weight w0; the region
