@@ -93,11 +93,13 @@ __global__ void b2p_density_kernel(GeomView g, const float2* __restrict__ neu, c
 }
 
 constexpr int kB2PThreads = 256;
-constexpr int kB2PRhs = 8;  // right-hand sides per register pass
 
 // out[p, s] += sum_{jq in chunk} G(x_p, y_jq) dn[jq, s] + D(x_p, y_jq) dd[jq, s]
 // (the -1, the weights and 1/(4 pi) are inside dn/dd).  Block = 32 listeners
-// (lanes) x one chunk of quadrature points split over 8 warps.
+// (lanes) x one chunk of quadrature points split over 8 warps; kB2PRhs
+// right-hand sides per pass (8, or 16 for more than 8 right-hand sides: the
+// distances and sin/cos are computed once per pass).
+template <int kB2PRhs>
 __global__ void __launch_bounds__(kB2PThreads)
     b2p_eval_kernel(GeomView g, const float* __restrict__ pts, int np, float k, const float2* __restrict__ dn,
                     const float2* __restrict__ dd, int nrhs, int rhs0, int chunk, float2* __restrict__ out) {
@@ -228,9 +230,13 @@ int b2p_enqueue(const GeomView& g, const float* points, int np, float k, const v
   int chunk = (nq + nchunks - 1) / nchunks;
   chunk = chunk < 256 ? 256 : chunk;
   nchunks = (nq + chunk - 1) / chunk;
-  for (int r0 = 0; r0 < nrhs; r0 += kB2PRhs) {
-    (b2p_eval_kernel<<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, r0, chunk,
-                                                                   (float2*)out), count_launch());
+  if (nrhs <= 8) {
+    (b2p_eval_kernel<8><<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, 0, chunk,
+                                                                      (float2*)out), count_launch());
+  } else {
+    for (int r0 = 0; r0 < nrhs; r0 += 16)
+      (b2p_eval_kernel<16><<<dim3(ptiles, nchunks), kB2PThreads, 0, s>>>(g, points, np, k, dn, dd, nrhs, r0, chunk,
+                                                                         (float2*)out), count_launch());
   }
   BEM_CUDA_TRY(cudaGetLastError());
   return BEM_OK;
